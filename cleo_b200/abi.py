@@ -1,0 +1,248 @@
+"""ctypes mirror of include/cleo_b200.h and the loader of the CUDA library.
+
+The structures here have exactly the field order and types of the C header, so one set of
+structures serves the CUDA library (``libcleo_b200.so``) and, in the tests, the CPU checkers that
+share its API shape. Loading the CUDA library never falls back to anything: if the shared object
+is missing, :func:`load_library` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libcleo_b200.so"
+
+STEP_OFF = 0xFFFFFFFF
+OOB = 0xFFFFFFFF
+
+# status codes (enum cleo_status)
+STATUS = {
+    0: "CLEO_OK",
+    1: "CLEO_ERR_XI_ZERO",
+    2: "CLEO_ERR_RADIUS_BELOW_DRY",
+    3: "CLEO_ERR_NEG_CONDENSATE",
+    4: "CLEO_ERR_COALESCENCE",
+    5: "CLEO_ERR_BREAKUP",
+    6: "CLEO_ERR_NR_NOCONVERGE",
+    7: "CLEO_ERR_SUBDELT",
+    8: "CLEO_ERR_CFL",
+    9: "CLEO_ERR_OUT_OF_BOX",
+    10: "CLEO_ERR_TEMPERATURE",
+    11: "CLEO_ERR_CAPACITY",
+    12: "CLEO_ERR_ARGUMENT",
+    13: "CLEO_ERR_CUDA",
+    14: "CLEO_ERR_TIMEOUT",
+    15: "CLEO_ERR_MLP",
+}
+CODE = {v: k for k, v in STATUS.items()}
+
+TV_NULL, TV_SIMMEL, TV_ROGERSYAU, TV_ROGERSGK = 0, 1, 2, 3
+PROB_GOLOVIN, PROB_LONG, PROB_CONST = 0, 1, 2
+ENACT_COALESCENCE, ENACT_BREAKUP, ENACT_COALBURE = 0, 1, 2
+NFRAGS_CONST, NFRAGS_CKE = 0, 1
+FLAG_STRAUB, FLAG_TESTIKSTRAUB, FLAG_SZAKALLURBICH, FLAG_CONST = 0, 1, 2, 3
+NRSEED_REFERENCE, NRSEED_MLP = 0, 1
+
+_d = C.POINTER(C.c_double)
+_u32 = C.POINTER(C.c_uint32)
+_u64 = C.POINTER(C.c_uint64)
+
+
+class Params(C.Structure):
+    """cleo_b200_params."""
+
+    _fields_ = [
+        ("condstep", C.c_uint32),
+        ("collstep", C.c_uint32),
+        ("motionstep", C.c_uint32),
+        ("pad0", C.c_uint32),
+        ("cond_delt", C.c_double),
+        ("cond_minsubdelt", C.c_double),
+        ("coll_delt", C.c_double),
+        ("motion_delt", C.c_double),
+        ("do_alter_thermo", C.c_int32),
+        ("maxniters", C.c_uint32),
+        ("rtol", C.c_double),
+        ("atol", C.c_double),
+        ("coll_prob", C.c_int32),
+        ("coll_enact", C.c_int32),
+        ("coaleff", C.c_double),
+        ("const_kernel", C.c_double),
+        ("nfrags_kind", C.c_int32),
+        ("nfrags_tv", C.c_int32),
+        ("nfrags", C.c_double),
+        ("flag_kind", C.c_int32),
+        ("flag_tv", C.c_int32),
+        ("flag_coaleff", C.c_double),
+        ("seed", C.c_uint64),
+        ("motion_tv", C.c_int32),
+        ("nr_seed", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Grid(C.Structure):
+    """cleo_b200_grid (pointers into numpy arrays kept alive by the owner)."""
+
+    _fields_ = [
+        ("ngbxs", C.c_uint32),
+        ("ndims", C.c_uint32 * 3),
+        ("coord3lo", _d), ("coord3hi", _d),
+        ("coord1lo", _d), ("coord1hi", _d),
+        ("coord2lo", _d), ("coord2hi", _d),
+        ("back3", _u32), ("fwd3", _u32),
+        ("back1", _u32), ("fwd1", _u32),
+        ("back2", _u32), ("fwd2", _u32),
+    ]
+
+
+STATE_FIELDS = ("volume", "press", "temp", "qvap", "qcond",
+                "wvel_lo", "wvel_hi", "uvel_lo", "uvel_hi", "vvel_lo", "vvel_hi")
+
+
+class GbxState(C.Structure):
+    """cleo_b200_gbx_state."""
+
+    _fields_ = [(f, _d) for f in STATE_FIELDS]
+
+
+SUPERS_FIELDS = (("sdgbxindex", np.uint32), ("coord3", np.float64), ("coord1", np.float64),
+                 ("coord2", np.float64), ("xi", np.uint64), ("radius", np.float64),
+                 ("msol", np.float64), ("sdid", np.uint64))
+
+
+class Supers(C.Structure):
+    """cleo_b200_supers."""
+
+    _fields_ = [
+        ("sdgbxindex", _u32),
+        ("coord3", _d), ("coord1", _d), ("coord2", _d),
+        ("xi", _u64),
+        ("radius", _d), ("msol", _d),
+        ("sdid", _u64),
+    ]
+
+
+class Error(C.Structure):
+    """cleo_b200_error."""
+
+    _fields_ = [("code", C.c_int32), ("gbxindex", C.c_uint32), ("index", C.c_uint64)]
+
+
+def ptr(a: np.ndarray, ctype):
+    """Pointer to the data of a contiguous numpy array."""
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+_CT = {np.float64: C.c_double, np.uint32: C.c_uint32, np.uint64: C.c_uint64}
+
+
+def supers_struct(arrs: dict) -> Supers:
+    """Supers struct pointing at the numpy arrays of ``arrs`` (keys of SUPERS_FIELDS)."""
+    s = Supers()
+    for name, dt in SUPERS_FIELDS:
+        a = arrs.get(name)
+        if a is None:
+            setattr(s, name, None)
+        else:
+            assert a.dtype == dt, (name, a.dtype)
+            setattr(s, name, ptr(a, _CT[dt]))
+    return s
+
+
+def state_struct(arrs: dict) -> GbxState:
+    st = GbxState()
+    for f in STATE_FIELDS:
+        a = arrs[f]
+        assert a.dtype == np.float64
+        setattr(st, f, ptr(a, C.c_double))
+    return st
+
+
+def grid_struct(g: dict) -> Grid:
+    gr = Grid()
+    gr.ngbxs = int(g["ngbxs"])
+    for i in range(3):
+        gr.ndims[i] = int(g["ndims"][i])
+    for f in ("coord3lo", "coord3hi", "coord1lo", "coord1hi", "coord2lo", "coord2hi"):
+        setattr(gr, f, ptr(g[f], C.c_double))
+    for f in ("back3", "fwd3", "back1", "fwd1", "back2", "fwd2"):
+        setattr(gr, f, ptr(g[f], C.c_uint32))
+    return gr
+
+
+def declare_api(lib: C.CDLL, prefix: str) -> C.CDLL:
+    """Declare argtypes/restype of the context API ``<prefix>_create`` ... on ``lib``."""
+    vp = C.c_void_p
+    f = getattr(lib, f"{prefix}_create")
+    f.argtypes = [C.POINTER(Params), C.POINTER(Grid), C.c_size_t, C.POINTER(vp)]
+    f.restype = C.c_int
+    f = getattr(lib, f"{prefix}_destroy")
+    f.argtypes = [vp]
+    f.restype = None
+    f = getattr(lib, f"{prefix}_upload_supers")
+    f.argtypes = [vp, C.POINTER(Supers), C.c_size_t]
+    f.restype = C.c_int
+    f = getattr(lib, f"{prefix}_upload_state")
+    f.argtypes = [vp, C.POINTER(GbxState)]
+    f.restype = C.c_int
+    f = getattr(lib, f"{prefix}_step")
+    f.argtypes = [vp, C.c_uint32, C.c_uint32]
+    f.restype = C.c_int
+    f = getattr(lib, f"{prefix}_status")
+    f.argtypes = [vp, C.POINTER(Error)]
+    f.restype = C.c_int
+    f = getattr(lib, f"{prefix}_download_supers")
+    f.argtypes = [vp, C.POINTER(Supers), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+    f.restype = C.c_int
+    f = getattr(lib, f"{prefix}_download_state")
+    f.argtypes = [vp, C.POINTER(GbxState)]
+    f.restype = C.c_int
+    f = getattr(lib, f"{prefix}_download_budgets")
+    f.argtypes = [vp, _d, _u64]
+    f.restype = C.c_int
+    return lib
+
+
+# Every symbol include/cleo_b200.h declares (checked by the CPU tests against the built library).
+EXPORTED = (
+    "cleo_b200_create", "cleo_b200_destroy", "cleo_b200_upload_supers", "cleo_b200_upload_state",
+    "cleo_b200_step", "cleo_b200_status", "cleo_b200_domain_nsupers", "cleo_b200_download_supers",
+    "cleo_b200_download_state", "cleo_b200_download_budgets", "cleo_b200_condensation_solve",
+    "cleo_b200_stream", "cleo_b200_version",
+)
+
+_LIB = None
+
+
+def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
+    """Load libcleo_b200.so (built in-tree by ``__graft_entry__.build()``); raises if absent."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(
+            f"{p} is missing: build the CUDA library first (python -c "
+            f"'import __graft_entry__ as g; g.build()'); there is no CPU fallback")
+    lib = C.CDLL(str(p), mode=C.RTLD_GLOBAL)
+    declare_api(lib, "cleo_b200")
+    vp = C.c_void_p
+    lib.cleo_b200_domain_nsupers.argtypes = [vp, C.POINTER(C.c_size_t)]
+    lib.cleo_b200_domain_nsupers.restype = C.c_int
+    lib.cleo_b200_condensation_solve.argtypes = [vp, C.c_size_t] + [vp] * 6 + [vp, vp]
+    lib.cleo_b200_condensation_solve.restype = C.c_int
+    lib.cleo_b200_stream.argtypes = [vp]
+    lib.cleo_b200_stream.restype = vp
+    lib.cleo_b200_version.argtypes = []
+    lib.cleo_b200_version.restype = C.c_char_p
+    if path is None:
+        _LIB = lib
+    return lib

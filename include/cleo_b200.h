@@ -1,0 +1,242 @@
+/*
+ * cleo_b200.h — C ABI of the B200 super-droplet microphysics hot path.
+ *
+ * One context owns the device structure-of-arrays (SoA) superdroplet state, the per-gridbox
+ * thermodynamic state, the Cartesian gridbox maps and all scratch memory for one domain on one
+ * GPU. Every entry point takes plain pointers and sizes; no C++ or torch types cross this
+ * boundary. All quantities are CLEO's non-dimensional ones (cleoconstants.hpp:72-102): radii in
+ * units of R0 = 1e-6 m, coordinates in COORD0 = 1000 m, volumes in VOL0 = 1e9 m^3, time in
+ * TIME0 = 1000 s, pressure in P0, temperature in TEMP0.
+ *
+ * Reference interfaces replaced (paths relative to the CLEO project root):
+ *   cleo_b200_create        ~ SDMMethods ctor + create_supers/create_gbxs
+ *                             (libs/runcleo/sdmmethods.hpp:244-250, libs/runcleo/createsupers.hpp:111-138,
+ *                              libs/runcleo/creategbxs.hpp:170-351)
+ *   cleo_b200_step          ~ SDMMethods::run_step (libs/runcleo/sdmmethods.hpp:319-332), i.e.
+ *                             MoveSupersInDomain::run_step (libs/gridboxes/movesupersindomain.hpp:292-301)
+ *                             then sdm_microphysics (libs/runcleo/sdmmethods.hpp:184-230) with
+ *                             Condensation >> CollCoal/CoalBuRe/CollBu (libs/superdrops/condensation.hpp:242-253,
+ *                             libs/superdrops/collisions/coalescence.hpp:133-160,
+ *                             libs/superdrops/collisions/coalbure.hpp:156-185, breakup.hpp:97-123)
+ *   cleo_b200_upload_* /    ~ the DualView host<->device syncs RunCLEO does around coupling and
+ *   cleo_b200_download_*      observation steps (libs/runcleo/runcleo.hpp:163-175)
+ *   cleo_b200_status        ~ Kokkos::abort sites of the hot path, reported as status codes
+ *   cleo_b200_condensation_solve ~ ImplicitEuler::solve_condensation applied to a batch of
+ *                             independent droplets (libs/superdrops/impliciteuler.cpp:35-54)
+ *
+ * Threading: one context per host thread; calls on a context are serialised on its CUDA stream.
+ * Errors: every function returns a cleo_status. Device-side failures (the reference's abort
+ * sites) are recorded in a device error word and surface from cleo_b200_status(), which
+ * synchronises the context's stream. Kernels never trap.
+ */
+#ifndef CLEO_B200_H_
+#define CLEO_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes: 0 = ok, one code per reference abort site ---- */
+typedef enum cleo_status {
+  CLEO_OK = 0,
+  CLEO_ERR_XI_ZERO = 1,          /* superdrop_attrs.hpp:157-163  xi < 1 */
+  CLEO_ERR_RADIUS_BELOW_DRY = 2, /* superdrop_attrs.hpp:176-182  r < r_dry - 1e-6 */
+  CLEO_ERR_NEG_CONDENSATE = 3,   /* superdrop_attrs.hpp:208-218 */
+  CLEO_ERR_COALESCENCE = 4,      /* coalescence.cpp:109-111,134-143,180-188 */
+  CLEO_ERR_BREAKUP = 5,          /* breakup.hpp:198-256 */
+  CLEO_ERR_NR_NOCONVERGE = 6,    /* impliciteuler.cpp:213-217 */
+  CLEO_ERR_SUBDELT = 7,          /* impliciteuler.hpp:323-325 */
+  CLEO_ERR_CFL = 8,              /* cfl_criteria.hpp:52-54 */
+  CLEO_ERR_OUT_OF_BOX = 9,       /* cartesian_motion.hpp:44-52 */
+  CLEO_ERR_TEMPERATURE = 10,     /* thermodynamic_equations.cpp:40-42 */
+  CLEO_ERR_CAPACITY = 11,        /* more superdroplets or gridboxes than the context holds */
+  CLEO_ERR_ARGUMENT = 12,        /* invalid argument (null pointer, bad enum, size mismatch) */
+  CLEO_ERR_CUDA = 13,            /* a CUDA runtime call failed */
+  CLEO_ERR_TIMEOUT = 14,         /* a bounded device-side wait gave up */
+  CLEO_ERR_MLP = 15              /* surrogate not loaded / bad shape */
+} cleo_status;
+
+/* ---- enumerations of the reference's plug-in choices ---- */
+enum cleo_terminalv {        /* libs/superdrops/terminalvelocity.hpp:44-122 */
+  CLEO_TV_NULL = 0,
+  CLEO_TV_SIMMEL = 1,
+  CLEO_TV_ROGERSYAU = 2,
+  CLEO_TV_ROGERSGK = 3
+};
+enum cleo_collprob {         /* PairProbability models */
+  CLEO_PROB_GOLOVIN = 0,     /* golovinprob.cpp:31-43 */
+  CLEO_PROB_LONG = 1,        /* longhydroprob.hpp:38-66 (Simmel terminal velocity) */
+  CLEO_PROB_CONST = 2        /* constprob.hpp:34-49 */
+};
+enum cleo_collenact {        /* PairEnactX models */
+  CLEO_ENACT_COALESCENCE = 0, /* coalescence.cpp:39-54 */
+  CLEO_ENACT_BREAKUP = 1,     /* breakup.hpp:141-151 */
+  CLEO_ENACT_COALBURE = 2     /* coalbure.hpp:207-256 */
+};
+enum cleo_nfrags {           /* breakup_nfrags.hpp:40-92 */
+  CLEO_NFRAGS_CONST = 0,
+  CLEO_NFRAGS_CKE = 1
+};
+enum cleo_coalbureflag {     /* coalbure_flag.hpp:42-198 */
+  CLEO_FLAG_STRAUB = 0,
+  CLEO_FLAG_TESTIKSTRAUB = 1,
+  CLEO_FLAG_SZAKALLURBICH = 2,
+  CLEO_FLAG_CONST = 3
+};
+enum cleo_nrseed {           /* initial guess of the condensation Newton solve */
+  CLEO_NRSEED_REFERENCE = 0, /* ImplicitIterations::initialguess, impliciteuler.cpp:156-170 */
+  CLEO_NRSEED_MLP = 1        /* surrogate-predicted post-step r^2 */
+};
+
+#define CLEO_STEP_OFF 0xFFFFFFFFu /* interval value that switches a process off (on_step false) */
+
+/*
+ * Parameters: one field per argument of the reference factories. Intervals are integer model
+ * steps (model_step = 0.01 s, libs/initialise/timesteps.hpp:34); the *_delt fields are the
+ * doubles those factories derive from them, passed in so host and device share one value.
+ */
+typedef struct cleo_b200_params {
+  uint32_t condstep;        /* Condensation interval (condensation.hpp:242) */
+  uint32_t collstep;        /* CollCoal / CoalBuRe / CollBu interval */
+  uint32_t motionstep;      /* CartesianMotion interval (cartesian_motion.hpp:61) */
+  uint32_t pad0;
+  double cond_delt;         /* step2dimlesstime(condstep)  (condensation.hpp:246) */
+  double cond_minsubdelt;   /* realtime2dimless(MINSUBTSTEP) (condensation.hpp:247) */
+  double coll_delt;         /* step2realtime(collstep), seconds (coalescence.hpp:137) */
+  double motion_delt;       /* step2dimlesstime(motionstep) (predcorr.hpp:150) */
+  /* condensation (DoCondensation / ImplicitEuler ctor arguments) */
+  int32_t do_alter_thermo;
+  uint32_t maxniters;
+  double rtol;
+  double atol;
+  /* collisions */
+  int32_t coll_prob;        /* enum cleo_collprob */
+  int32_t coll_enact;       /* enum cleo_collenact */
+  double coaleff;           /* LongHydroProb(coaleff) */
+  double const_kernel;      /* ConstProb(k) */
+  int32_t nfrags_kind;      /* enum cleo_nfrags */
+  int32_t nfrags_tv;        /* terminal velocity used by CollisionKineticEnergyNFrags */
+  double nfrags;            /* ConstNFrags(nfrags) */
+  int32_t flag_kind;        /* enum cleo_coalbureflag */
+  int32_t flag_tv;          /* terminal velocity used by the Straub/TS/SU flags */
+  double flag_coaleff;      /* ConstCoalBuReFlag(coaleff) */
+  uint64_t seed;            /* seed of the injected counter-based random stream */
+  /* motion */
+  int32_t motion_tv;        /* terminal velocity subtracted from w (predcorr.hpp:83-105) */
+  int32_t nr_seed;          /* enum cleo_nrseed */
+} cleo_b200_params;
+
+/*
+ * Cartesian gridbox maps (the content of CartesianMaps, cartesianmaps.hpp:49-303, for an
+ * undecomposed domain): per gridbox {lower, upper} bounds in each direction and the index of the
+ * backwards/forwards neighbour. Index = iz + nz*(ix + nx*iy) (doubly_periodic_domain.hpp:41-70).
+ * A neighbour equal to 0xFFFFFFFF is out of the domain. Directions that a model does not resolve
+ * carry bounds {-DBL_MAX, DBL_MAX} and the gridbox itself as neighbour (createcartesianmaps.cpp:38-45).
+ */
+typedef struct cleo_b200_grid {
+  uint32_t ngbxs;
+  uint32_t ndims[3]; /* number of gridboxes along [coord3, coord1, coord2] */
+  const double *coord3lo, *coord3hi, *coord1lo, *coord1hi, *coord2lo, *coord2hi;
+  const uint32_t *back3, *fwd3, *back1, *fwd1, *back2, *fwd2;
+} cleo_b200_grid;
+
+/* Per-gridbox thermodynamic State (state.hpp:33-120) as SoA arrays of length ngbxs. */
+typedef struct cleo_b200_gbx_state {
+  double *volume, *press, *temp, *qvap, *qcond;
+  double *wvel_lo, *wvel_hi, *uvel_lo, *uvel_hi, *vvel_lo, *vvel_hi;
+} cleo_b200_gbx_state;
+
+/* Superdroplets (Superdrop, superdrop.hpp:36-48) as SoA arrays of length n. */
+typedef struct cleo_b200_supers {
+  uint32_t *sdgbxindex;
+  double *coord3, *coord1, *coord2;
+  uint64_t *xi;
+  double *radius, *msol;
+  uint64_t *sdid;
+} cleo_b200_supers;
+
+/* Where the first device-side failure happened. */
+typedef struct cleo_b200_error {
+  int32_t code;      /* cleo_status */
+  uint32_t gbxindex; /* gridbox of the failing superdroplet (0xFFFFFFFF if unknown) */
+  uint64_t index;    /* position of the failing superdroplet in the SoA arrays */
+} cleo_b200_error;
+
+typedef struct cleo_b200_ctx cleo_b200_ctx;
+
+/*
+ * Create a context on the current CUDA device for up to `capacity` superdroplets on the given
+ * grid. Allocates all device memory the context will use. Validates the parameters the way the
+ * reference constructors do (e.g. ImplicitEuler: cond_delt >= cond_minsubdelt).
+ */
+int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid, size_t capacity,
+                     cleo_b200_ctx** out);
+void cleo_b200_destroy(cleo_b200_ctx* ctx);
+
+/*
+ * Copy n superdroplets (host SoA) into the context and sort them by gridbox, like the
+ * SupersInDomain constructor (supersindomain.hpp:55-62). n <= capacity.
+ */
+int cleo_b200_upload_supers(cleo_b200_ctx* ctx, const cleo_b200_supers* host, size_t n);
+/* Copy ngbxs gridbox states (host SoA) into the context. */
+int cleo_b200_upload_state(cleo_b200_ctx* ctx, const cleo_b200_gbx_state* host);
+
+/*
+ * Advance the domain from model step t_mdl to t_next: motion + sort, then microphysics
+ * sub-stepping in every gridbox, then removal of null superdroplets (SDMMethods::run_step).
+ * Asynchronous: enqueues work on the context's stream. Device failures are reported by
+ * cleo_b200_status().
+ */
+int cleo_b200_step(cleo_b200_ctx* ctx, uint32_t t_mdl, uint32_t t_next);
+
+/* Synchronise the context's stream and return the first recorded failure (CLEO_OK if none). */
+int cleo_b200_status(cleo_b200_ctx* ctx, cleo_b200_error* err);
+
+/* Number of superdroplets inside the domain (SupersInDomain::domain_nsupers). Synchronises. */
+int cleo_b200_domain_nsupers(cleo_b200_ctx* ctx, size_t* n);
+
+/*
+ * Copy superdroplets back to host SoA arrays of length >= capacity. The first *n_domain entries
+ * are the in-domain superdroplets, sorted by gridbox with the reference's order inside each
+ * gridbox; the remaining *n_total - *n_domain are out of the domain (order unspecified, as in
+ * sortsupers.hpp:89-92).
+ */
+int cleo_b200_download_supers(cleo_b200_ctx* ctx, cleo_b200_supers* host, size_t* n_domain,
+                              size_t* n_total);
+/* Copy the gridbox states back. */
+int cleo_b200_download_state(cleo_b200_ctx* ctx, cleo_b200_gbx_state* host);
+/*
+ * Cumulative FP64 budgets per gridbox (length ngbxs each, may be NULL): condensed mass (the sum of
+ * the per-step totmass_condensed that DoCondensation reports to its monitor, condensation.hpp:149)
+ * and the number of Newton iterations spent by the condensation solves in the gridbox.
+ */
+int cleo_b200_download_budgets(cleo_b200_ctx* ctx, double* cond_mass, uint64_t* nr_iters);
+
+/*
+ * Solve one implicit-Euler condensation step for n independent droplets already resident in
+ * device memory (ImplicitEuler::solve_condensation, impliciteuler.cpp:35-54, with the
+ * per-droplet Kohler factors of thermodynamic_equations.hpp:95-107 and the diffusion factor of
+ * thermodynamic_equations.cpp:93-114). Inputs are device pointers of length n: radius, msol,
+ * temp, press, s_ratio and delt (dimensionless). Writes the new radius (after change_radius, i.e.
+ * not below the dry radius) to radius_out and, if niters_out is non-NULL, the Newton iterations
+ * spent per droplet. Uses the context's maxniters/rtol/atol/minsubdelt and nr_seed.
+ */
+int cleo_b200_condensation_solve(cleo_b200_ctx* ctx, size_t n, const double* d_radius,
+                                 const double* d_msol, const double* d_temp, const double* d_press,
+                                 const double* d_s_ratio, const double* d_delt,
+                                 double* d_radius_out, uint32_t* d_niters_out);
+
+/* The CUDA stream the context enqueues on (cudaStream_t, as void*). */
+void* cleo_b200_stream(cleo_b200_ctx* ctx);
+
+/* Library version string. */
+const char* cleo_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLEO_B200_H_ */

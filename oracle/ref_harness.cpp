@@ -1,0 +1,424 @@
+/*
+ * ref_harness.cpp — drives CLEO's own hot-path sources (TEST INFRASTRUCTURE ONLY).
+ *
+ * Compiled together with the reference's translation units, unmodified, against the
+ * project-written Kokkos-API shim in oracle/kokkos_shim (see oracle/Makefile). It builds the
+ * reference's own objects — CartesianMaps, Gridbox DualViews, SupersInDomain,
+ * MoveSupersInDomain<CartesianMaps, PredCorrMotion, CartesianTransportAcrossDomain,
+ * NullBoundaryConditions> and SDMMethods with Condensation >> DoCollisions — and exposes them
+ * through the same C-API shape as oracle/cleo_oracle.h (prefix ref_ instead of oc_).
+ *
+ * The only project code on the arithmetic path is the dispatch below: small structs that satisfy
+ * the reference's VelocityFormula / PairProbability / PairEnactX / NFragments / CoalBuReFlag
+ * concepts by forwarding to the reference's own implementations, so that one instantiation of
+ * SDMMethods serves every plug-in combination selected at run time. DoCollisions is built the
+ * way CollCoal/CollBu/CoalBuRe build it (coalescence.hpp:149-160, breakup.hpp:111-123,
+ * coalbure.hpp:173-185) and Condensation through its own factory (condensation.hpp:242-253).
+ */
+#include <cfloat>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../include/cleo_b200.h"
+#include "cartesiandomain/cartesianmaps.hpp"
+#include "cartesiandomain/movement/cartesian_motion.hpp"
+#include "cartesiandomain/movement/cartesian_movement.hpp"
+#include "gridboxes/boundary_conditions.hpp"
+#include "runcleo/sdmmethods.hpp"
+#include "superdrops/collisions/breakup.hpp"
+#include "superdrops/collisions/breakup_nfrags.hpp"
+#include "superdrops/collisions/coalbure.hpp"
+#include "superdrops/collisions/coalbure_flag.hpp"
+#include "superdrops/collisions/coalescence.hpp"
+#include "superdrops/collisions/collisions.hpp"
+#include "superdrops/collisions/constprob.hpp"
+#include "superdrops/collisions/golovinprob.hpp"
+#include "superdrops/collisions/longhydroprob.hpp"
+#include "superdrops/condensation.hpp"
+#include "superdrops/impliciteuler.hpp"
+#include "superdrops/microphysicalprocess.hpp"
+#include "superdrops/terminalvelocity.hpp"
+#include "superdrops/thermodynamic_equations.hpp"
+
+namespace {
+
+/* ---- run-time selection of the reference's plug-ins ---- */
+struct AnyTV {
+  int kind = CLEO_TV_NULL;
+  KOKKOS_FUNCTION double operator()(const Superdrop& d) const {
+    switch (kind) {
+      case CLEO_TV_SIMMEL: return SimmelTerminalVelocity{}(d);
+      case CLEO_TV_ROGERSYAU: return RogersYauTerminalVelocity{}(d);
+      case CLEO_TV_ROGERSGK: return RogersGKTerminalVelocity{}(d);
+      default: return NullTerminalVelocity{}(d);
+    }
+  }
+};
+
+struct AnyProb {
+  int kind;
+  GolovinProb golovin;
+  LongHydroProb longhydro;
+  ConstProb constprob;
+  AnyProb(int k, double coaleff, double kernel)
+      : kind(k), golovin(), longhydro(coaleff), constprob(kernel) {}
+  KOKKOS_FUNCTION double operator()(const Superdrop& a, const Superdrop& b, const double DELT,
+                                    const double VOLUME) const {
+    switch (kind) {
+      case CLEO_PROB_GOLOVIN: return golovin(a, b, DELT, VOLUME);
+      case CLEO_PROB_LONG: return longhydro(a, b, DELT, VOLUME);
+      default: return constprob(a, b, DELT, VOLUME);
+    }
+  }
+};
+
+struct AnyNFrags {
+  int kind;
+  ConstNFrags cnf;
+  CollisionKineticEnergyNFrags<AnyTV> cke;
+  AnyNFrags(int k, double nfrags, int tv) : kind(k), cnf(nfrags), cke(AnyTV{tv}) {}
+  KOKKOS_FUNCTION double operator()(const Superdrop& a, const Superdrop& b) const {
+    return kind == CLEO_NFRAGS_CONST ? cnf(a, b) : cke(a, b);
+  }
+};
+
+struct AnyFlag {
+  int kind;
+  StraubCoalBuReFlag<AnyTV> straub;
+  TSCoalBuReFlag<AnyTV> ts;
+  SUCoalBuReFlag<AnyTV> su;
+  ConstCoalBuReFlag cst;
+  AnyFlag(int k, int tv, double coaleff)
+      : kind(k), straub(AnyTV{tv}), ts(AnyTV{tv}), su(AnyTV{tv}), cst(coaleff) {}
+  KOKKOS_FUNCTION unsigned int operator()(const double phi, const Superdrop& a,
+                                          const Superdrop& b) const {
+    switch (kind) {
+      case CLEO_FLAG_STRAUB: return straub(phi, a, b);
+      case CLEO_FLAG_TESTIKSTRAUB: return ts(phi, a, b);
+      case CLEO_FLAG_SZAKALLURBICH: return su(phi, a, b);
+      default: return cst(phi, a, b);
+    }
+  }
+};
+
+struct AnyEnact {
+  int kind;
+  DoCoalescence coal;
+  DoBreakup<AnyNFrags> bu;
+  DoCoalBuRe<AnyNFrags, AnyFlag> coalbure;
+  AnyEnact(int k, AnyNFrags nf, AnyFlag fl) : kind(k), coal(), bu(nf), coalbure(nf, fl) {}
+  KOKKOS_FUNCTION size_t operator()(Superdrop& d1, Superdrop& d2, const double prob,
+                                    const double phi_coll, const double phi_out) const {
+    switch (kind) {
+      case CLEO_ENACT_COALESCENCE: return coal(d1, d2, prob, phi_coll, phi_out);
+      case CLEO_ENACT_BREAKUP: return bu(d1, d2, prob, phi_coll, phi_out);
+      default: return coalbure(d1, d2, prob, phi_coll, phi_out);
+    }
+  }
+};
+
+/* ---- monitor that accumulates the condensed mass per gridbox (condensation.hpp:149) ---- */
+struct BudgetMonitor {
+  Kokkos::View<double*> cond_mass;
+  void reset_monitor() const {}
+  KOKKOS_FUNCTION void before_timestepping(const TeamMember&, const viewd_constsupers) const {}
+  KOKKOS_FUNCTION void monitor_condensation(const TeamMember& tm, const double d) const {
+    cond_mass(tm.league_rank()) += d;
+  }
+  KOKKOS_FUNCTION void monitor_microphysics(const TeamMember&, const viewd_constsupers) const {}
+  void monitor_motion(const auto, const auto) const {}
+  KOKKOS_FUNCTION void monitor_precipitation(const TeamMember&, const unsigned int, const auto&,
+                                             Superdrop&) const {}
+};
+struct BudgetObserver {
+  BudgetMonitor mo;
+  void before_timestepping(const viewd_constgbx, const subviewd_constsupers) const {}
+  void after_timestepping() const {}
+  unsigned int next_obs(const unsigned int) const { return LIMITVALUES::uintmax; }
+  bool on_step(const unsigned int) const { return false; }
+  void at_start_step(const unsigned int, const viewd_constgbx, const subviewd_constsupers) const {}
+  SDMMonitor auto get_sdmmonitor() const { return mo; }
+};
+
+using Colls = ConstTstepMicrophysics<DoCollisions<AnyProb, AnyEnact>>;
+using Cond = decltype(Condensation(1u, std::function<double(unsigned int)>{}, false, 1, 0.0, 0.0,
+                                   0.0, std::function<double(double)>{}));
+using Microphys = CombinedMicrophysicalProcess<Cond, Colls>;
+using MotionT = PredCorrMotion<CartesianMaps, AnyTV, CartesianCheckBounds>;
+using MoveT = MoveSupersInDomain<CartesianMaps, MotionT, CartesianTransportAcrossDomain,
+                                 NullBoundaryConditions>;
+using SDM = SDMMethods<CartesianMaps, Microphys, MotionT, CartesianTransportAcrossDomain,
+                       NullBoundaryConditions, BudgetObserver>;
+
+int code_of(const std::string& m) {
+  if (m.find("xi should not be less than 1") != std::string::npos) return CLEO_ERR_XI_ZERO;
+  if (m.find("less than dry radius") != std::string::npos) return CLEO_ERR_RADIUS_BELOW_DRY;
+  if (m.find("condensate mass cannot") != std::string::npos) return CLEO_ERR_NEG_CONDENSATE;
+  if (m.find("coalescence") != std::string::npos || m.find("colllision") != std::string::npos)
+    return CLEO_ERR_COALESCENCE;
+  if (m.find("nfrags") != std::string::npos) return CLEO_ERR_BREAKUP;
+  if (m.find("No root converged") != std::string::npos) return CLEO_ERR_NR_NOCONVERGE;
+  if (m.find("subtimestep") != std::string::npos) return CLEO_ERR_SUBDELT;
+  if (m.find("CFL") != std::string::npos) return CLEO_ERR_CFL;
+  if (m.find("SD not in previous gbx") != std::string::npos) return CLEO_ERR_OUT_OF_BOX;
+  if (m.find("psat ERROR") != std::string::npos) return CLEO_ERR_TEMPERATURE;
+  return CLEO_ERR_ARGUMENT;
+}
+
+}  // namespace
+
+struct ref_ctx {
+  cleo_b200_params p;
+  uint32_t ngbxs;
+  CartesianMaps gbxmaps;
+  std::unique_ptr<SDM> sdm;
+  dualview_gbx gbxs;
+  std::unique_ptr<SupersInDomain> allsupers;
+  Kokkos::View<double*> cond_mass;
+  cleo_b200_error err{CLEO_OK, 0xFFFFFFFFu, 0};
+};
+
+static void fail(ref_ctx* c, int code) {
+  if (c->err.code == CLEO_OK) c->err.code = code;
+}
+
+extern "C" {
+
+void ref_set_num_threads(int n) { kokkos_shim::set_num_threads(n); }
+
+int ref_create(const cleo_b200_params* p, const cleo_b200_grid* g, size_t capacity,
+               ref_ctx** out) {
+  if (!p || !g || !out) return CLEO_ERR_ARGUMENT;
+  auto c = std::make_unique<ref_ctx>();
+  c->p = *p;
+  c->ngbxs = g->ngbxs;
+  try {
+    /* CartesianMaps for an undecomposed domain, filled like set_cartesian_maps
+     * (createcartesianmaps.cpp:143-252) from the given bounds and neighbours. */
+    const size_t sz = (size_t)g->ngbxs + 1;
+    const auto h3 = kokkos_pairmap::HostMirror(sz), h1 = kokkos_pairmap::HostMirror(sz),
+               h2 = kokkos_pairmap::HostMirror(sz);
+    const auto b3 = kokkos_uintmap::HostMirror(sz), f3 = kokkos_uintmap::HostMirror(sz),
+               b1 = kokkos_uintmap::HostMirror(sz), f1 = kokkos_uintmap::HostMirror(sz),
+               b2 = kokkos_uintmap::HostMirror(sz), f2 = kokkos_uintmap::HostMirror(sz);
+    const auto areas = kokkos_dblmaph(sz), vols = kokkos_dblmaph(sz);
+    const auto oob = LIMITVALUES::oob_gbxindex;
+    const Kokkos::pair<double, double> nullb{LIMITVALUES::llim, LIMITVALUES::ulim};
+    h3.insert(oob, nullb); h1.insert(oob, nullb); h2.insert(oob, nullb);
+    b3.insert(oob, oob); f3.insert(oob, oob); b1.insert(oob, oob);
+    f1.insert(oob, oob); b2.insert(oob, oob); f2.insert(oob, oob);
+    areas.insert(oob, 0.0); vols.insert(oob, 0.0);
+    for (unsigned int i = 0; i < g->ngbxs; ++i) {
+      h3.insert(i, {g->coord3lo[i], g->coord3hi[i]});
+      h1.insert(i, {g->coord1lo[i], g->coord1hi[i]});
+      h2.insert(i, {g->coord2lo[i], g->coord2hi[i]});
+      b3.insert(i, g->back3[i]); f3.insert(i, g->fwd3[i]);
+      b1.insert(i, g->back1[i]); f1.insert(i, g->fwd1[i]);
+      b2.insert(i, g->back2[i]); f2.insert(i, g->fwd2[i]);
+      areas.insert(i, 0.0); vols.insert(i, 0.0);
+    }
+    c->gbxmaps.set_coord3bounds_via_copy(h3);
+    c->gbxmaps.set_coord1bounds_via_copy(h1);
+    c->gbxmaps.set_coord2bounds_via_copy(h2);
+    c->gbxmaps.set_back_coord3nghbr_via_copy(b3);
+    c->gbxmaps.set_forward_coord3nghbr_via_copy(f3);
+    c->gbxmaps.set_back_coord1nghbr_via_copy(b1);
+    c->gbxmaps.set_forward_coord1nghbr_via_copy(f1);
+    c->gbxmaps.set_back_coord2nghbr_via_copy(b2);
+    c->gbxmaps.set_forward_coord2nghbr_via_copy(f2);
+    c->gbxmaps.set_gbxareas_map(areas);
+    c->gbxmaps.set_gbxvolumes_map(vols);
+    auto hnd = Kokkos::create_mirror_view(c->gbxmaps.get_global_ndims());
+    for (int m = 0; m < 3; ++m) hnd(m) = g->ndims[m];
+    c->gbxmaps.set_global_ndims_via_copy(hnd);
+
+    /* microphysics: Condensation >> collisions */
+    const auto P = c->p;
+    const Cond cond = Condensation(
+        P.condstep, [P](unsigned int) { return P.cond_delt; }, P.do_alter_thermo != 0,
+        P.maxniters, P.rtol, P.atol, 0.0, [P](double) { return P.cond_minsubdelt; });
+    const AnyNFrags nf(P.nfrags_kind, P.nfrags, P.nfrags_tv);
+    const AnyFlag fl(P.flag_kind, P.flag_tv, P.flag_coaleff);
+    const AnyEnact enact(P.coll_enact, nf, fl);
+    const AnyProb prob(P.coll_prob, P.coaleff, P.const_kernel);
+    const Colls colls(P.collstep, DoCollisions<AnyProb, AnyEnact>(P.coll_delt, prob, enact, P.seed));
+    const Microphys microphys = cond >> colls;
+
+    /* motion: CartesianMotion (cartesian_motion.hpp:60-66) + cartesian_movement */
+    const MotionT motion = CartesianMotion(P.motionstep, [P](unsigned int) { return P.motion_delt; },
+                                           AnyTV{P.motion_tv});
+    const MoveT movesupers = cartesian_movement(c->gbxmaps, motion, NullBoundaryConditions{});
+
+    c->cond_mass = Kokkos::View<double*>("cond_mass", g->ngbxs);
+    BudgetObserver obs{BudgetMonitor{c->cond_mass}};
+    const unsigned int couplstep = P.motionstep == CLEO_STEP_OFF ? 1u : P.motionstep;
+    c->sdm = std::make_unique<SDM>(couplstep, c->gbxmaps, microphys, movesupers, obs);
+    c->gbxs = dualview_gbx("gbxs", g->ngbxs);
+    (void)capacity;
+  } catch (const kokkos_shim::Abort& e) {
+    return code_of(e.what());
+  }
+  *out = c.release();
+  return CLEO_OK;
+}
+
+void ref_destroy(ref_ctx* c) { delete c; }
+
+int ref_upload_supers(ref_ctx* c, const cleo_b200_supers* h, size_t n) {
+  try {
+    viewd_supers totsupers("totsupers", n);
+    for (size_t k = 0; k < n; ++k) {
+      const SuperdropAttrs attrs(SoluteProperties{}, h->xi[k], h->radius[k], h->msol[k], true);
+      totsupers(k) = Superdrop(h->sdgbxindex[k], h->coord3[k], h->coord1[k], h->coord2[k], attrs,
+                               IntID{h->sdid ? (size_t)h->sdid[k] : k});
+    }
+    c->allsupers = std::make_unique<SupersInDomain>(totsupers, c->ngbxs);
+    /* gridboxes refer to the sorted superdroplets (Gridbox ctor, gridbox.hpp:44-46) */
+    auto hg = c->gbxs.view_host();
+    for (unsigned int ii = 0; ii < c->ngbxs; ++ii) {
+      const State st = hg(ii).state;
+      hg(ii) = Gridbox(Gbxindex{ii}, st, c->allsupers->domain_supers_readonly());
+    }
+  } catch (const kokkos_shim::Abort& e) {
+    fail(c, code_of(e.what()));
+    return c->err.code;
+  }
+  return CLEO_OK;
+}
+
+int ref_upload_state(ref_ctx* c, const cleo_b200_gbx_state* h) {
+  auto hg = c->gbxs.view_host();
+  for (unsigned int ii = 0; ii < c->ngbxs; ++ii) {
+    const State st(h->volume[ii], h->press[ii], h->temp[ii], h->qvap[ii], h->qcond[ii],
+                   {h->wvel_lo[ii], h->wvel_hi[ii]}, {h->uvel_lo[ii], h->uvel_hi[ii]},
+                   {h->vvel_lo[ii], h->vvel_hi[ii]});
+    if (c->allsupers) {
+      hg(ii) = Gridbox(Gbxindex{ii}, st, c->allsupers->domain_supers_readonly());
+    } else {
+      hg(ii).gbxindex = Gbxindex{ii};
+      hg(ii).state = st;
+    }
+  }
+  return CLEO_OK;
+}
+
+/* One SDMMethods::run_step call per SDM step, so that the injected stream is keyed by t_sdm. */
+int ref_step(ref_ctx* c, uint32_t t_mdl, uint32_t t_next) {
+  if (c->err.code != CLEO_OK) return c->err.code;
+  try {
+    uint32_t t_sdm = t_mdl;
+    while (t_sdm < t_next) {
+      uint32_t next_move = CLEO_STEP_OFF;
+      if (c->p.motionstep != CLEO_STEP_OFF) next_move = ((t_sdm / c->p.motionstep) + 1) * c->p.motionstep;
+      const uint32_t t_sdm_next = t_next < next_move ? t_next : next_move;
+      kokkos_shim::set_rng_time(t_sdm);
+      c->sdm->run_step(t_sdm, t_sdm_next, c->gbxs.view_device(), *c->allsupers);
+      t_sdm = t_sdm_next;
+    }
+  } catch (const kokkos_shim::Abort& e) {
+    fail(c, code_of(e.what()));
+  }
+  return c->err.code;
+}
+
+int ref_status(ref_ctx* c, cleo_b200_error* err) {
+  if (err) *err = c->err;
+  return c->err.code;
+}
+
+int ref_download_supers(ref_ctx* c, cleo_b200_supers* h, size_t* n_domain, size_t* n_total) {
+  const auto tot = c->allsupers->get_totsupers_readonly();
+  for (size_t k = 0; k < tot.extent(0); ++k) {
+    const Superdrop& d = tot(k);
+    h->sdgbxindex[k] = d.get_sdgbxindex();
+    h->coord3[k] = d.get_coord3();
+    h->coord1[k] = d.get_coord1();
+    h->coord2[k] = d.get_coord2();
+    h->xi[k] = d.get_xi();
+    h->radius[k] = d.get_radius();
+    h->msol[k] = d.get_msol();
+    if (h->sdid) h->sdid[k] = d.sdId.get_value();
+  }
+  if (n_domain) *n_domain = c->allsupers->domain_nsupers();
+  if (n_total) *n_total = tot.extent(0);
+  return CLEO_OK;
+}
+
+int ref_download_state(ref_ctx* c, cleo_b200_gbx_state* h) {
+  const auto hg = c->gbxs.view_host();
+  for (unsigned int ii = 0; ii < c->ngbxs; ++ii) {
+    const State& s = hg(ii).state;
+    h->volume[ii] = s.get_volume();
+    h->press[ii] = s.press;
+    h->temp[ii] = s.temp;
+    h->qvap[ii] = s.qvap;
+    h->qcond[ii] = s.qcond;
+    h->wvel_lo[ii] = s.wvel.first; h->wvel_hi[ii] = s.wvel.second;
+    h->uvel_lo[ii] = s.uvel.first; h->uvel_hi[ii] = s.uvel.second;
+    h->vvel_lo[ii] = s.vvel.first; h->vvel_hi[ii] = s.vvel.second;
+  }
+  return CLEO_OK;
+}
+
+int ref_download_budgets(ref_ctx* c, double* cond_mass, uint64_t* nr_iters) {
+  for (unsigned int ii = 0; ii < c->ngbxs; ++ii) {
+    if (cond_mass) cond_mass[ii] = c->cond_mass(ii);
+    if (nr_iters) nr_iters[ii] = 0; /* not observable in the reference */
+  }
+  return CLEO_OK;
+}
+
+/* ImplicitEuler::solve_condensation for independent droplets, set up like
+ * DoCondensation::superdroplets_change / superdrop_mass_change (condensation.cpp:43-112). */
+int ref_condensation_solve(const cleo_b200_params* p, size_t n, const double* radius,
+                           const double* msol, const double* temp, const double* press,
+                           const double* s_ratio, const double* delt, double* radius_out) {
+  int code = CLEO_OK;
+  for (size_t i = 0; i < n; ++i) {
+    try {
+      const ImplicitEuler impe(delt[i], p->maxniters, p->rtol, p->atol, p->cond_minsubdelt);
+      Superdrop drop(0u, 0.0, 0.0, 0.0,
+                     SuperdropAttrs(SoluteProperties{}, 1, radius[i], msol[i], true), IntID{i});
+      const auto psat = saturation_pressure(temp[i]);
+      const auto ffactor = diffusion_factor(press[i], temp[i], psat);
+      const auto ab = kohler_factors(drop, temp[i]);
+      const auto newr = impe.solve_condensation(s_ratio[i], ab, ffactor, drop.get_radius());
+      drop.change_radius(newr);
+      radius_out[i] = drop.get_radius();
+    } catch (const kokkos_shim::Abort& e) {
+      if (code == CLEO_OK) code = code_of(e.what());
+      radius_out[i] = NAN;
+    }
+  }
+  return code;
+}
+
+double ref_terminal_velocity(int kind, double radius) {
+  const Superdrop d(0u, 0.0, 0.0, 0.0, SuperdropAttrs(SoluteProperties{}, 1, radius, 0.0, true),
+                    IntID{0});
+  return AnyTV{kind}(d);
+}
+
+double ref_pair_probability(const cleo_b200_params* p, double r1, uint64_t xi1, double msol1,
+                            double r2, uint64_t xi2, double msol2, double volume) {
+  const Superdrop a(0u, 0.0, 0.0, 0.0, SuperdropAttrs(SoluteProperties{}, xi1, r1, msol1, true),
+                    IntID{0});
+  const Superdrop b(0u, 0.0, 0.0, 0.0, SuperdropAttrs(SoluteProperties{}, xi2, r2, msol2, true),
+                    IntID{1});
+  const AnyProb prob(p->coll_prob, p->coaleff, p->const_kernel);
+  return prob(a, b, p->coll_delt, volume * dlc::VOL0);
+}
+
+/* Neighbour maps as the reference builds them (doubly_periodic_domain.hpp:41-101 via
+ * createcartesianmaps.cpp:203-220) for a 3-D domain; used to pin the host-side grid builder. */
+void ref_cartesian_neighbours(const uint32_t ndims[3], uint32_t idx, uint32_t out[6]) {
+  const std::vector<size_t> nd{ndims[0], ndims[1], ndims[2]};
+  const auto z = DoublyPeriodicDomain::cartesian_coord3nghbrs(idx, nd);
+  const auto x = DoublyPeriodicDomain::cartesian_coord1nghbrs(idx, nd);
+  const auto y = DoublyPeriodicDomain::cartesian_coord2nghbrs(idx, nd);
+  out[0] = z.first; out[1] = z.second; out[2] = x.first;
+  out[3] = x.second; out[4] = y.first; out[5] = y.second;
+}
+
+}  // extern "C"

@@ -1,0 +1,172 @@
+"""Loading the CPU checkers and comparing domain states (test infrastructure).
+
+* the oracle: oracle/liboracle.so, the C restatement of the hot path (built by oracle/Makefile);
+* the reference build: oracle/_ref/libcleo_ref.so, CLEO's own sources compiled against the
+  Kokkos-API shim (present only where CLEO's sources were available to build it).
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from cleo_b200 import abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libcleo_ref.so")
+
+_oracle = None
+_ref = None
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True,
+                           capture_output=True)
+        lib = C.CDLL(ORACLE_SO)
+        abi.declare_api(lib, "oc")
+        P = C.POINTER(abi.Params)
+        d = C.POINTER(C.c_double)
+        lib.oc_condensation_solve.argtypes = [P, C.c_size_t] + [d] * 6 + [d, C.POINTER(C.c_uint32)]
+        lib.oc_condensation_solve.restype = C.c_int
+        lib.oc_condensation_solve_seeded.argtypes = ([P, C.c_size_t] + [d] * 7
+                                                     + [d, C.POINTER(C.c_uint32)])
+        lib.oc_condensation_solve_seeded.restype = C.c_int
+        lib.oc_rng_u64.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64]
+        lib.oc_rng_u64.restype = C.c_uint64
+        lib.oc_rng_drand.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64]
+        lib.oc_rng_drand.restype = C.c_double
+        lib.oc_rng_urand.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64,
+                                     C.c_uint64, C.c_uint64]
+        lib.oc_rng_urand.restype = C.c_uint64
+        lib.oc_terminal_velocity.argtypes = [C.c_int, C.c_double]
+        lib.oc_terminal_velocity.restype = C.c_double
+        lib.oc_pair_probability.argtypes = [P, C.c_double, C.c_uint64, C.c_double, C.c_double,
+                                            C.c_uint64, C.c_double, C.c_double]
+        lib.oc_pair_probability.restype = C.c_double
+        _oracle = lib
+    return _oracle
+
+
+def ref_available():
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        lib = C.CDLL(REF_SO)
+        abi.declare_api(lib, "ref")
+        P = C.POINTER(abi.Params)
+        d = C.POINTER(C.c_double)
+        lib.ref_set_num_threads.argtypes = [C.c_int]
+        lib.ref_set_num_threads.restype = None
+        lib.ref_condensation_solve.argtypes = [P, C.c_size_t] + [d] * 6 + [d]
+        lib.ref_condensation_solve.restype = C.c_int
+        lib.ref_terminal_velocity.argtypes = [C.c_int, C.c_double]
+        lib.ref_terminal_velocity.restype = C.c_double
+        lib.ref_pair_probability.argtypes = [P, C.c_double, C.c_uint64, C.c_double, C.c_double,
+                                             C.c_uint64, C.c_double, C.c_double]
+        lib.ref_pair_probability.restype = C.c_double
+        lib.ref_cartesian_neighbours.argtypes = [C.POINTER(C.c_uint32), C.c_uint32,
+                                                 C.POINTER(C.c_uint32)]
+        lib.ref_cartesian_neighbours.restype = None
+        _ref = lib
+    return _ref
+
+
+def dptr(a):
+    return abi.ptr(a, C.c_double)
+
+
+def condsolve(lib, prefix, params, w, seed_rsqrd=None):
+    n = len(w["radius"])
+    out = np.zeros(n)
+    arrs = [np.ascontiguousarray(w[k], dtype=np.float64)
+            for k in ("radius", "msol", "temp", "press", "s_ratio", "delt")]
+    if prefix == "ref":
+        rc = lib.ref_condensation_solve(C.byref(params), n, *[dptr(a) for a in arrs], dptr(out))
+        return rc, out, None
+    it = np.zeros(n, dtype=np.uint32)
+    if seed_rsqrd is None:
+        rc = lib.oc_condensation_solve(C.byref(params), n, *[dptr(a) for a in arrs], dptr(out),
+                                       abi.ptr(it, C.c_uint32))
+    else:
+        s = np.ascontiguousarray(seed_rsqrd, dtype=np.float64)
+        rc = lib.oc_condensation_solve_seeded(C.byref(params), n, *[dptr(a) for a in arrs],
+                                              dptr(s), dptr(out), abi.ptr(it, C.c_uint32))
+    return rc, out, it
+
+
+def assert_same_domain(a: dict, b: dict, rtol=1e-12, what=""):
+    """In-domain superdroplets: order, gridbox index, xi and id bit-identical; radius, msol and
+    coordinates within rtol (relative, FP64). Out-of-domain ones: the same set of ids."""
+    assert a["n_domain"] == b["n_domain"], (what, a["n_domain"], b["n_domain"])
+    assert a["n_total"] == b["n_total"], (what, a["n_total"], b["n_total"])
+    nd = a["n_domain"]
+    for k in ("sdid", "sdgbxindex", "xi"):
+        x, y = a[k][:nd], b[k][:nd]
+        bad = np.nonzero(x != y)[0]
+        assert bad.size == 0, (what, k, bad[:10], x[bad[:5]], y[bad[:5]])
+    for k in ("radius", "msol", "coord3", "coord1", "coord2"):
+        x, y = a[k][:nd], b[k][:nd]
+        scale = np.maximum(np.abs(x), np.abs(y))
+        err = np.abs(x - y)
+        ok = err <= rtol * scale + 1e-300
+        if k.startswith("coord"):
+            ok |= err <= 1e-15  # coordinates near zero
+        bad = np.nonzero(~ok)[0]
+        assert bad.size == 0, (what, k, bad[:10], x[bad[:5]], y[bad[:5]])
+    ia = np.sort(a["sdid"][nd:])
+    ib = np.sort(b["sdid"][nd:])
+    assert np.array_equal(ia, ib), (what, "oob ids differ")
+
+
+def max_rel(x, y):
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    s = np.maximum(np.abs(x), np.abs(y))
+    s[s == 0] = 1.0
+    return float(np.max(np.abs(x - y) / s)) if x.size else 0.0
+
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def params_from_bytes(b) -> abi.Params:
+    p = abi.Params()
+    C.memmove(C.byref(p), bytes(np.asarray(b, dtype=np.uint8)), C.sizeof(abi.Params))
+    return p
+
+
+def load_step_fixture(path):
+    """(workload dict, expected outputs dict) of a golden step fixture."""
+    z = np.load(path)
+    grid = {}
+    for k in z.files:
+        if k.startswith("grid_"):
+            v = z[k]
+            grid[k[5:]] = v.item() if v.ndim == 0 else v
+    grid["ndims"] = tuple(int(x) for x in grid["ndims"])
+    w = {
+        "grid": grid,
+        "state": {k[9:]: z[k] for k in z.files if k.startswith("in_state_")},
+        "supers": {k[6:]: z[k] for k in z.files if k.startswith("in_sd_")},
+        "params": params_from_bytes(z["params"]),
+        "tstep": int(z["tstep"]),
+    }
+    exp = {
+        "supers": {k[7:]: (z[k].item() if z[k].ndim == 0 else z[k])
+                   for k in z.files if k.startswith("out_sd_")},
+        "state": {k[10:]: z[k] for k in z.files if k.startswith("out_state_")},
+        "cond_mass": z["out_cond_mass"],
+        "nsteps": int(z["nsteps"]),
+    }
+    return w, exp
+
+
+def step_fixtures():
+    return sorted(f for f in os.listdir(GOLDEN) if f.startswith("step_") and f.endswith(".npz"))
