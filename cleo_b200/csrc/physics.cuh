@@ -1,0 +1,600 @@
+// physics.cuh — device implementations of CLEO's per-droplet and per-pair microphysics.
+//
+// Each function follows the reference function named beside it with the same floating-point
+// association (compiled with -fmad=false, so no contraction), so results match the reference up
+// to the difference between CUDA's and the host libm's pow/exp. Abort sites of the reference
+// record a status in the device error word instead of trapping.
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/cleo_b200.h"
+#include "../../include/cleo_b200_rng.h"
+
+namespace cleo {
+
+// ---- constants: libs/cleoconstants.hpp:32-118 ----
+constexpr double PI = 3.141592653589793238462643383279502884;
+constexpr double DC_RGAS_UNIV = 8.314462618;
+constexpr double DC_MR_WATER = 0.01801528;
+constexpr double DC_MR_DRY = 0.028966216;
+constexpr double DC_RGAS_DRY = DC_RGAS_UNIV / DC_MR_DRY;
+constexpr double DC_RGAS_V = DC_RGAS_UNIV / DC_MR_WATER;
+constexpr double DC_LATENT_V = 2500930.0;
+constexpr double DC_CP_DRY = 1004.64;
+constexpr double DC_CP_V = 1865.01;
+constexpr double DC_C_L = 4192.664;
+constexpr double DC_RHO_L = 998.203;
+constexpr double DC_RHO_SOL = 2016.5;
+constexpr double DC_MR_SOL = 0.05844277;
+constexpr double DC_SURFSIGMA = 7.28e-2;
+constexpr double W0 = 1.0;
+constexpr double TIME0 = 1000.0;
+constexpr double COORD0 = TIME0 * W0;
+constexpr double VOL0 = COORD0 * COORD0 * COORD0;
+constexpr double CP0 = DC_CP_DRY;
+constexpr double MR0 = DC_MR_DRY;
+constexpr double R0 = 1e-6;
+constexpr double P0 = 100000.0;
+constexpr double TEMP0 = 273.15;
+constexpr double RHO0 = P0 / (CP0 * TEMP0);
+constexpr double MASS0 = R0 * R0 * R0 * RHO0;
+constexpr double MASS0grams = MASS0 * 1000;
+constexpr double F0 = TIME0 / (RHO0 * R0 * R0);
+constexpr double Mr_ratio = DC_MR_WATER / DC_MR_DRY;
+constexpr double Cp_dry = DC_CP_DRY / CP0;
+constexpr double Cp_v = DC_CP_V / CP0;
+constexpr double C_l = DC_C_L / CP0;
+constexpr double Latent_v = DC_LATENT_V / (TEMP0 * CP0);
+constexpr double Rgas_dry = DC_RGAS_DRY / CP0;
+constexpr double Rgas_v = DC_RGAS_V / CP0;
+constexpr double Rho_l = DC_RHO_L / RHO0;
+constexpr double Rho_sol = DC_RHO_SOL / RHO0;
+constexpr double Mr_sol = DC_MR_SOL / MR0;
+constexpr double IONIC = 2.0;
+constexpr double surfconst = 4.0 * DC_SURFSIGMA * PI * R0 * R0;
+constexpr uint32_t OOB = 0xFFFFFFFFu;
+constexpr double DBLMAX = 1.7976931348623157e308;
+
+// ---- device error word ----
+struct DevError {
+  int32_t code;
+  uint32_t gbx;
+  unsigned long long index;
+};
+
+__device__ __forceinline__ void record_error(DevError* e, int code, uint32_t gbx, uint64_t index) {
+  if (atomicCAS(&e->code, 0, code) == 0) {
+    e->gbx = gbx;
+    e->index = index;
+  }
+}
+
+// context for error attribution of one droplet / pair
+struct Where {
+  DevError* err;
+  uint32_t gbx;
+  uint64_t index;
+  __device__ void fail(int code) const { record_error(err, code, gbx, index); }
+};
+
+// ---- SuperdropAttrs: superdrop_attrs.hpp:61-259, superdrop_attrs.cpp:34-62 ----
+__device__ __forceinline__ double dryradius(double msol) {  // :227-231
+  const double vconst = 3.0 / (4.0 * PI);
+  const double dryrcubed = vconst * msol / Rho_sol;
+  return pow(dryrcubed, 1.0 / 3.0);
+}
+__device__ __forceinline__ double rcubed(double r) { return r * r * r; }       // :238
+__device__ __forceinline__ double vol(double r) { return 4.0 / 3.0 * PI * rcubed(r); }  // :247
+__device__ __forceinline__ double sd_mass(double r, double msol) {  // superdrop_attrs.cpp:54-62
+  const double massconst = 4.0 / 3.0 * PI * Rho_l;
+  const double density_factor = 1.0 - Rho_l / Rho_sol;
+  double m = msol * density_factor;
+  m += massconst * rcubed(r);
+  return m;
+}
+__device__ __forceinline__ double condensate_mass(double r, double msol, const Where& w) {  // :208-218
+  double m_cond = sd_mass(r, msol) - msol;
+  if (m_cond <= -0.0001 * msol) w.fail(CLEO_ERR_NEG_CONDENSATE);
+  return fmax(0.0, m_cond);
+}
+// set_radius: superdrop_attrs.hpp:175-182 (the check; the caller stores)
+__device__ __forceinline__ void check_radius(double r, double msol, const Where& w) {
+  if (r - dryradius(msol) <= -1e-12 / R0) w.fail(CLEO_ERR_RADIUS_BELOW_DRY);
+}
+__device__ __forceinline__ void check_xi(uint64_t xi, const Where& w) {  // set_xi :156-163
+  if (xi <= 0) w.fail(CLEO_ERR_XI_ZERO);
+}
+
+// ---- terminal velocities: terminalvelocity.cpp:32-147 ----
+__device__ __forceinline__ double tv_simmel(double radius) {  // :57-85
+  const double r1 = 6.7215e-5 / R0;
+  const double r2 = 7.5582e-4 / R0;
+  const double r3 = 1.73892e-3 / R0;
+  const double VELCONST = (100.0 * W0);
+  const double a1 = 457950 / VELCONST;
+  const double a2 = 4962 / VELCONST;
+  const double a3 = 1732 / VELCONST;
+  const double a4 = 917 / VELCONST;
+  if (radius >= r3) return a4;
+  const double massconst = 4.0 / 3.0 * PI * Rho_l;  // watermass :32-40
+  const double MASS = (massconst * radius * radius * radius) * MASS0grams;
+  if (radius >= r2) return a3 * pow(MASS, 1.0 / 6.0);
+  if (radius >= r1) return a2 * pow(MASS, 1.0 / 3.0);
+  return a1 * pow(MASS, 2.0 / 3.0);
+}
+__device__ __forceinline__ double tv_rogersyau(double radius) {  // :95-117
+  const double r1 = 3e-5 / R0;
+  const double r2 = 6e-4 / R0;
+  const double r3 = 2e-3 / R0;
+  const double k1 = 1.19e8 * R0 * R0 / W0;
+  const double k2 = 8000 * R0 / W0;
+  const double k3 = 201 / W0;
+  const double k4 = 9 / W0;
+  if (radius < r1) return k1 * pow(radius, 2.0);
+  if (radius < r2) return k2 * radius;
+  if (radius < r3) return k3 * pow((radius * R0), 0.5);
+  return k4;
+}
+__device__ __forceinline__ double tv_rogersgk(double radius) {  // :127-147
+  const double radius0 = 3.725 * 1e-4 / R0;
+  const double kcaps = 2.0 * 4.0 * 1000 * R0 / W0;
+  const double smallk = -1.0 * 2.0 * 12.0 * 1000 * R0;
+  const double acaps = 9.65 / W0;
+  const double bcaps = 10.43 / W0;
+  const double ccaps = -1.0 * 2.0 * 0.6 * 1000 * R0;
+  if (radius < radius0) {
+    const double term = 1.0 - exp(smallk * radius);
+    return term * kcaps * radius;
+  }
+  return acaps - bcaps * exp(ccaps * radius);
+}
+__device__ __forceinline__ double terminalv(int kind, double radius) {
+  switch (kind) {
+    case CLEO_TV_SIMMEL: return tv_simmel(radius);
+    case CLEO_TV_ROGERSYAU: return tv_rogersyau(radius);
+    case CLEO_TV_ROGERSGK: return tv_rogersgk(radius);
+    default: return 0.0;
+  }
+}
+
+// ---- collision probabilities ----
+__device__ __forceinline__ double prob_golovin(double r1, double r2, double DELT, double VOLUME) {
+  const double prob_jk_const = 1.5e3 * R0 * R0 * R0;  // golovinprob.hpp:40
+  const double DELT_DELVOL = DELT / VOLUME;            // golovinprob.cpp:31-43
+  const double golovins_kernel = prob_jk_const * (vol(r1) + vol(r2));
+  return golovins_kernel * DELT_DELVOL;
+}
+__device__ __forceinline__ double long_kerneleff(double ra, double rb, double coaleff) {
+  const double k1 = 4.5e4 * R0 * R0 * 100 * 100;  // longhydroprob.cpp:29-48
+  const double k2 = 3e-4 / R0 / 100;
+  const double rlim = 5e-5 / R0;
+  const double colleff_min = 0.001;
+  const double rsmall = fmin(ra, rb);
+  const double rbig = fmax(ra, rb);
+  double colleff = 1.0;
+  if (rbig < rlim) {
+    colleff = k1 * rbig * rbig * (1 - (k2 / rsmall));
+    colleff = fmax(colleff, colleff_min);
+  }
+  return colleff * coaleff;
+}
+__device__ __forceinline__ double prob_hydrodynamic(double r1, double r2, double eff, double DELT,
+                                                    double VOLUME) {  // hydrodynamicprob.hpp:49-66
+  const double prob_jk_const = PI * R0 * R0 * W0;
+  const double DELT_DELVOL = DELT / VOLUME;
+  const double sumr = r1 + r2;
+  const double sumrsqrd = sumr * sumr;
+  const double vdiff = fabs(tv_simmel(r1) - tv_simmel(r2));
+  const double hydro_kernel = prob_jk_const * eff * sumrsqrd * vdiff;
+  return hydro_kernel * DELT_DELVOL;
+}
+__device__ __forceinline__ double pair_prob(const cleo_b200_params& p, double r1, double r2,
+                                            double VOLUME) {
+  switch (p.coll_prob) {
+    case CLEO_PROB_GOLOVIN: return prob_golovin(r1, r2, p.coll_delt, VOLUME);
+    case CLEO_PROB_LONG:
+      return prob_hydrodynamic(r1, r2, long_kerneleff(r1, r2, p.coaleff), p.coll_delt, VOLUME);
+    default: return p.const_kernel * p.coll_delt / VOLUME;  // constprob.hpp:44-48
+  }
+}
+
+// ---- collision kinetics: collisionkinetics.cpp:31-67, coalescence_efficiency.cpp:27-38 ----
+__device__ __forceinline__ double collision_kinetic_energy(double r1, double r2, double tv1,
+                                                          double tv2) {
+  const double R0cubed = R0 * R0 * R0;
+  const double ckeconst = R0cubed * 2.0 / 3.0 * DC_RHO_L * PI * W0 * W0;
+  const double r1cubed = r1 * r1 * r1;
+  const double r1_r2cubed = (r1 / r2) * (r1 / r2) * (r1 / r2);
+  const double rratio = r1cubed / (1 + r1_r2cubed);
+  const double vdiff = tv1 - tv2;
+  return ckeconst * rratio * vdiff * vdiff;
+}
+__device__ __forceinline__ double coal_surfenergy(double r1, double r2) {
+  const double r1cubed = r1 * r1 * r1;
+  const double r2cubed = r2 * r2 * r2;
+  const double rcubedsum = r1cubed + r2cubed;
+  return surfconst * pow(rcubedsum, 2.0 / 3.0);
+}
+__device__ __forceinline__ double surfenergy(double radius) { return surfconst * (radius * radius); }
+__device__ __forceinline__ double ecoal_straub2010(double r1, double r2, double cke) {
+  const double beta = -1.15;
+  const double surf_c = coal_surfenergy(r1, r2);
+  const double weber = cke / surf_c;
+  return exp(beta * weber);
+}
+__device__ __forceinline__ double nfrags_of(const cleo_b200_params& p, double r1, double r2) {
+  if (p.nfrags_kind == CLEO_NFRAGS_CONST) return p.nfrags;  // breakup_nfrags.hpp:40-50
+  const double alpha = 1.5;                                   // :54-92
+  const double beta = 0.135;
+  const double ckemax = 16.49789599 / 1000000;
+  const double epsilon = 11.0 / 6.0;
+  const double cke = collision_kinetic_energy(r1, r2, terminalv(p.nfrags_tv, r1),
+                                              terminalv(p.nfrags_tv, r2));
+  const double cke_cap = fmin(ckemax, cke);
+  const double gamma = pow(cke_cap * 1e6, beta);
+  return 1.0 / (alpha - gamma) + epsilon;
+}
+__device__ __forceinline__ unsigned coalbure_flag(const cleo_b200_params& p, double phi, double r1,
+                                                  double r2) {  // coalbure_flag.hpp:42-198
+  switch (p.flag_kind) {
+    case CLEO_FLAG_STRAUB: {
+      const double cke = collision_kinetic_energy(r1, r2, terminalv(p.flag_tv, r1),
+                                                  terminalv(p.flag_tv, r2));
+      return (phi < ecoal_straub2010(r1, r2, cke)) ? 1u : 2u;
+    }
+    case CLEO_FLAG_TESTIKSTRAUB: {
+      const double cke = collision_kinetic_energy(r1, r2, terminalv(p.flag_tv, r1),
+                                                  terminalv(p.flag_tv, r2));
+      if (cke < surfenergy(fmin(r1, r2))) return (phi < ecoal_straub2010(r1, r2, cke)) ? 1u : 0u;
+      if (cke < surfenergy(fmax(r1, r2))) return (phi < ecoal_straub2010(r1, r2, cke)) ? 1u : 2u;
+      return 2u;
+    }
+    case CLEO_FLAG_SZAKALLURBICH: {
+      const double cke = collision_kinetic_energy(r1, r2, terminalv(p.flag_tv, r1),
+                                                  terminalv(p.flag_tv, r2));
+      if (cke < surfenergy(fmin(r1, r2))) return 0u;
+      if (cke < coal_surfenergy(r1, r2)) return 1u;
+      return 2u;
+    }
+    default: return (phi < p.flag_coaleff) ? 1u : 2u;
+  }
+}
+
+// one superdroplet's attributes while it takes part in a collision
+struct Drop {
+  uint64_t xi;
+  double r, msol;
+};
+
+// ---- coalescence: coalescence.cpp:39-196 ----
+__device__ __forceinline__ uint64_t coalescence_gamma(uint64_t xi1, uint64_t xi2, double prob,
+                                                      double phi) {  // :68-79
+  uint64_t gamma = (uint64_t)floor(prob);
+  if (phi < (prob - (double)gamma)) ++gamma;
+  const uint64_t maxgamma = xi1 / xi2;
+  return (uint64_t)fmin((double)gamma, (double)maxgamma);
+}
+__device__ __forceinline__ void twin_coalescence(uint64_t gamma, Drop& d1, Drop& d2,
+                                                 const Where& w) {  // :131-162
+  if (d1.xi != gamma * d2.xi) w.fail(CLEO_ERR_COALESCENCE);
+  const uint64_t old_xi = d2.xi;
+  const uint64_t new_xi = old_xi / 2;
+  if (new_xi >= old_xi) w.fail(CLEO_ERR_COALESCENCE);
+  const double new_rcubed = rcubed(d2.r) + (double)gamma * rcubed(d1.r);
+  const double new_r = pow(new_rcubed, (1.0 / 3.0));
+  const double new_msol = d2.msol + (double)gamma * d1.msol;
+  if (new_xi == 0) {
+    d1.xi = 0;  // set_null
+  } else {
+    check_xi(new_xi, w);
+    d1.xi = new_xi;
+  }
+  check_xi(old_xi - new_xi, w);
+  d2.xi = old_xi - new_xi;
+  check_radius(new_r, d1.msol, w);
+  d1.r = new_r;
+  check_radius(new_r, d2.msol, w);
+  d2.r = new_r;
+  d1.msol = new_msol;
+  d2.msol = new_msol;
+}
+__device__ __forceinline__ void different_coalescence(uint64_t gamma, Drop& d1, Drop& d2,
+                                                      const Where& w) {  // :177-196
+  if (d1.xi <= gamma * d2.xi) w.fail(CLEO_ERR_COALESCENCE);
+  const uint64_t new_xi = d1.xi - gamma * d2.xi;
+  if (new_xi >= d1.xi) w.fail(CLEO_ERR_COALESCENCE);
+  check_xi(new_xi, w);
+  d1.xi = new_xi;
+  const double new_rcubed = rcubed(d2.r) + (double)gamma * rcubed(d1.r);
+  const double nr = pow(new_rcubed, (1.0 / 3.0));
+  check_radius(nr, d2.msol, w);
+  d2.r = nr;
+  d2.msol = d2.msol + (double)gamma * d1.msol;
+}
+__device__ __forceinline__ uint32_t coalesce_pair(uint64_t gamma, Drop& d1, Drop& d2,
+                                                  const Where& w) {  // :92-113
+  const uint64_t xi1 = d1.xi, xi2 = d2.xi;
+  if (xi1 - gamma * xi2 > 0) {
+    different_coalescence(gamma, d1, d2, w);
+    return 0;
+  } else if (xi1 - gamma * xi2 == 0) {
+    twin_coalescence(gamma, d1, d2, w);
+    return d1.xi == 0 ? 1u : 0u;
+  }
+  return 0;
+}
+
+// ---- breakup: breakup.hpp:140-268 ----
+__device__ __forceinline__ void twin_breakup(const cleo_b200_params& p, Drop& d1, Drop& d2,
+                                             const Where& w) {  // :193-228
+  const uint64_t old_xi = d2.xi;
+  const double totnfrags = nfrags_of(p, d1.r, d2.r) * (double)old_xi;
+  if ((totnfrags / (double)old_xi) <= 2.5) w.fail(CLEO_ERR_BREAKUP);
+  const uint64_t new_xi1 = (uint64_t)round(totnfrags / 2);
+  const uint64_t new_xi2 = (uint64_t)round(totnfrags - (double)new_xi1);
+  const uint64_t new_xitot = new_xi1 + new_xi2;
+  if (new_xi2 <= old_xi) w.fail(CLEO_ERR_BREAKUP);
+  if (new_xitot <= (old_xi * 2)) w.fail(CLEO_ERR_BREAKUP);
+  const double sum_rcubed = rcubed(d1.r) + rcubed(d2.r);
+  const double new_rcubed = sum_rcubed * (double)old_xi / (double)new_xitot;
+  const double new_r = pow(new_rcubed, (1.0 / 3.0));
+  const double sum_msol = d1.msol + d2.msol;
+  const double new_msol = sum_msol * (double)old_xi / (double)new_xitot;
+  check_xi(new_xi1, w);
+  d1.xi = new_xi1;
+  check_xi(new_xi2, w);
+  d2.xi = new_xi2;
+  check_radius(new_r, d1.msol, w);
+  d1.r = new_r;
+  check_radius(new_r, d2.msol, w);
+  d2.r = new_r;
+  d1.msol = new_msol;
+  d2.msol = new_msol;
+}
+__device__ __forceinline__ void different_breakup(const cleo_b200_params& p, Drop& d1, Drop& d2,
+                                                  const Where& w) {  // :235-268
+  const uint64_t old_xi1 = d1.xi;
+  const uint64_t old_xi2 = d2.xi;
+  const uint64_t new_xi1 = old_xi1 - old_xi2;
+  check_xi(new_xi1, w);
+  d1.xi = new_xi1;
+  const double totnfrags = nfrags_of(p, d1.r, d2.r) * (double)old_xi2;
+  const uint64_t new_xi2 = (uint64_t)round(totnfrags);
+  if ((totnfrags / (double)old_xi2) <= 2.5) w.fail(CLEO_ERR_BREAKUP);
+  if (new_xi2 <= old_xi2) w.fail(CLEO_ERR_BREAKUP);
+  if ((new_xi1 + new_xi2) <= (old_xi1 + old_xi2)) w.fail(CLEO_ERR_BREAKUP);
+  const double sum_rcubed = rcubed(d1.r) + rcubed(d2.r);
+  const double new_rcubed = sum_rcubed * (double)old_xi2 / (double)new_xi2;
+  const double new_r = pow(new_rcubed, (1.0 / 3.0));
+  const double sum_msol = d1.msol + d2.msol;
+  const double new_msol = sum_msol * (double)old_xi2 / (double)new_xi2;
+  check_xi(new_xi2, w);
+  d2.xi = new_xi2;
+  check_radius(new_r, d2.msol, w);
+  d2.r = new_r;
+  d2.msol = new_msol;
+}
+__device__ __forceinline__ uint32_t breakup_pair(const cleo_b200_params& p, Drop& d1, Drop& d2,
+                                                 const Where& w) {  // :176-186
+  if (d1.xi == d2.xi) {
+    twin_breakup(p, d1, d2, w);
+  } else {
+    different_breakup(p, d1, d2, w);
+  }
+  return 0;
+}
+
+// Enact the collision of a pair (already ordered so that d1.xi >= d2.xi): returns the number of
+// superdroplets made null. coalescence.cpp:39-54, breakup.hpp:140-166, coalbure.hpp:207-256.
+__device__ __forceinline__ uint32_t enact_collision(const cleo_b200_params& p, Drop& d1, Drop& d2,
+                                                   double prob, double phi_coll, double phi_out,
+                                                   const Where& w) {
+  if (p.coll_enact == CLEO_ENACT_COALESCENCE) {
+    const uint64_t gamma = coalescence_gamma(d1.xi, d2.xi, prob, phi_coll);
+    if (gamma != 0) return coalesce_pair(gamma, d1, d2, w);
+    return 0;
+  }
+  if (p.coll_enact == CLEO_ENACT_BREAKUP) {
+    if (phi_coll < (prob - floor(prob))) return breakup_pair(p, d1, d2, w);
+    return 0;
+  }
+  const uint64_t gamma = coalescence_gamma(d1.xi, d2.xi, prob, phi_coll);
+  if (gamma != 0) {
+    const unsigned flag = coalbure_flag(p, phi_out, d1.r, d2.r);
+    if (flag == 1u) return coalesce_pair(gamma, d1, d2, w);
+    if (flag == 2u) return breakup_pair(p, d1, d2, w);
+  }
+  return 0;
+}
+
+// ---- thermodynamic equations: thermodynamic_equations.{hpp:44-107, cpp:38-145} ----
+__device__ __forceinline__ double dry_air_density(double press, double temp, double qvap) {
+  const double rgas_equiv = Rgas_dry + Rgas_v * qvap;
+  return press / (rgas_equiv * temp);
+}
+__device__ __forceinline__ double moist_specifc_heat(double qvap, double qcond) {
+  return Cp_dry + Cp_v * (qvap) + C_l * (qcond);
+}
+__device__ __forceinline__ double supersaturation_ratio(double press, double qvap, double psat) {
+  return (press * qvap) / ((Mr_ratio + qvap) * psat);
+}
+__device__ __forceinline__ double saturation_pressure(double temp, const Where& w) {
+  if (temp <= 0) w.fail(CLEO_ERR_TEMPERATURE);
+  const double A = 17.4146;
+  const double B = 33.639;
+  const double TREF = 273.16;
+  const double PREF = 611.655;
+  const double T = temp * TEMP0;
+  return (PREF * exp(A * (T - TREF) / (T - B))) / P0;
+}
+__device__ __forceinline__ double diffusion_factor(double press, double temp, double psat) {
+  const double A = 7.11756e-5;
+  const double B = 4.38127686e-3;
+  const double LATENT_RGAS_V = DC_LATENT_V / DC_RGAS_V;
+  const double D = 4.012182971e-5;
+  const double TEMP = temp * TEMP0;
+  const double PRESS = press * P0;
+  const double PSAT = psat * P0;
+  const double THERMK = A * pow(TEMP, 2.0) + TEMP * B;
+  const double DIFFUSE_V = (D / PRESS * pow(TEMP, 1.94)) / DC_RGAS_V;
+  const double fkl = (LATENT_RGAS_V / TEMP - 1.0) * DC_LATENT_V / (THERMK * F0);
+  const double fdl = TEMP / (DIFFUSE_V * PSAT) / F0;
+  return Rho_l * (fkl + fdl);
+}
+__device__ __forceinline__ double ventilation_factor(double radius) {
+  const double vent_factor_max = 20;
+  const double C1 = 6.954e+7;
+  const double A = 1.963;
+  const double C2 = 1.069e+3;
+  const double B = 0.702;
+  const double a = 1.0 / (C1 * pow(radius * R0, A));
+  const double b = 1.0 / (C2 * pow(radius * R0, B));
+  const double vent_factor = 1.0 + 1.0 / (a + b);
+  return fmin(vent_factor, vent_factor_max);
+}
+__device__ __forceinline__ void kohler_factors(double msol, double temp, double& akoh,
+                                               double& bkoh) {
+  const double akoh_constant = 3.3e-7 / (TEMP0 * R0);
+  akoh = akoh_constant / temp;
+  const double bkoh_constant = 4.3e-6 * RHO0 / MR0;
+  bkoh = bkoh_constant * msol * IONIC / Mr_sol;
+}
+
+// ---- ImplicitEuler: impliciteuler.{hpp:41-345, cpp:35-301} ----
+struct OdeConsts {
+  double s_ratio, akoh, bkoh, ffactor_fv;
+};
+struct NewtonCfg {
+  uint32_t maxniters;
+  double rtol, atol;
+};
+// Upper bound on the Newton iterations of one solve (all sub-steps). Legitimate solves need at
+// most (delt / minsubdelt) * (2 + maxniters); this bound only stops a runaway solve, reported as
+// CLEO_ERR_TIMEOUT, so that no thread can spin for long.
+constexpr uint32_t NR_ITER_CAP = 4u << 20;
+
+__device__ __forceinline__ double ode_gfunc(const OdeConsts& o, double subdelt, double rprev,
+                                            double rsqrd) {  // :270-281
+  const double radius = sqrt(rsqrd);
+  const double alpha = o.s_ratio - 1 - o.akoh / radius + o.bkoh / pow(radius, 3.0);
+  const double beta = 2.0 * subdelt / (rsqrd * o.ffactor_fv);
+  const double gamma = pow(rprev / radius, 2.0);
+  return 1 - gamma - alpha * beta;
+}
+__device__ __forceinline__ double ode_gfuncderivative(const OdeConsts& o, double subdelt,
+                                                      double rsqrd) {  // :291-301
+  const double radius = sqrt(rsqrd);
+  const double alpha = o.akoh / radius - 3.0 * o.bkoh / pow(radius, 3.0);
+  const double beta = subdelt / (rsqrd * o.ffactor_fv);
+  return 1 - alpha * beta;
+}
+// iterate_rootfinding_algorithm: impliciteuler.cpp:239-255 (+ check_for_convergence, hpp:213-219)
+__device__ __forceinline__ double nr_iterate(const NewtonCfg& c, const OdeConsts& o,
+                                             double subdelt, double rprev, double ziter,
+                                             bool& converged, uint32_t& niters) {
+  const double numerator = ode_gfunc(o, subdelt, rprev, ziter);
+  const double denominator = ode_gfuncderivative(o, subdelt, ziter);
+  ziter = ziter * (1 - numerator / denominator);
+  ziter = fmax(ziter, 1e-8);
+  const double newnumerator = ode_gfunc(o, subdelt, rprev, ziter);
+  const double conv = c.rtol * fabs(newnumerator) + c.atol;
+  converged = fabs(newnumerator - numerator) < conv;
+  ++niters;
+  return ziter;
+}
+// integrate_condensation_ode: impliciteuler.cpp:128-141 with newtonraphson_niterations (:181-194)
+// and newtonraphson_untilconverged (:207-227)
+__device__ __forceinline__ double integrate_ode(const NewtonCfg& c, const OdeConsts& o,
+                                                double subdelt, double rprev, double ziter,
+                                                uint32_t& niters, const Where& w) {
+  bool conv = false;
+  double z = ziter;
+  for (int it = 0; it < 2; ++it) z = nr_iterate(c, o, subdelt, rprev, z, conv, niters);
+  if (conv) return z;
+  z = ziter;
+  conv = false;
+  uint32_t niter = 1;
+  while (!conv) {
+    if (niter > c.maxniters) {
+      w.fail(CLEO_ERR_NR_NOCONVERGE);
+      break;
+    }
+    if (niters >= NR_ITER_CAP) {
+      w.fail(CLEO_ERR_TIMEOUT);
+      break;
+    }
+    z = nr_iterate(c, o, subdelt, rprev, z, conv, niters);
+    niter += 1;
+  }
+  return z;
+}
+__device__ __forceinline__ double initialguess(const OdeConsts& o, double rprev) {  // :156-170
+  const double s_act = 1 + sqrt(4.0 * pow(o.akoh, 3.0) / 27 / o.bkoh);
+  if (o.s_ratio > s_act) {
+    const double bigr = 1e-3 / R0;
+    const double maxradius = fmax(bigr, rprev);
+    return maxradius * maxradius;
+  }
+  return rprev * rprev;
+}
+__device__ __forceinline__ bool first_unique_criteria(const OdeConsts& o, double rprev,
+                                                      double ziter) {  // :69-83
+  const double akoh = o.akoh;
+  const double bkoh = o.bkoh;
+  const double rcritsqrd = 3.0 * bkoh / akoh;
+  const bool is_ziter_unactivated = ziter < rcritsqrd;
+  const bool is_unactivated = (rprev * rprev < rcritsqrd && is_ziter_unactivated);
+  const double sqrdval = 4.0 * akoh * akoh * akoh / 27.0 / bkoh;
+  const bool is_subactivated_saturation = (o.s_ratio <= 1.0 + pow(sqrdval, 0.5));
+  return (is_unactivated && is_subactivated_saturation);
+}
+__device__ __forceinline__ double critical_timestep(const OdeConsts& o) {  // hpp:266-269
+  const double cuberoot = pow(5.0 * o.bkoh / o.akoh, 1.5);
+  return 2.5 * o.ffactor_fv / o.akoh * cuberoot;
+}
+// solve_condensation: impliciteuler.cpp:35-54 (+ substepping :98-113). seed_rsqrd > 0 replaces
+// the Newton start (not the branch decision) by a predicted r^2.
+__device__ __forceinline__ double solve_condensation(const NewtonCfg& c, double delt,
+                                                     double minsubdelt, double s_ratio,
+                                                     double akoh, double bkoh, double ffactor,
+                                                     double rprev, double seed_rsqrd,
+                                                     uint32_t& niters, const Where& w) {
+  const double ffactor_fv = ffactor / ventilation_factor(rprev);
+  const OdeConsts o{s_ratio, akoh, bkoh, ffactor_fv};
+  double ziter = initialguess(o, rprev);
+  const bool ucrit1 = first_unique_criteria(o, rprev, ziter);
+  const bool ucrit2 = (delt <= critical_timestep(o));
+  double rsqrd;
+  if (ucrit1 || ucrit2) {
+    if (seed_rsqrd > 0.0) ziter = seed_rsqrd;
+    rsqrd = integrate_ode(c, o, delt, rprev, ziter, niters, w);
+  } else {
+    const double critdelt = critical_timestep(o);
+    const double mindelt = fmax(critdelt, minsubdelt);
+    double remdelt = delt;
+    while (remdelt > 0.0) {
+      if (niters >= NR_ITER_CAP) {
+        w.fail(CLEO_ERR_TIMEOUT);
+        break;
+      }
+      const double subdelt = fmin(mindelt, remdelt);
+      ziter = integrate_ode(c, o, subdelt, rprev, ziter, niters, w);
+      rprev = pow(ziter, 0.5);
+      remdelt -= subdelt;
+    }
+    rsqrd = ziter;
+  }
+  return sqrt(rsqrd);
+}
+
+// ---- scheduling: microphysicalprocess.hpp:222-248 ----
+__host__ __device__ __forceinline__ bool on_step(uint32_t interval, uint32_t t) {
+  return (t % interval == 0) && (interval != CLEO_STEP_OFF);
+}
+__host__ __device__ __forceinline__ uint32_t next_step(uint32_t interval, uint32_t t) {
+  if (interval == CLEO_STEP_OFF) return CLEO_STEP_OFF;
+  return ((t / interval) + 1) * interval;
+}
+
+}  // namespace cleo

@@ -1,0 +1,958 @@
+// sdm.cu — the B200 SDM step behind the C ABI of include/cleo_b200.h.
+//
+// Device layout: structure-of-arrays superdroplets (sdgbxindex u32, coord3/1/2 f64, xi u64,
+// radius f64, msol f64, sdid u64), double-buffered for the sort, with the in-domain superdroplets
+// sorted by gridbox in [0, nrange); per gridbox g the superdroplets [gstart[g], gstart[g] +
+// gcount[g]) are the ones SupersInGbx refs would select. Superdroplets that leave the domain or
+// become null are appended to a separate out-of-domain store (the reference keeps them at the tail
+// of its array in unspecified order). Null superdroplets made by collisions stay in their
+// gridbox's range, after the gcount valid ones, until the next sort (the reference re-sorts at
+// once, sdmmethods.hpp:221-229; both give the same in-domain superdroplets in the same order).
+//
+// One SDM step (SDMMethods::run_step, sdmmethods.hpp:319-332):
+//   motion  -> k_motion: predictor-corrector coords + new gridbox index + sort key per droplet
+//   sort    -> radix passes over (key, position), gather of all fields, gridbox refs by binary
+//              search, append of out-of-domain droplets to the store
+//   microphysics -> k_micro: one CTA per gridbox: qcond from the moved droplets, condensation
+//              (FP64 Newton) and collisions (shared-memory shuffle, parallel pairs, null removal)
+//              for every sub-step of the SDM step.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "physics.cuh"
+#include "sort.cuh"
+
+using namespace cleo;
+
+namespace {
+
+constexpr int MICRO_THREADS = 256;
+constexpr uint32_t NSMEM = 1024;  // gridboxes up to this size are staged in shared memory
+constexpr size_t MICRO_SMEM = (size_t)NSMEM * (8 + 8 + 8 + 4 + 4);
+
+struct Fields {  // one SoA buffer
+  uint32_t* gbx;
+  double *c3, *c1, *c2;
+  unsigned long long* xi;
+  double *r, *msol;
+  unsigned long long* id;
+};
+
+struct DevCtx {
+  cleo_b200_params p;
+  uint32_t ngbxs;
+  uint32_t ndims[3];
+  uint32_t capacity;
+  // maps
+  const double *b3lo, *b3hi, *b1lo, *b1hi, *b2lo, *b2hi;
+  const uint32_t *back3, *fwd3, *back1, *fwd1, *back2, *fwd2;
+  // states
+  double *volume, *press, *temp, *qvap, *qcond, *wlo, *whi, *ulo, *uhi, *vlo, *vhi;
+  double* cond_mass;
+  unsigned long long* nr_iters;
+  // superdroplets (current buffer) and the out-of-domain store
+  Fields sd;
+  Fields grave;
+  uint32_t* gstart;  // ngbxs + 2
+  uint32_t* gcount;  // ngbxs
+  uint32_t* counters;  // [0] nrange, [1] ndomain, [2] ngrave
+  // scratch
+  double *scr_r, *scr_m, *scr_c3, *scr_c1, *scr_c2;
+  unsigned long long *scr_x, *scr_id;
+  uint32_t *scr_p, *scr_j;
+  DevError* err;
+};
+
+}  // namespace
+
+struct cleo_b200_ctx {
+  DevCtx d;
+  Fields buf[2];
+  int cur = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int device = 0;
+  // sort scratch
+  uint32_t *keys[2], *vals[2], *hist, *tile_sums;
+  uint32_t ntiles_max, key_bits;
+  std::vector<void*> allocs;
+};
+
+#define CUDA_TRY(expr)                                          \
+  do {                                                          \
+    cudaError_t e_ = (expr);                                    \
+    if (e_ != cudaSuccess) {                                    \
+      fprintf(stderr, "cleo_b200: %s failed: %s\n", #expr, cudaGetErrorString(e_)); \
+      return CLEO_ERR_CUDA;                                     \
+    }                                                           \
+  } while (0)
+
+// ------------------------------------------------------------------------------------------
+// kernels
+// ------------------------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ void bounds_of(const double* lo, const double* hi, uint32_t ngbxs,
+                                          uint32_t i, double& l, double& h) {
+  if (i < ngbxs) {
+    l = lo[i];
+    h = hi[i];
+  } else {  // oob key: nullbounds (createcartesianmaps.cpp:40)
+    l = -DBLMAX;
+    h = DBLMAX;
+  }
+}
+
+// interpolation: predcorr.cpp:30-42
+__device__ __forceinline__ double interpolation(double blo, double bhi, double vlo, double vhi,
+                                                double sdcoord) {
+  const double coord = fmin(bhi, fmax(blo, sdcoord));
+  const double alpha = (coord - blo) / (bhi - blo);
+  return alpha * vhi + (1 - alpha) * vlo;
+}
+
+__device__ __forceinline__ int flag_sdgbxindex(uint32_t idx, uint32_t ngbxs, double blo,
+                                               double bhi, double coord) {
+  if (idx == OOB || idx >= ngbxs) return 0;  // cartesianmaps.cpp:93-107
+  if (coord < blo) return 1;
+  if (coord >= bhi) return 2;
+  return 0;
+}
+
+__device__ __forceinline__ bool beyond_domainboundary(uint32_t gbxindex, uint32_t increment,
+                                                      uint32_t ndim) {
+  return (gbxindex / increment) % ndim == 0;  // domainboundaries.hpp:34-37
+}
+
+// k_motion: MoveSupersInGridboxesFunctor (movesupersindomain.hpp:47-93) for every droplet:
+// PredCorr::operator() (predcorr.hpp:156-171), cfl_criteria, PredCorrMotion::superdrop_gbx
+// (predcorrmotion.hpp:85-106) with get_no_decomposition_bounding_gridbox (cartesianmaps.cpp:278)
+// and CartesianCheckBounds. Writes the sort key min(gbx, ngbxs) and the position.
+__global__ void k_motion(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const uint32_t n = c.counters[0];
+  const uint32_t ng = c.ngbxs;
+  const double delt = c.p.motion_delt;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t g = c.sd.gbx[i];
+    vals[i] = i;
+    if (g >= ng) {  // null superdroplet left by collisions: out of the domain
+      keys[i] = ng;
+      continue;
+    }
+    const Where w{c.err, g, i};
+    double bzl, bzh, bxl, bxh, byl, byh;
+    bounds_of(c.b3lo, c.b3hi, ng, g, bzl, bzh);
+    bounds_of(c.b1lo, c.b1hi, ng, g, bxl, bxh);
+    bounds_of(c.b2lo, c.b2hi, ng, g, byl, byh);
+    const double wl = c.wlo[g], wh = c.whi[g], ul = c.ulo[g], uh = c.uhi[g], vl = c.vlo[g],
+                 vh = c.vhi[g];
+    const double c3 = c.sd.c3[i], c1 = c.sd.c1[i], c2 = c.sd.c2[i];
+    // delta_coord3: predcorr.hpp:83-105
+    double coord3 = c3;
+    const double terminal = terminalv(c.p.motion_tv, c.sd.r[i]);
+    double vel3 = interpolation(bzl, bzh, wl, wh, coord3);
+    vel3 -= terminal;
+    coord3 += vel3 * delt;
+    double corrvel3 = interpolation(bzl, bzh, wl, wh, coord3);
+    corrvel3 -= terminal;
+    const double delta3 = (vel3 + corrvel3) * (delt / 2);
+    // delta_coord1: predcorr.hpp:107-125
+    double coord1 = c1;
+    const double vel1 = interpolation(bxl, bxh, ul, uh, coord1);
+    coord1 += vel1 * delt;
+    const double corrvel1 = interpolation(bxl, bxh, ul, uh, coord1);
+    const double delta1 = (vel1 + corrvel1) * (delt / 2);
+    // delta_coord2: predcorr.hpp:127-145
+    double coord2 = c2;
+    const double vel2 = interpolation(byl, byh, vl, vh, coord2);
+    coord2 += vel2 * delt;
+    const double corrvel2 = interpolation(byl, byh, vl, vh, coord2);
+    const double delta2 = (vel2 + corrvel2) * (delt / 2);
+    // cfl_criteria: cfl_criteria.hpp:30-57
+    bool cfl = (fabs(delta3) <= fabs(bzh - bzl));
+    cfl = (fabs(delta1) <= fabs(bxh - bxl)) && cfl;
+    cfl = (fabs(delta2) <= fabs(byh - byl)) && cfl;
+    if (!cfl) w.fail(CLEO_ERR_CFL);
+    double n3 = c3 + delta3, n1 = c1 + delta1, n2 = c2 + delta2;
+    // change_if_coord3nghbr: finite z, coordinate unchanged at the edge (cartesianmaps.cpp:184-213)
+    uint32_t idx = g;
+    int flag = flag_sdgbxindex(idx, ng, bzl, bzh, n3);
+    if (flag == 1) idx = c.back3[idx];
+    else if (flag == 2) idx = c.fwd3[idx];
+    // change_if_coord1nghbr: periodic x (cartesianmaps.cpp:148-179)
+    {
+      double l, h;
+      bounds_of(c.b1lo, c.b1hi, ng, idx, l, h);
+      flag = flag_sdgbxindex(idx, ng, l, h, n1);
+      const uint32_t incre = c.ndims[0];
+      if (flag == 1) {
+        const uint32_t nghbr = c.back1[idx];
+        if (beyond_domainboundary(idx, incre, c.ndims[1])) {
+          double nl, nh;
+          bounds_of(c.b1lo, c.b1hi, ng, nghbr, nl, nh);
+          n1 = n1 + nh - l;
+        }
+        idx = nghbr;
+      } else if (flag == 2) {
+        const uint32_t nghbr = c.fwd1[idx];
+        if (beyond_domainboundary(idx + incre, incre, c.ndims[1])) {
+          double nl, nh;
+          bounds_of(c.b1lo, c.b1hi, ng, nghbr, nl, nh);
+          n1 = n1 + nl - h;
+        }
+        idx = nghbr;
+      }
+    }
+    // change_if_coord2nghbr: periodic y (cartesianmaps.cpp:112-143)
+    {
+      double l, h;
+      bounds_of(c.b2lo, c.b2hi, ng, idx, l, h);
+      flag = flag_sdgbxindex(idx, ng, l, h, n2);
+      const uint32_t incre = c.ndims[0] * c.ndims[1];
+      if (flag == 1) {
+        const uint32_t nghbr = c.back2[idx];
+        if (beyond_domainboundary(idx, incre, c.ndims[2])) {
+          double nl, nh;
+          bounds_of(c.b2lo, c.b2hi, ng, nghbr, nl, nh);
+          n2 = n2 + nh - l;
+        }
+        idx = nghbr;
+      } else if (flag == 2) {
+        const uint32_t nghbr = c.fwd2[idx];
+        if (beyond_domainboundary(idx + incre, incre, c.ndims[2])) {
+          double nl, nh;
+          bounds_of(c.b2lo, c.b2hi, ng, nghbr, nl, nh);
+          n2 = n2 + nl - h;
+        }
+        idx = nghbr;
+      }
+    }
+    c.sd.c3[i] = n3;
+    c.sd.c1[i] = n1;
+    c.sd.c2[i] = n2;
+    c.sd.gbx[i] = idx;
+    if (idx < ng) {  // CartesianCheckBounds (cartesian_motion.hpp:38-54)
+      double l, h;
+      bool bad = false;
+      bounds_of(c.b3lo, c.b3hi, ng, idx, l, h);
+      bad |= (n3 < l) | (n3 >= h);
+      bounds_of(c.b1lo, c.b1hi, ng, idx, l, h);
+      bad |= (n1 < l) | (n1 >= h);
+      bounds_of(c.b2lo, c.b2hi, ng, idx, l, h);
+      bad |= (n2 < l) | (n2 >= h);
+      if (bad) w.fail(CLEO_ERR_OUT_OF_BOX);
+    }
+    keys[i] = idx < ng ? idx : ng;
+  }
+}
+
+// sort keys of freshly uploaded droplets
+__global__ void k_keys_from_gbx(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const uint32_t n = c.counters[0];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t g = c.sd.gbx[i];
+    keys[i] = g < c.ngbxs ? g : c.ngbxs;
+    vals[i] = i;
+  }
+}
+
+// permute every field of the current buffer into the other one
+__global__ void k_gather(Fields src, Fields dst, const uint32_t* __restrict__ perm,
+                         const uint32_t* __restrict__ n_ptr) {
+  const uint32_t n = *n_ptr;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const uint32_t s = perm[j];
+    dst.gbx[j] = src.gbx[s];
+    dst.c3[j] = src.c3[s];
+    dst.c1[j] = src.c1[s];
+    dst.c2[j] = src.c2[s];
+    dst.xi[j] = src.xi[s];
+    dst.r[j] = src.r[s];
+    dst.msol[j] = src.msol[s];
+    dst.id[j] = src.id[s];
+  }
+}
+
+// gridbox refs from the sorted keys: gstart[k] = lower_bound(keys, k) for k in [0, ngbxs + 1]
+// (find_refs by partition point, findrefs.hpp:54-126)
+__global__ void k_refs(DevCtx c, const uint32_t* __restrict__ keys) {
+  const uint32_t n = c.counters[0];
+  const uint32_t nk = c.ngbxs + 2;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, len = n;
+    while (len > 0) {
+      const uint32_t half = len >> 1;
+      if (keys[lo + half] < k) {
+        lo = lo + half + 1;
+        len -= half + 1;
+      } else {
+        len = half;
+      }
+    }
+    c.gstart[k] = lo;
+    if (k > 0 && k <= c.ngbxs) {
+      // gcount of gridbox k-1 written once gstart[k-1] is known: computed below
+    }
+  }
+}
+
+__global__ void k_counts(DevCtx c) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x)
+    c.gcount[g] = c.gstart[g + 1] - c.gstart[g];
+  if (blockIdx.x == 0 && threadIdx.x == 0) c.counters[1] = c.gstart[c.ngbxs];
+}
+
+// append [ndomain, nrange) to the out-of-domain store, then nrange = ndomain
+__global__ void k_to_grave(DevCtx c) {
+  const uint32_t nd = c.gstart[c.ngbxs];
+  const uint32_t n = c.counters[0];
+  const uint32_t ng0 = c.counters[2];
+  for (uint32_t j = nd + blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const uint32_t o = ng0 + (j - nd);
+    c.grave.gbx[o] = c.sd.gbx[j];
+    c.grave.c3[o] = c.sd.c3[j];
+    c.grave.c1[o] = c.sd.c1[j];
+    c.grave.c2[o] = c.sd.c2[j];
+    c.grave.xi[o] = c.sd.xi[j];
+    c.grave.r[o] = c.sd.r[j];
+    c.grave.msol[o] = c.sd.msol[j];
+    c.grave.id[o] = c.sd.id[j];
+  }
+}
+__global__ void k_grave_commit(DevCtx c) {
+  const uint32_t nd = c.gstart[c.ngbxs];
+  c.counters[2] += c.counters[0] - nd;
+  c.counters[0] = nd;
+  c.counters[1] = nd;
+}
+
+// ---- block reductions (fixed order: warp shuffles then warps in order) ----
+template <class T>
+__device__ __forceinline__ T block_sum(T v, T* sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+  __syncthreads();
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  T s = 0;
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += sh[k];
+    sh[0] = s;
+  }
+  __syncthreads();
+  s = sh[0];
+  __syncthreads();
+  return s;
+}
+
+// exclusive scan over a block (any blockDim multiple of 32, <= 1024)
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* wsum, uint32_t& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t s = 0;
+    for (int k = 0; k < nw; ++k) {
+      const uint32_t t = wsum[k];
+      wsum[k] = s;
+      s += t;
+    }
+    wsum[nw] = s;
+  }
+  __syncthreads();
+  const uint32_t r = wsum[warp] + x - v;
+  total = wsum[nw];
+  __syncthreads();
+  return r;
+}
+
+// ------------------------------------------------------------------------------------------
+// k_micro: SDMMicrophysicsFunctor (sdmmethods.hpp:54-93) for one gridbox per CTA
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(MICRO_THREADS)
+k_micro(DevCtx c, uint32_t t_sdm, uint32_t t_sdm_next, int did_motion) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double shd[32];
+  __shared__ unsigned long long shu[32];
+  __shared__ uint32_t shw[40];
+  const cleo_b200_params& p = c.p;
+  const int tid = threadIdx.x;
+  for (uint32_t g = blockIdx.x; g < c.ngbxs; g += gridDim.x) {
+    const uint32_t base = c.gstart[g];
+    uint32_t n = c.gcount[g];
+    // effect_on_hydrometeor_states after motion (movesupersindomain.hpp:95-136)
+    if (did_motion) {
+      double m = 0.0;
+      for (uint32_t k = tid; k < n; k += blockDim.x) {
+        const Where w{c.err, g, base + k};
+        m += condensate_mass(c.sd.r[base + k], c.sd.msol[base + k], w) * (double)c.sd.xi[base + k];
+      }
+      const double totmass_cond = block_sum(m, shd);
+      if (tid == 0) {
+        const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
+        const double rho_cond = totmass_cond / c.volume[g] * R0cubed_VOL0;
+        const double rho_dry = dry_air_density(c.press[g], c.temp[g], c.qvap[g]);
+        c.qcond[g] = rho_cond / rho_dry;
+      }
+    }
+    const uint64_t key = cleo_rng_key(p.seed, t_sdm, g);
+    uint64_t slot = 0;
+    uint32_t subt = t_sdm;
+    while (subt < t_sdm_next) {
+      // ---- DoCondensation (condensation.cpp:43-138) ----
+      if (on_step(p.condstep, subt)) {
+        const Where wg{c.err, g, base};
+        const double temp = c.temp[g];
+        const double psat = saturation_pressure(temp, wg);
+        const double s_ratio = supersaturation_ratio(c.press[g], c.qvap[g], psat);
+        const double ffactor = diffusion_factor(c.press[g], temp, psat);
+        const NewtonCfg cfg{p.maxniters, p.rtol, p.atol};
+        double dm = 0.0;
+        unsigned long long its = 0;
+        for (uint32_t k = tid; k < n; k += blockDim.x) {
+          const uint32_t i = base + k;
+          const Where w{c.err, g, i};
+          const double r = c.sd.r[i], msol = c.sd.msol[i];
+          const double old_m_cond = condensate_mass(r, msol, w);
+          double akoh, bkoh;
+          kohler_factors(msol, temp, akoh, bkoh);
+          uint32_t ni = 0;
+          const double newr = solve_condensation(cfg, p.cond_delt, p.cond_minsubdelt, s_ratio,
+                                                 akoh, bkoh, ffactor, r, 0.0, ni, w);
+          const double rnew = fmax(newr, dryradius(msol));  // change_radius
+          c.sd.r[i] = rnew;
+          dm += (condensate_mass(rnew, msol, w) - old_m_cond) * (double)c.sd.xi[i];
+          its += ni;
+        }
+        const double totmass = block_sum(dm, shd);
+        const unsigned long long totits = block_sum(its, shu);
+        if (tid == 0) {
+          if (p.do_alter_thermo) {  // state_change: condensation.cpp:126-138
+            const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
+            const double totrho = totmass / c.volume[g] * R0cubed_VOL0;
+            const double rho_dry = dry_air_density(c.press[g], c.temp[g], c.qvap[g]);
+            const double dq = totrho / rho_dry;
+            c.qvap[g] -= dq;
+            c.qcond[g] += dq;
+            const double dtemp = (Latent_v / moist_specifc_heat(c.qvap[g], c.qcond[g])) * dq;
+            c.temp[g] += dtemp;
+          }
+          c.cond_mass[g] += totmass;
+          c.nr_iters[g] += totits;
+        }
+        __syncthreads();
+      }
+      // ---- DoCollisions (collisions.hpp:263-278) ----
+      if (on_step(p.collstep, subt)) {
+        const bool in_smem = n <= NSMEM;
+        double* Sr = in_smem ? reinterpret_cast<double*>(smem) : c.scr_r + base;
+        double* Sm = in_smem ? reinterpret_cast<double*>(smem) + NSMEM : c.scr_m + base;
+        unsigned long long* Sx = in_smem ? reinterpret_cast<unsigned long long*>(smem) + 2 * NSMEM
+                                         : c.scr_x + base;
+        uint32_t* P = in_smem ? reinterpret_cast<uint32_t*>(smem + 24 * NSMEM) : c.scr_p + base;
+        uint32_t* J = in_smem ? reinterpret_cast<uint32_t*>(smem + 28 * NSMEM) : c.scr_j + base;
+        for (uint32_t k = tid; k < n; k += blockDim.x) {
+          Sr[k] = c.sd.r[base + k];
+          Sm[k] = c.sd.msol[base + k];
+          Sx[k] = c.sd.xi[base + k];
+          P[k] = k;
+          // Fisher-Yates draw for position k (k >= 1): slot n-1-k (shuffle.hpp:80-87)
+          if (k >= 1) J[k] = (uint32_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - k)), 0, (uint64_t)k + 1);
+        }
+        __syncthreads();
+        if (tid == 0) {
+          for (uint32_t it = n > 0 ? n - 1 : 0; it > 0; --it) {
+            const uint32_t j = J[it];
+            const uint32_t t = P[it];
+            P[it] = P[j];
+            P[j] = t;
+          }
+        }
+        __syncthreads();
+        const uint64_t slot_pairs = slot + (n >= 1 ? n - 1 : 0);
+        const uint32_t npairs = n / 2;
+        const double scale_p = (double)n * ((double)n - 1.0) / (2.0 * (double)npairs);
+        const double VOLUME = c.volume[g] * VOL0;
+        uint32_t nnull = 0;
+        for (uint32_t jj = tid; jj < npairs; jj += blockDim.x) {
+          const uint32_t a = P[2 * jj], b = P[2 * jj + 1];
+          const Where w{c.err, g, (uint64_t)base + 2 * jj};
+          Drop dA{Sx[a], Sr[a], Sm[a]};
+          Drop dB{Sx[b], Sr[b], Sm[b]};
+          const bool swap = dA.xi < dB.xi;  // assign_drops: collisions.hpp:94-101
+          Drop& d1 = swap ? dB : dA;
+          Drop& d2 = swap ? dA : dB;
+          const double prob_jk = pair_prob(p, d1.r, d2.r, VOLUME);
+          const double large_xi = (double)d1.xi;
+          const double prob = scale_p * large_xi * prob_jk;
+          const double phi_coll = cleo_rng_to_unit(cleo_rng_u64(key, slot_pairs + 2ull * jj));
+          const double phi_out = cleo_rng_to_unit(cleo_rng_u64(key, slot_pairs + 2ull * jj + 1));
+          nnull += enact_collision(p, d1, d2, prob, phi_coll, phi_out, w);
+          Sx[a] = dA.xi; Sr[a] = dA.r; Sm[a] = dA.msol;
+          Sx[b] = dB.xi; Sr[b] = dB.r; Sm[b] = dB.msol;
+        }
+        slot = slot_pairs + 2ull * npairs;
+        const uint32_t totnull = block_sum(nnull, shw);
+        // write back in shuffled order; nulls moved behind the valid ones, stably
+        // (remove_null_supers: collisions.hpp:240-248)
+        uint32_t nvalid = n - totnull;
+        uint32_t cval = 0, cnull = 0;
+        for (uint32_t k0 = 0; k0 < n; k0 += blockDim.x) {
+          const uint32_t k = k0 + tid;
+          const bool act = k < n;
+          const uint32_t src = act ? P[k] : 0;
+          const bool valid = act && Sx[src] != 0;
+          uint32_t tv, tn;
+          const uint32_t ev = block_excl_scan(valid ? 1u : 0u, shw, tv);
+          const uint32_t en = block_excl_scan((act && !valid) ? 1u : 0u, shw, tn);
+          if (act) {
+            const uint32_t q = valid ? (cval + ev) : (nvalid + cnull + en);
+            const uint32_t o = base + q;
+            const uint32_t s = base + src;
+            c.scr_c3[o] = c.sd.c3[s];
+            c.scr_c1[o] = c.sd.c1[s];
+            c.scr_c2[o] = c.sd.c2[s];
+            c.scr_id[o] = c.sd.id[s];
+            J[q] = src;  // inverse map, J no longer needed
+          }
+          cval += tv;
+          cnull += tn;
+        }
+        __syncthreads();
+        for (uint32_t q = tid; q < n; q += blockDim.x) {
+          const uint32_t src = J[q];
+          const uint32_t o = base + q;
+          c.sd.r[o] = Sr[src];
+          c.sd.msol[o] = Sm[src];
+          c.sd.xi[o] = Sx[src];
+          c.sd.gbx[o] = q < nvalid ? g : OOB;
+          c.sd.c3[o] = c.scr_c3[o];
+          c.sd.c1[o] = c.scr_c1[o];
+          c.sd.c2[o] = c.scr_c2[o];
+          c.sd.id[o] = c.scr_id[o];
+        }
+        __syncthreads();
+        n = nvalid;
+      }
+      subt = min(next_step(p.condstep, subt), next_step(p.collstep, subt));
+    }
+    if (tid == 0) c.gcount[g] = n;
+    __syncthreads();
+  }
+}
+
+// batched implicit-Euler solves of independent droplets
+__global__ void k_condsolve(DevCtx c, uint32_t n, const double* __restrict__ radius,
+                            const double* __restrict__ msol, const double* __restrict__ temp,
+                            const double* __restrict__ press, const double* __restrict__ s_ratio,
+                            const double* __restrict__ delt, double* __restrict__ out,
+                            uint32_t* __restrict__ niters_out) {
+  const NewtonCfg cfg{c.p.maxniters, c.p.rtol, c.p.atol};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const Where w{c.err, OOB, i};
+    const double T = temp[i];
+    const double psat = saturation_pressure(T, w);
+    const double ffactor = diffusion_factor(press[i], T, psat);
+    double akoh, bkoh;
+    kohler_factors(msol[i], T, akoh, bkoh);
+    uint32_t ni = 0;
+    const double newr = solve_condensation(cfg, delt[i], c.p.cond_minsubdelt, s_ratio[i], akoh,
+                                           bkoh, ffactor, radius[i], 0.0, ni, w);
+    out[i] = fmax(newr, dryradius(msol[i]));
+    if (niters_out) niters_out[i] = ni;
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------
+namespace {
+
+template <class T>
+int dalloc(cleo_b200_ctx* x, T** p, size_t n) {
+  void* q = nullptr;
+  CUDA_TRY(cudaMalloc(&q, (n ? n : 1) * sizeof(T)));
+  x->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return CLEO_OK;
+}
+
+int alloc_fields(cleo_b200_ctx* x, Fields& f, size_t n) {
+  int rc = 0;
+  rc |= dalloc(x, &f.gbx, n);
+  rc |= dalloc(x, &f.c3, n);
+  rc |= dalloc(x, &f.c1, n);
+  rc |= dalloc(x, &f.c2, n);
+  rc |= dalloc(x, &f.xi, n);
+  rc |= dalloc(x, &f.r, n);
+  rc |= dalloc(x, &f.msol, n);
+  rc |= dalloc(x, &f.id, n);
+  return rc ? CLEO_ERR_CUDA : CLEO_OK;
+}
+
+int grid_for(size_t n, int threads) {
+  size_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > 148 * 64) b = 148 * 64;
+  return (int)b;
+}
+
+// stable sort of the current buffer's [0, nrange) by key, then gather, refs and store append
+int sort_current(cleo_b200_ctx* x) {
+  DevCtx& d = x->d;
+  cudaStream_t s = x->stream;
+  const uint32_t nt = x->ntiles_max;
+  uint32_t* kin = x->keys[0];
+  uint32_t* vin = x->vals[0];
+  uint32_t* kout = x->keys[1];
+  uint32_t* vout = x->vals[1];
+  const uint64_t nh = (uint64_t)256 * nt;
+  const uint32_t nscan_tiles = (uint32_t)((nh + SCAN_TILE - 1) / SCAN_TILE);
+  for (uint32_t shift = 0; shift < x->key_bits; shift += 8) {
+    k_rs_upsweep<<<nt, RS_THREADS, 0, s>>>(kin, d.counters, (int)shift, x->hist, nt);
+    k_scan_tiles<<<nscan_tiles, SCAN_THREADS, 0, s>>>(x->hist, x->hist, nh, x->tile_sums);
+    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(x->tile_sums, nscan_tiles, nullptr);
+    k_scan_add<<<(unsigned)((nh + 255) / 256), 256, 0, s>>>(x->hist, nh, x->tile_sums);
+    k_rs_downsweep<<<nt, RS_THREADS, 0, s>>>(kin, vin, d.counters, (int)shift, x->hist, nt, kout,
+                                             vout);
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+  // sorted (key, position) now in kin/vin
+  Fields& src = x->buf[x->cur];
+  Fields& dst = x->buf[1 - x->cur];
+  k_gather<<<grid_for(d.capacity, 256), 256, 0, s>>>(src, dst, vin, d.counters);
+  x->cur = 1 - x->cur;
+  d.sd = x->buf[x->cur];
+  k_refs<<<grid_for((size_t)d.ngbxs + 2, 256), 256, 0, s>>>(d, kin);
+  k_counts<<<grid_for(d.ngbxs, 256), 256, 0, s>>>(d);
+  k_to_grave<<<grid_for(d.capacity, 256), 256, 0, s>>>(d);
+  k_grave_commit<<<1, 1, 0, s>>>(d);
+  CUDA_TRY(cudaGetLastError());
+  return CLEO_OK;
+}
+
+int run_sdm_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
+  DevCtx& d = x->d;
+  cudaStream_t s = x->stream;
+  const bool did_motion = on_step(d.p.motionstep, t_sdm);
+  if (did_motion) {
+    k_motion<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, x->keys[0], x->vals[0]);
+    const int rc = sort_current(x);
+    if (rc) return rc;
+  }
+  const bool micro = (d.p.condstep != CLEO_STEP_OFF || d.p.collstep != CLEO_STEP_OFF);
+  if (micro || did_motion) {
+    const uint32_t blocks = d.ngbxs < (1u << 30) ? d.ngbxs : (1u << 30);
+    if (blocks > 0)
+      k_micro<<<blocks, MICRO_THREADS, MICRO_SMEM, s>>>(d, t_sdm, t_sdm_next, did_motion ? 1 : 0);
+  }
+  CUDA_TRY(cudaGetLastError());
+  return CLEO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cleo_b200_version(void) { return "cleo_b200 0.1 (sm_100a)"; }
+
+int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid, size_t capacity,
+                     cleo_b200_ctx** out) {
+  if (!params || !grid || !out) return CLEO_ERR_ARGUMENT;
+  if (capacity >= 0xFFFFFFFFull || grid->ngbxs >= 0xFFFFFFF0u) return CLEO_ERR_CAPACITY;
+  if (params->condstep != CLEO_STEP_OFF && params->cond_delt < params->cond_minsubdelt)
+    return CLEO_ERR_SUBDELT;  // ImplicitEuler ctor, impliciteuler.hpp:320-326
+  if (params->condstep == 0 || params->collstep == 0 || params->motionstep == 0)
+    return CLEO_ERR_ARGUMENT;
+  // a sub-stepping loop needs a positive minimum sub-step, and Newton solves a finite budget
+  if (params->condstep != CLEO_STEP_OFF &&
+      (!(params->cond_minsubdelt > 0.0) || params->maxniters > 1000000u))
+    return CLEO_ERR_ARGUMENT;
+  if ((uint64_t)grid->ndims[0] * grid->ndims[1] * grid->ndims[2] != grid->ngbxs ||
+      grid->ndims[0] == 0 || grid->ndims[1] == 0 || grid->ndims[2] == 0)
+    return CLEO_ERR_ARGUMENT;
+  auto* x = new (std::nothrow) cleo_b200_ctx();
+  if (!x) return CLEO_ERR_CAPACITY;
+  CUDA_TRY(cudaGetDevice(&x->device));
+  DevCtx& d = x->d;
+  d.p = *params;
+  d.ngbxs = grid->ngbxs;
+  for (int i = 0; i < 3; ++i) d.ndims[i] = grid->ndims[i];
+  d.capacity = (uint32_t)capacity;
+  const size_t ng = grid->ngbxs, cap = capacity;
+  int rc = 0;
+  double* maps[6];
+  for (int k = 0; k < 6; ++k) rc |= dalloc(x, &maps[k], ng);
+  uint32_t* nb[6];
+  for (int k = 0; k < 6; ++k) rc |= dalloc(x, &nb[k], ng);
+  double* st[11];
+  for (int k = 0; k < 11; ++k) rc |= dalloc(x, &st[k], ng);
+  rc |= dalloc(x, &d.cond_mass, ng);
+  rc |= dalloc(x, &d.nr_iters, ng);
+  rc |= alloc_fields(x, x->buf[0], cap);
+  rc |= alloc_fields(x, x->buf[1], cap);
+  rc |= alloc_fields(x, d.grave, cap);
+  rc |= dalloc(x, &d.gstart, ng + 2);
+  rc |= dalloc(x, &d.gcount, ng);
+  rc |= dalloc(x, &d.counters, 4);
+  rc |= dalloc(x, &d.scr_r, cap);
+  rc |= dalloc(x, &d.scr_m, cap);
+  rc |= dalloc(x, &d.scr_c3, cap);
+  rc |= dalloc(x, &d.scr_c1, cap);
+  rc |= dalloc(x, &d.scr_c2, cap);
+  rc |= dalloc(x, &d.scr_x, cap);
+  rc |= dalloc(x, &d.scr_id, cap);
+  rc |= dalloc(x, &d.scr_p, cap);
+  rc |= dalloc(x, &d.scr_j, cap);
+  rc |= dalloc(x, &d.err, 1);
+  x->ntiles_max = (uint32_t)((cap + RS_TILE - 1) / RS_TILE);
+  if (x->ntiles_max == 0) x->ntiles_max = 1;
+  for (int k = 0; k < 2; ++k) {
+    rc |= dalloc(x, &x->keys[k], cap);
+    rc |= dalloc(x, &x->vals[k], cap);
+  }
+  rc |= dalloc(x, &x->hist, (size_t)256 * x->ntiles_max);
+  rc |= dalloc(x, &x->tile_sums, ((size_t)256 * x->ntiles_max + SCAN_TILE - 1) / SCAN_TILE + 1);
+  if (rc) {
+    cleo_b200_destroy(x);
+    return CLEO_ERR_CUDA;
+  }
+  // key bits: keys run over [0, ngbxs]
+  uint32_t bits = 0;
+  while (bits < 32 && (((uint64_t)1 << bits) <= (uint64_t)ng)) ++bits;
+  x->key_bits = bits == 0 ? 8 : ((bits + 7) / 8) * 8;
+  d.b3lo = maps[0]; d.b3hi = maps[1]; d.b1lo = maps[2]; d.b1hi = maps[3]; d.b2lo = maps[4]; d.b2hi = maps[5];
+  d.back3 = nb[0]; d.fwd3 = nb[1]; d.back1 = nb[2]; d.fwd1 = nb[3]; d.back2 = nb[4]; d.fwd2 = nb[5];
+  d.volume = st[0]; d.press = st[1]; d.temp = st[2]; d.qvap = st[3]; d.qcond = st[4];
+  d.wlo = st[5]; d.whi = st[6]; d.ulo = st[7]; d.uhi = st[8]; d.vlo = st[9]; d.vhi = st[10];
+  d.sd = x->buf[0];
+  CUDA_TRY(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
+  x->own_stream = true;
+  const double* src_maps[6] = {grid->coord3lo, grid->coord3hi, grid->coord1lo,
+                               grid->coord1hi, grid->coord2lo, grid->coord2hi};
+  const uint32_t* src_nb[6] = {grid->back3, grid->fwd3, grid->back1, grid->fwd1, grid->back2, grid->fwd2};
+  for (int k = 0; k < 6; ++k) {
+    if (!src_maps[k] || !src_nb[k]) {
+      cleo_b200_destroy(x);
+      return CLEO_ERR_ARGUMENT;
+    }
+    CUDA_TRY(cudaMemcpyAsync(maps[k], src_maps[k], ng * 8, cudaMemcpyHostToDevice, x->stream));
+    CUDA_TRY(cudaMemcpyAsync(nb[k], src_nb[k], ng * 4, cudaMemcpyHostToDevice, x->stream));
+  }
+  CUDA_TRY(cudaMemsetAsync(d.cond_mass, 0, ng * 8, x->stream));
+  CUDA_TRY(cudaMemsetAsync(d.nr_iters, 0, ng * 8, x->stream));
+  CUDA_TRY(cudaMemsetAsync(d.counters, 0, 16, x->stream));
+  CUDA_TRY(cudaMemsetAsync(d.gstart, 0, (ng + 2) * 4, x->stream));
+  CUDA_TRY(cudaMemsetAsync(d.gcount, 0, (ng ? ng : 1) * 4, x->stream));
+  CUDA_TRY(cudaMemsetAsync(d.err, 0, sizeof(DevError), x->stream));
+  CUDA_TRY(cudaFuncSetAttribute(k_micro, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MICRO_SMEM));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  *out = x;
+  return CLEO_OK;
+}
+
+void cleo_b200_destroy(cleo_b200_ctx* x) {
+  if (!x) return;
+  if (x->stream) cudaStreamSynchronize(x->stream);
+  for (void* p : x->allocs) cudaFree(p);
+  if (x->own_stream && x->stream) cudaStreamDestroy(x->stream);
+  delete x;
+}
+
+void* cleo_b200_stream(cleo_b200_ctx* x) { return x ? (void*)x->stream : nullptr; }
+
+int cleo_b200_upload_supers(cleo_b200_ctx* x, const cleo_b200_supers* h, size_t n) {
+  if (!x || !h) return CLEO_ERR_ARGUMENT;
+  if (n > x->d.capacity) return CLEO_ERR_CAPACITY;
+  if (!h->sdgbxindex || !h->coord3 || !h->coord1 || !h->coord2 || !h->xi || !h->radius || !h->msol)
+    return CLEO_ERR_ARGUMENT;
+  cudaStream_t s = x->stream;
+  Fields& f = x->buf[x->cur];
+  CUDA_TRY(cudaMemcpyAsync(f.gbx, h->sdgbxindex, n * 4, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(f.c3, h->coord3, n * 8, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(f.c1, h->coord1, n * 8, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(f.c2, h->coord2, n * 8, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(f.xi, h->xi, n * 8, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(f.r, h->radius, n * 8, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(f.msol, h->msol, n * 8, cudaMemcpyHostToDevice, s));
+  if (h->sdid) {
+    CUDA_TRY(cudaMemcpyAsync(f.id, h->sdid, n * 8, cudaMemcpyHostToDevice, s));
+  } else {
+    std::vector<unsigned long long> ids(n);
+    for (size_t k = 0; k < n; ++k) ids[k] = k;
+    CUDA_TRY(cudaMemcpyAsync(f.id, ids.data(), n * 8, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  const uint32_t cnt[4] = {(uint32_t)n, 0, 0, 0};
+  CUDA_TRY(cudaMemcpyAsync(x->d.counters, cnt, 16, cudaMemcpyHostToDevice, s));
+  k_keys_from_gbx<<<grid_for(x->d.capacity, 256), 256, 0, s>>>(x->d, x->keys[0], x->vals[0]);
+  const int rc = sort_current(x);  // SupersInDomain ctor: supersindomain.hpp:55-62
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return CLEO_OK;
+}
+
+int cleo_b200_upload_state(cleo_b200_ctx* x, const cleo_b200_gbx_state* h) {
+  if (!x || !h) return CLEO_ERR_ARGUMENT;
+  const size_t ng = x->d.ngbxs;
+  const double* src[11] = {h->volume, h->press, h->temp, h->qvap, h->qcond, h->wvel_lo,
+                           h->wvel_hi, h->uvel_lo, h->uvel_hi, h->vvel_lo, h->vvel_hi};
+  double* dst[11] = {x->d.volume, x->d.press, x->d.temp, x->d.qvap, x->d.qcond, x->d.wlo,
+                     x->d.whi, x->d.ulo, x->d.uhi, x->d.vlo, x->d.vhi};
+  for (int k = 0; k < 11; ++k) {
+    if (!src[k]) return CLEO_ERR_ARGUMENT;
+    CUDA_TRY(cudaMemcpyAsync(dst[k], src[k], ng * 8, cudaMemcpyHostToDevice, x->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  return CLEO_OK;
+}
+
+int cleo_b200_step(cleo_b200_ctx* x, uint32_t t_mdl, uint32_t t_next) {
+  if (!x) return CLEO_ERR_ARGUMENT;
+  uint32_t t_sdm = t_mdl;
+  while (t_sdm < t_next) {
+    const uint32_t next_move = next_step(x->d.p.motionstep, t_sdm);
+    const uint32_t t_sdm_next = t_next < next_move ? t_next : next_move;
+    const int rc = run_sdm_step(x, t_sdm, t_sdm_next);
+    if (rc) return rc;
+    t_sdm = t_sdm_next;
+  }
+  return CLEO_OK;
+}
+
+int cleo_b200_status(cleo_b200_ctx* x, cleo_b200_error* err) {
+  if (!x) return CLEO_ERR_ARGUMENT;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  DevError e;
+  CUDA_TRY(cudaMemcpy(&e, x->d.err, sizeof(e), cudaMemcpyDeviceToHost));
+  if (err) {
+    err->code = e.code;
+    err->gbxindex = e.gbx;
+    err->index = e.index;
+  }
+  return e.code;
+}
+
+int cleo_b200_domain_nsupers(cleo_b200_ctx* x, size_t* n) {
+  if (!x || !n) return CLEO_ERR_ARGUMENT;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  std::vector<uint32_t> cnt(x->d.ngbxs ? x->d.ngbxs : 1);
+  CUDA_TRY(cudaMemcpy(cnt.data(), x->d.gcount, (size_t)x->d.ngbxs * 4, cudaMemcpyDeviceToHost));
+  size_t s = 0;
+  for (uint32_t g = 0; g < x->d.ngbxs; ++g) s += cnt[g];
+  *n = s;
+  return CLEO_OK;
+}
+
+int cleo_b200_download_supers(cleo_b200_ctx* x, cleo_b200_supers* h, size_t* n_domain,
+                              size_t* n_total) {
+  if (!x || !h) return CLEO_ERR_ARGUMENT;
+  cudaStream_t s = x->stream;
+  CUDA_TRY(cudaStreamSynchronize(s));
+  uint32_t cnt[4];
+  CUDA_TRY(cudaMemcpy(cnt, x->d.counters, 16, cudaMemcpyDeviceToHost));
+  const uint32_t nrange = cnt[0], ngrave = cnt[2];
+  const size_t ng = x->d.ngbxs;
+  std::vector<uint32_t> gstart(ng + 2), gcount(ng ? ng : 1);
+  CUDA_TRY(cudaMemcpy(gstart.data(), x->d.gstart, (ng + 2) * 4, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(gcount.data(), x->d.gcount, ng * 4, cudaMemcpyDeviceToHost));
+  // pull both regions to host staging
+  struct HostF {
+    std::vector<uint32_t> gbx;
+    std::vector<double> c3, c1, c2, r, m;
+    std::vector<unsigned long long> xi, id;
+    void resize(size_t n) {
+      gbx.resize(n); c3.resize(n); c1.resize(n); c2.resize(n); r.resize(n); m.resize(n);
+      xi.resize(n); id.resize(n);
+    }
+  };
+  auto pull = [&](const Fields& f, size_t n, HostF& o) -> int {
+    o.resize(n ? n : 1);
+    if (!n) return CLEO_OK;
+    CUDA_TRY(cudaMemcpy(o.gbx.data(), f.gbx, n * 4, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(o.c3.data(), f.c3, n * 8, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(o.c1.data(), f.c1, n * 8, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(o.c2.data(), f.c2, n * 8, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(o.xi.data(), f.xi, n * 8, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(o.r.data(), f.r, n * 8, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(o.m.data(), f.msol, n * 8, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(o.id.data(), f.id, n * 8, cudaMemcpyDeviceToHost));
+    return CLEO_OK;
+  };
+  HostF dom, grv;
+  if (pull(x->buf[x->cur], nrange, dom) || pull(x->d.grave, ngrave, grv)) return CLEO_ERR_CUDA;
+  size_t o = 0;
+  auto put = [&](const HostF& f, size_t k) {
+    h->sdgbxindex[o] = f.gbx[k];
+    h->coord3[o] = f.c3[k]; h->coord1[o] = f.c1[k]; h->coord2[o] = f.c2[k];
+    h->xi[o] = f.xi[k]; h->radius[o] = f.r[k]; h->msol[o] = f.m[k];
+    if (h->sdid) h->sdid[o] = f.id[k];
+    ++o;
+  };
+  for (size_t g = 0; g < ng; ++g)
+    for (uint32_t k = gstart[g]; k < gstart[g] + gcount[g]; ++k) put(dom, k);
+  const size_t nd = o;
+  for (size_t g = 0; g < ng; ++g)  // null superdroplets still inside gridbox ranges
+    for (uint32_t k = gstart[g] + gcount[g]; k < gstart[g + 1]; ++k) put(dom, k);
+  for (uint32_t k = gstart[ng]; k < nrange; ++k) put(dom, k);
+  for (uint32_t k = 0; k < ngrave; ++k) put(grv, k);
+  if (n_domain) *n_domain = nd;
+  if (n_total) *n_total = o;
+  return CLEO_OK;
+}
+
+int cleo_b200_download_state(cleo_b200_ctx* x, cleo_b200_gbx_state* h) {
+  if (!x || !h) return CLEO_ERR_ARGUMENT;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  const size_t ng = x->d.ngbxs;
+  double* dst[11] = {h->volume, h->press, h->temp, h->qvap, h->qcond, h->wvel_lo,
+                     h->wvel_hi, h->uvel_lo, h->uvel_hi, h->vvel_lo, h->vvel_hi};
+  const double* src[11] = {x->d.volume, x->d.press, x->d.temp, x->d.qvap, x->d.qcond, x->d.wlo,
+                           x->d.whi, x->d.ulo, x->d.uhi, x->d.vlo, x->d.vhi};
+  for (int k = 0; k < 11; ++k) {
+    if (!dst[k]) return CLEO_ERR_ARGUMENT;
+    CUDA_TRY(cudaMemcpy(dst[k], src[k], ng * 8, cudaMemcpyDeviceToHost));
+  }
+  return CLEO_OK;
+}
+
+int cleo_b200_download_budgets(cleo_b200_ctx* x, double* cond_mass, uint64_t* nr_iters) {
+  if (!x) return CLEO_ERR_ARGUMENT;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  const size_t ng = x->d.ngbxs;
+  if (cond_mass) CUDA_TRY(cudaMemcpy(cond_mass, x->d.cond_mass, ng * 8, cudaMemcpyDeviceToHost));
+  if (nr_iters) CUDA_TRY(cudaMemcpy(nr_iters, x->d.nr_iters, ng * 8, cudaMemcpyDeviceToHost));
+  return CLEO_OK;
+}
+
+int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_radius,
+                                 const double* d_msol, const double* d_temp, const double* d_press,
+                                 const double* d_s_ratio, const double* d_delt,
+                                 double* d_radius_out, uint32_t* d_niters_out) {
+  if (!x || !d_radius || !d_msol || !d_temp || !d_press || !d_s_ratio || !d_delt || !d_radius_out)
+    return CLEO_ERR_ARGUMENT;
+  if (n >= 0xFFFFFFFFull) return CLEO_ERR_CAPACITY;
+  if (n == 0) return CLEO_OK;
+  k_condsolve<<<grid_for(n, 128), 128, 0, x->stream>>>(x->d, (uint32_t)n, d_radius, d_msol, d_temp,
+                                                       d_press, d_s_ratio, d_delt, d_radius_out,
+                                                       d_niters_out);
+  CUDA_TRY(cudaGetLastError());
+  return CLEO_OK;
+}
+
+}  // extern "C"

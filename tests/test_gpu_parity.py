@@ -1,0 +1,147 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and the golden fixtures.
+
+Bar: sort order, gridbox indices, multiplicities and ids bit-exact; radius, solute mass,
+coordinates and gridbox state within 1e-12 relative in FP64 (the only differences allowed come
+from CUDA's vs the host libm's pow/exp and from the order of per-gridbox FP64 sums).
+"""
+import ctypes as C
+import math
+import os
+
+import numpy as np
+import pytest
+
+import checkers as K
+from cleo_b200 import abi, workloads as W
+from cleo_b200.config import make_params
+from cleo_b200.sdm import CleoError, make_sdm
+from test_oracle import ERRS, VARIANTS, _err_case, golovin_l1
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return abi.load_library()
+
+
+def run_pair(lib, w, nsteps):
+    g = make_sdm(w, lib=lib)
+    o = make_sdm(w, lib=K.oracle_lib(), prefix="oc")
+    ts = w["tstep"]
+    for s in range(nsteps):
+        g.run_step(s * ts, (s + 1) * ts)
+        o.run_step(s * ts, (s + 1) * ts)
+    g.check()
+    return g, o
+
+
+@pytest.mark.parametrize("fname", K.step_fixtures())
+def test_gpu_matches_golden(lib, fname):
+    w, exp = K.load_step_fixture(os.path.join(K.GOLDEN, fname))
+    g = make_sdm(w, lib=lib)
+    for s in range(exp["nsteps"]):
+        g.run_step(s * w["tstep"], (s + 1) * w["tstep"])
+    g.check()
+    K.assert_same_domain(g.download_supers(), exp["supers"], rtol=RTOL, what=fname)
+    st = g.download_state()
+    for f in abi.STATE_FIELDS:
+        assert K.max_rel(st[f], exp["state"][f]) <= RTOL, (fname, f)
+    assert K.max_rel(g.download_budgets()[0], exp["cond_mass"]) <= 1e-11
+
+
+@pytest.mark.parametrize("name,build,nsteps", VARIANTS, ids=[v[0] for v in VARIANTS])
+def test_gpu_matches_oracle_variants(lib, name, build, nsteps):
+    w = build()
+    g, o = run_pair(lib, w, nsteps)
+    K.assert_same_domain(g.download_supers(), o.download_supers(), rtol=RTOL, what=name)
+    sg, so = g.download_state(), o.download_state()
+    for f in abi.STATE_FIELDS:
+        assert K.max_rel(sg[f], so[f]) <= RTOL, (name, f)
+    cg, ig = g.download_budgets()
+    co, io = o.download_budgets()
+    assert K.max_rel(cg, co) <= 1e-11
+    assert np.array_equal(ig, io), (name, "newton iteration counts")
+
+
+@pytest.mark.parametrize("tol", [(50, 0.0, 0.01), (200, 0.0, 1e-10)])
+def test_gpu_condensation_solve(lib, tol):
+    import torch
+    mx, rt, at = tol
+    p = make_params(condtstep=1.0, maxniters=mx, rtol=rt, atol=at)
+    w = W.condsolve(50000, seed=13)
+    rc, ro, io = K.condsolve(K.oracle_lib(), "oc", p, w)
+    assert rc == 0
+    grid = W.cartesian_grid((1, 1, 1), (1.0, 1.0, 1.0), nspacedims=0)
+    from cleo_b200.sdm import SDM
+    s = SDM(p, grid, 1, lib=lib)
+    dev = {k: torch.tensor(w[k], dtype=torch.float64, device="cuda")
+           for k in ("radius", "msol", "temp", "press", "s_ratio", "delt")}
+    out = torch.empty_like(dev["radius"])
+    nit = torch.empty(len(w["radius"]), dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    rc = lib.cleo_b200_condensation_solve(
+        s.ctx, len(w["radius"]), *[C.c_void_p(dev[k].data_ptr()) for k in
+                                   ("radius", "msol", "temp", "press", "s_ratio", "delt")],
+        C.c_void_p(out.data_ptr()), C.c_void_p(nit.data_ptr()))
+    assert rc == 0
+    s.check()
+    rg = out.cpu().numpy()
+    assert K.max_rel(rg, ro) <= RTOL
+    assert np.array_equal(nit.cpu().numpy().astype(np.uint32), io)
+
+
+@pytest.mark.parametrize("name,pov,sov,dov,code", ERRS, ids=[e[0] for e in ERRS])
+def test_gpu_error_codes(lib, name, pov, sov, dov, code):
+    w = _err_case(pov, sov, dov)
+    s = make_sdm(w, lib=lib)
+    with pytest.raises(CleoError) as ei:
+        for k in range(3):
+            s.run_step(k * 100, (k + 1) * 100)
+        s.check()
+    assert ei.value.name == code
+    # the context stays usable after a reported failure
+    s.download_supers()
+
+
+def test_gpu_rainshaft_config(lib):
+    """1-D rain shaft at full size (256 boxes x 256 superdroplets), 10 steps."""
+    w = W.rainshaft()
+    g, o = run_pair(lib, w, 10)
+    K.assert_same_domain(g.download_supers(), o.download_supers(), rtol=RTOL, what="rainshaft")
+
+
+def test_gpu_uneven3d_medium(lib):
+    """3-D uneven counts on 32x32x16 boxes (~0.6 M superdroplets), 4 steps."""
+    w = W.uneven3d(ndims=(16, 32, 32), seed=8)
+    g, o = run_pair(lib, w, 4)
+    K.assert_same_domain(g.download_supers(), o.download_supers(), rtol=RTOL, what="uneven3d")
+
+
+def test_gpu_deterministic(lib):
+    w = W.bubble3d(ndims=(8, 16, 8), seed=9)
+    runs = []
+    for _ in range(2):
+        g = make_sdm(w, lib=lib)
+        for s in range(5):
+            g.run_step(s * 100, (s + 1) * 100)
+        d = g.download_supers()
+        runs.append(d)
+    for k in ("sdid", "xi", "radius", "coord3", "coord1"):
+        assert np.array_equal(runs[0][k], runs[1][k]), k
+
+
+def test_gpu_golovin_analytic(lib):
+    """The box model reproduces the Golovin analytic spectrum on the GPU (statistical)."""
+    errs = []
+    for seed in range(3):
+        w = W.box_golovin(8192, seed=200 + seed)
+        g = make_sdm(w, lib=lib)
+        for t in range(1200):
+            g.run_step(t * 100, (t + 1) * 100)
+        errs.append(golovin_l1(g.download_supers(), 1200))
+    assert np.mean(errs) < 0.12, errs
