@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 SDM hot path: superdroplet-steps/s on the 3-D uneven-count workload.
+
+Workload (one GPU): 64 x 128 x 128 gridboxes of 50 m^3, per-gridbox superdroplet count drawn from
+a lognormal (median 32, sigma 0.586, clipped to 0..2048), ~40 M superdroplets with lognormal NaCl
+dry radii at Kohler equilibrium; every 1 s step runs motion (sedimentation, RogersGK) + sort,
+condensation (implicit Euler, FP64 Newton) and collisions (Long kernel, CoalBuRe with ConstNFrags 5
+and the Straub flag). Synthetic, seeded inputs; the 2.4 GB of superdroplet state exceeds L2, so
+no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W]      # this implementation, one JSON line
+  python bench.py --impl reference [...]                    # CLEO's own sources on the host cores
+
+value  = in-domain superdroplets (all ranks) x K / max-over-ranks device time of the K steps
+e2e    = the same metric through the public API with host buffers: per step the gridbox states
+         are copied from pinned host memory (as a coupled dynamics step would) and the condensed
+         mass budget is read back.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from cleo_b200 import abi, workloads as W  # noqa: E402
+from cleo_b200.sdm import SDM, make_sdm  # noqa: E402
+
+METRIC = "superdroplet-steps/s on 1 B200: batched+MLP-seeded vs plain GPU, matched error"
+UNIT = "superdroplet-steps/s"
+NDIMS = (64, 128, 128)
+WORKLOAD = ("uneven3d: 64x128x128 gridboxes of 50 m^3, lognormal counts (median 32, sigma 0.586, "
+            "clip 0..2048), ~40M superdroplets; condensation + Long CoalBuRe(ConstNFrags 5, "
+            "Straub) + sedimentation (RogersGK), 1 s steps")
+# algorithmic bytes of one k_micro launch: per superdroplet read r, msol, xi, coord3/1/2, id
+# (56 B) and write them back permuted plus sdgbxindex (60 B); per gridbox read volume, press,
+# temp, qvap and write qcond, cond_mass, nr_iters (56 B)
+MICRO_BYTES_PER_SD = 116
+MICRO_BYTES_PER_GBX = 56
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+        time.sleep(0.15)
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            self.p.wait(timeout=10)
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.strip().split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        loaded = [v for v in sm if mx and v > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def reference_lib():
+    """CLEO's own sources built against the Kokkos-API shim, else the C restatement."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import checkers as K
+    if K.ref_available():
+        lib = K.ref_lib()
+        threads = os.cpu_count() or 1
+        lib.ref_set_num_threads(threads)
+        return lib, "ref", "reference", threads
+    return K.oracle_lib(), "oc", "port", 1
+
+
+def cpu_sample(steps, warmup, lib, prefix):
+    """SD-steps/s of a CPU implementation on a sub-grid of the workload (same per-box physics)."""
+    w = W.uneven3d(ndims=(64, 16, 16), seed=3)
+    s = make_sdm(w, lib=lib, prefix=prefix)
+    t = 0
+    for _ in range(warmup):
+        s.run_step(t * 100, (t + 1) * 100)
+        t += 1
+    nsd = s.download_supers()["n_domain"]
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.run_step(t * 100, (t + 1) * 100)
+        t += 1
+    dt = time.perf_counter() - t0
+    return nsd * steps / dt, nsd, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    lib, prefix, kind, cores = reference_lib()
+    steps = max(1, min(args.steps, 3))
+    warm = 1
+    value, nsd, dt = cpu_sample(steps, warm, lib, prefix)
+    sample = (f"64x16x16 gridboxes of the workload ({nsd} superdroplets), {steps} steps after "
+              f"{warm} warm-up, {cores} host threads")
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+           "n_gpus": args.gpus, "steps": steps, "warmup": warm,
+           "ms_per_step": 1000.0 * dt / steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "sample": sample},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                            "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    lib = abi.load_library()
+    ndims = tuple(int(x) for x in args.ndims.split(","))
+    wl = W.uneven3d(ndims=ndims, seed=3 + rank)  # one independent domain per rank (weak scaling)
+    sdm = make_sdm(wl, lib=lib)
+    ctx = sdm.ctx
+    stream = torch.cuda.ExternalStream(lib.cleo_b200_stream(ctx))
+    ngbxs = int(wl["grid"]["ngbxs"])
+    t = 0
+    for _ in range(args.warmup):
+        sdm.run_step(t * 100, (t + 1) * 100)
+        t += 1
+    sdm.check()
+    nd = C.c_size_t()
+    lib.cleo_b200_domain_nsupers(ctx, C.byref(nd))
+    nsd = int(nd.value)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-timed region ----
+    lib.cleo_b200_set_profiling(ctx, 1)
+    ms3, cnt3 = (C.c_double * 3)(), (C.c_uint64 * 3)()
+    lib.cleo_b200_stage_times(ctx, ms3, cnt3)  # reset
+    l0 = C.c_uint64()
+    lib.cleo_b200_kernel_launches(ctx, C.byref(l0))
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            sdm.run_step(t * 100, (t + 1) * 100)
+            t += 1
+        ev1.record(stream)
+        ev1.synchronize()
+    barrier()
+    clocks = clk.summary()
+    l1 = C.c_uint64()
+    lib.cleo_b200_kernel_launches(ctx, C.byref(l1))
+    lib.cleo_b200_stage_times(ctx, ms3, cnt3)
+    lib.cleo_b200_set_profiling(ctx, 0)
+    sdm.check()
+    ms = ev0.elapsed_time(ev1)
+    stage_ms = {k: ms3[i] / max(1, cnt3[i]) for i, k in enumerate(("motion", "sort", "microphysics"))}
+
+    # ---- end-to-end region through the public API with pinned host buffers ----
+    pinned = {f: torch.from_numpy(wl["state"][f]).pin_memory() for f in abi.STATE_FIELDS}
+    st_struct = abi.state_struct({f: pinned[f].numpy() for f in abi.STATE_FIELDS})
+    cm_out = torch.empty(ngbxs, dtype=torch.float64).pin_memory()
+    it_out = torch.empty(ngbxs, dtype=torch.int64).pin_memory()
+    h2d = 8 * len(abi.STATE_FIELDS) * ngbxs
+    d2h = 16 * ngbxs
+    # keep the current thermodynamics: read back and re-send it each step
+    lib.cleo_b200_download_state(ctx, C.byref(st_struct))
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        rc = lib.cleo_b200_upload_state(ctx, C.byref(st_struct))
+        assert rc == 0
+        sdm.run_step(t * 100, (t + 1) * 100)
+        t += 1
+        rc = lib.cleo_b200_download_budgets(ctx, C.cast(cm_out.data_ptr(), C.POINTER(C.c_double)),
+                                            C.cast(it_out.data_ptr(), C.POINTER(C.c_uint64)))
+        assert rc == 0
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    ms_e2e = e0.elapsed_time(e1)
+    sdm.check()
+
+    # ---- max over ranks ----
+    vals = torch.tensor([ms, ms_e2e, float(nsd), stage_ms["microphysics"]], dtype=torch.float64,
+                        device="cuda")
+    if dist is not None:
+        mx = vals.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = vals.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms, ms_e2e = float(mx[0]), float(mx[1])
+        total_sd = float(sm[2])
+    else:
+        total_sd = float(nsd)
+    value = total_sd * args.steps / (ms / 1000.0)
+    e2e = total_sd * args.steps / (ms_e2e / 1000.0)
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        micro_ms = stage_ms["microphysics"]
+        bytes_micro = MICRO_BYTES_PER_SD * nsd + MICRO_BYTES_PER_GBX * ngbxs
+        achieved = bytes_micro / (micro_ms / 1000.0) / 1e9 if micro_ms > 0 else None
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "k_micro_traffic.json")
+        if os.path.exists(tp):
+            with open(tp) as f:
+                tj = json.load(f)
+            traffic = tj["bytes_per_sd"] * nsd + tj.get("bytes_per_gbx", 0.0) * ngbxs
+        lc, lprefix, lref, lcores = reference_lib()
+        cpu_value, cpu_nsd, cpu_dt = cpu_sample(1, 1, lc, lprefix)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "ndims": list(ndims), "ngbxs_per_gpu": ngbxs,
+                       "superdroplets_per_gpu": nsd, "path": "plain (one CTA per gridbox)",
+                       "l2": "inputs larger than L2 (2.4 GB SoA per GPU), no flush"},
+            "roofline": {"bound": "hbm", "kernel": "k_micro", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "bytes_per_launch": bytes_micro, "ms_per_launch": micro_ms},
+            "cpu_baseline": {"value": cpu_value, "unit": UNIT, "cores": lcores, "kind": lref,
+                             "sample": f"64x16x16 gridboxes of the workload ({cpu_nsd} "
+                                       f"superdroplets), 1 step after 1 warm-up"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(l1.value - l0.value),
+            "clocks": clocks,
+            "stages_ms_per_step": stage_ms,
+        }
+        print(json.dumps(out), flush=True)
+    sdm.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ndims", default=",".join(str(n) for n in NDIMS))
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

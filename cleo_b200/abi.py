@@ -216,7 +216,8 @@ EXPORTED = (
     "cleo_b200_create", "cleo_b200_destroy", "cleo_b200_upload_supers", "cleo_b200_upload_state",
     "cleo_b200_step", "cleo_b200_status", "cleo_b200_domain_nsupers", "cleo_b200_download_supers",
     "cleo_b200_download_state", "cleo_b200_download_budgets", "cleo_b200_condensation_solve",
-    "cleo_b200_stream", "cleo_b200_version",
+    "cleo_b200_stream", "cleo_b200_kernel_launches", "cleo_b200_set_profiling",
+    "cleo_b200_stage_times", "cleo_b200_version",
 )
 
 _LIB = None
@@ -241,6 +242,12 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
     lib.cleo_b200_condensation_solve.restype = C.c_int
     lib.cleo_b200_stream.argtypes = [vp]
     lib.cleo_b200_stream.restype = vp
+    lib.cleo_b200_kernel_launches.argtypes = [vp, C.POINTER(C.c_uint64)]
+    lib.cleo_b200_kernel_launches.restype = C.c_int
+    lib.cleo_b200_set_profiling.argtypes = [vp, C.c_int]
+    lib.cleo_b200_set_profiling.restype = C.c_int
+    lib.cleo_b200_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
+    lib.cleo_b200_stage_times.restype = C.c_int
     lib.cleo_b200_version.argtypes = []
     lib.cleo_b200_version.restype = C.c_char_p
     if path is None:

@@ -10,6 +10,7 @@
 
 #include "../../include/cleo_b200.h"
 #include "../../include/cleo_b200_rng.h"
+#include "ddmath.h"
 
 namespace cleo {
 
@@ -82,7 +83,7 @@ struct Where {
 __device__ __forceinline__ double dryradius(double msol) {  // :227-231
   const double vconst = 3.0 / (4.0 * PI);
   const double dryrcubed = vconst * msol / Rho_sol;
-  return pow(dryrcubed, 1.0 / 3.0);
+  return dpow(dryrcubed, 1.0 / 3.0);
 }
 __device__ __forceinline__ double rcubed(double r) { return r * r * r; }       // :238
 __device__ __forceinline__ double vol(double r) { return 4.0 / 3.0 * PI * rcubed(r); }  // :247
@@ -119,9 +120,9 @@ __device__ __forceinline__ double tv_simmel(double radius) {  // :57-85
   if (radius >= r3) return a4;
   const double massconst = 4.0 / 3.0 * PI * Rho_l;  // watermass :32-40
   const double MASS = (massconst * radius * radius * radius) * MASS0grams;
-  if (radius >= r2) return a3 * pow(MASS, 1.0 / 6.0);
-  if (radius >= r1) return a2 * pow(MASS, 1.0 / 3.0);
-  return a1 * pow(MASS, 2.0 / 3.0);
+  if (radius >= r2) return a3 * dpow(MASS, 1.0 / 6.0);
+  if (radius >= r1) return a2 * dpow(MASS, 1.0 / 3.0);
+  return a1 * dpow(MASS, 2.0 / 3.0);
 }
 __device__ __forceinline__ double tv_rogersyau(double radius) {  // :95-117
   const double r1 = 3e-5 / R0;
@@ -131,9 +132,9 @@ __device__ __forceinline__ double tv_rogersyau(double radius) {  // :95-117
   const double k2 = 8000 * R0 / W0;
   const double k3 = 201 / W0;
   const double k4 = 9 / W0;
-  if (radius < r1) return k1 * pow(radius, 2.0);
+  if (radius < r1) return k1 * dpow(radius, 2.0);
   if (radius < r2) return k2 * radius;
-  if (radius < r3) return k3 * pow((radius * R0), 0.5);
+  if (radius < r3) return k3 * dpow((radius * R0), 0.5);
   return k4;
 }
 __device__ __forceinline__ double tv_rogersgk(double radius) {  // :127-147
@@ -144,10 +145,10 @@ __device__ __forceinline__ double tv_rogersgk(double radius) {  // :127-147
   const double bcaps = 10.43 / W0;
   const double ccaps = -1.0 * 2.0 * 0.6 * 1000 * R0;
   if (radius < radius0) {
-    const double term = 1.0 - exp(smallk * radius);
+    const double term = 1.0 - dexp(smallk * radius);
     return term * kcaps * radius;
   }
-  return acaps - bcaps * exp(ccaps * radius);
+  return acaps - bcaps * dexp(ccaps * radius);
 }
 __device__ __forceinline__ double terminalv(int kind, double radius) {
   switch (kind) {
@@ -214,14 +215,14 @@ __device__ __forceinline__ double coal_surfenergy(double r1, double r2) {
   const double r1cubed = r1 * r1 * r1;
   const double r2cubed = r2 * r2 * r2;
   const double rcubedsum = r1cubed + r2cubed;
-  return surfconst * pow(rcubedsum, 2.0 / 3.0);
+  return surfconst * dpow(rcubedsum, 2.0 / 3.0);
 }
 __device__ __forceinline__ double surfenergy(double radius) { return surfconst * (radius * radius); }
 __device__ __forceinline__ double ecoal_straub2010(double r1, double r2, double cke) {
   const double beta = -1.15;
   const double surf_c = coal_surfenergy(r1, r2);
   const double weber = cke / surf_c;
-  return exp(beta * weber);
+  return dexp(beta * weber);
 }
 __device__ __forceinline__ double nfrags_of(const cleo_b200_params& p, double r1, double r2) {
   if (p.nfrags_kind == CLEO_NFRAGS_CONST) return p.nfrags;  // breakup_nfrags.hpp:40-50
@@ -232,7 +233,7 @@ __device__ __forceinline__ double nfrags_of(const cleo_b200_params& p, double r1
   const double cke = collision_kinetic_energy(r1, r2, terminalv(p.nfrags_tv, r1),
                                               terminalv(p.nfrags_tv, r2));
   const double cke_cap = fmin(ckemax, cke);
-  const double gamma = pow(cke_cap * 1e6, beta);
+  const double gamma = dpow(cke_cap * 1e6, beta);
   return 1.0 / (alpha - gamma) + epsilon;
 }
 __device__ __forceinline__ unsigned coalbure_flag(const cleo_b200_params& p, double phi, double r1,
@@ -282,7 +283,7 @@ __device__ __forceinline__ void twin_coalescence(uint64_t gamma, Drop& d1, Drop&
   const uint64_t new_xi = old_xi / 2;
   if (new_xi >= old_xi) w.fail(CLEO_ERR_COALESCENCE);
   const double new_rcubed = rcubed(d2.r) + (double)gamma * rcubed(d1.r);
-  const double new_r = pow(new_rcubed, (1.0 / 3.0));
+  const double new_r = dpow(new_rcubed, (1.0 / 3.0));
   const double new_msol = d2.msol + (double)gamma * d1.msol;
   if (new_xi == 0) {
     d1.xi = 0;  // set_null
@@ -307,7 +308,7 @@ __device__ __forceinline__ void different_coalescence(uint64_t gamma, Drop& d1, 
   check_xi(new_xi, w);
   d1.xi = new_xi;
   const double new_rcubed = rcubed(d2.r) + (double)gamma * rcubed(d1.r);
-  const double nr = pow(new_rcubed, (1.0 / 3.0));
+  const double nr = dpow(new_rcubed, (1.0 / 3.0));
   check_radius(nr, d2.msol, w);
   d2.r = nr;
   d2.msol = d2.msol + (double)gamma * d1.msol;
@@ -338,7 +339,7 @@ __device__ __forceinline__ void twin_breakup(const cleo_b200_params& p, Drop& d1
   if (new_xitot <= (old_xi * 2)) w.fail(CLEO_ERR_BREAKUP);
   const double sum_rcubed = rcubed(d1.r) + rcubed(d2.r);
   const double new_rcubed = sum_rcubed * (double)old_xi / (double)new_xitot;
-  const double new_r = pow(new_rcubed, (1.0 / 3.0));
+  const double new_r = dpow(new_rcubed, (1.0 / 3.0));
   const double sum_msol = d1.msol + d2.msol;
   const double new_msol = sum_msol * (double)old_xi / (double)new_xitot;
   check_xi(new_xi1, w);
@@ -366,7 +367,7 @@ __device__ __forceinline__ void different_breakup(const cleo_b200_params& p, Dro
   if ((new_xi1 + new_xi2) <= (old_xi1 + old_xi2)) w.fail(CLEO_ERR_BREAKUP);
   const double sum_rcubed = rcubed(d1.r) + rcubed(d2.r);
   const double new_rcubed = sum_rcubed * (double)old_xi2 / (double)new_xi2;
-  const double new_r = pow(new_rcubed, (1.0 / 3.0));
+  const double new_r = dpow(new_rcubed, (1.0 / 3.0));
   const double sum_msol = d1.msol + d2.msol;
   const double new_msol = sum_msol * (double)old_xi2 / (double)new_xi2;
   check_xi(new_xi2, w);
@@ -426,7 +427,7 @@ __device__ __forceinline__ double saturation_pressure(double temp, const Where& 
   const double TREF = 273.16;
   const double PREF = 611.655;
   const double T = temp * TEMP0;
-  return (PREF * exp(A * (T - TREF) / (T - B))) / P0;
+  return (PREF * dexp(A * (T - TREF) / (T - B))) / P0;
 }
 __device__ __forceinline__ double diffusion_factor(double press, double temp, double psat) {
   const double A = 7.11756e-5;
@@ -436,8 +437,8 @@ __device__ __forceinline__ double diffusion_factor(double press, double temp, do
   const double TEMP = temp * TEMP0;
   const double PRESS = press * P0;
   const double PSAT = psat * P0;
-  const double THERMK = A * pow(TEMP, 2.0) + TEMP * B;
-  const double DIFFUSE_V = (D / PRESS * pow(TEMP, 1.94)) / DC_RGAS_V;
+  const double THERMK = A * dpow(TEMP, 2.0) + TEMP * B;
+  const double DIFFUSE_V = (D / PRESS * dpow(TEMP, 1.94)) / DC_RGAS_V;
   const double fkl = (LATENT_RGAS_V / TEMP - 1.0) * DC_LATENT_V / (THERMK * F0);
   const double fdl = TEMP / (DIFFUSE_V * PSAT) / F0;
   return Rho_l * (fkl + fdl);
@@ -448,8 +449,8 @@ __device__ __forceinline__ double ventilation_factor(double radius) {
   const double A = 1.963;
   const double C2 = 1.069e+3;
   const double B = 0.702;
-  const double a = 1.0 / (C1 * pow(radius * R0, A));
-  const double b = 1.0 / (C2 * pow(radius * R0, B));
+  const double a = 1.0 / (C1 * dpow(radius * R0, A));
+  const double b = 1.0 / (C2 * dpow(radius * R0, B));
   const double vent_factor = 1.0 + 1.0 / (a + b);
   return fmin(vent_factor, vent_factor_max);
 }
@@ -477,15 +478,15 @@ constexpr uint32_t NR_ITER_CAP = 4u << 20;
 __device__ __forceinline__ double ode_gfunc(const OdeConsts& o, double subdelt, double rprev,
                                             double rsqrd) {  // :270-281
   const double radius = sqrt(rsqrd);
-  const double alpha = o.s_ratio - 1 - o.akoh / radius + o.bkoh / pow(radius, 3.0);
+  const double alpha = o.s_ratio - 1 - o.akoh / radius + o.bkoh / dpow(radius, 3.0);
   const double beta = 2.0 * subdelt / (rsqrd * o.ffactor_fv);
-  const double gamma = pow(rprev / radius, 2.0);
+  const double gamma = dpow(rprev / radius, 2.0);
   return 1 - gamma - alpha * beta;
 }
 __device__ __forceinline__ double ode_gfuncderivative(const OdeConsts& o, double subdelt,
                                                       double rsqrd) {  // :291-301
   const double radius = sqrt(rsqrd);
-  const double alpha = o.akoh / radius - 3.0 * o.bkoh / pow(radius, 3.0);
+  const double alpha = o.akoh / radius - 3.0 * o.bkoh / dpow(radius, 3.0);
   const double beta = subdelt / (rsqrd * o.ffactor_fv);
   return 1 - alpha * beta;
 }
@@ -530,7 +531,7 @@ __device__ __forceinline__ double integrate_ode(const NewtonCfg& c, const OdeCon
   return z;
 }
 __device__ __forceinline__ double initialguess(const OdeConsts& o, double rprev) {  // :156-170
-  const double s_act = 1 + sqrt(4.0 * pow(o.akoh, 3.0) / 27 / o.bkoh);
+  const double s_act = 1 + sqrt(4.0 * dpow(o.akoh, 3.0) / 27 / o.bkoh);
   if (o.s_ratio > s_act) {
     const double bigr = 1e-3 / R0;
     const double maxradius = fmax(bigr, rprev);
@@ -546,11 +547,11 @@ __device__ __forceinline__ bool first_unique_criteria(const OdeConsts& o, double
   const bool is_ziter_unactivated = ziter < rcritsqrd;
   const bool is_unactivated = (rprev * rprev < rcritsqrd && is_ziter_unactivated);
   const double sqrdval = 4.0 * akoh * akoh * akoh / 27.0 / bkoh;
-  const bool is_subactivated_saturation = (o.s_ratio <= 1.0 + pow(sqrdval, 0.5));
+  const bool is_subactivated_saturation = (o.s_ratio <= 1.0 + dpow(sqrdval, 0.5));
   return (is_unactivated && is_subactivated_saturation);
 }
 __device__ __forceinline__ double critical_timestep(const OdeConsts& o) {  // hpp:266-269
-  const double cuberoot = pow(5.0 * o.bkoh / o.akoh, 1.5);
+  const double cuberoot = dpow(5.0 * o.bkoh / o.akoh, 1.5);
   return 2.5 * o.ffactor_fv / o.akoh * cuberoot;
 }
 // solve_condensation: impliciteuler.cpp:35-54 (+ substepping :98-113). seed_rsqrd > 0 replaces
@@ -580,7 +581,7 @@ __device__ __forceinline__ double solve_condensation(const NewtonCfg& c, double 
       }
       const double subdelt = fmin(mindelt, remdelt);
       ziter = integrate_ode(c, o, subdelt, rprev, ziter, niters, w);
-      rprev = pow(ziter, 0.5);
+      rprev = dpow(ziter, 0.5);
       remdelt -= subdelt;
     }
     rsqrd = ziter;

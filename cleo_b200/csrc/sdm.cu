@@ -79,8 +79,49 @@ struct cleo_b200_ctx {
   // sort scratch
   uint32_t *keys[2], *vals[2], *hist, *tile_sums;
   uint32_t ntiles_max, key_bits;
+  unsigned long long launches = 0;  // kernels launched by this context
   std::vector<void*> allocs;
+  // stage timing: (stage, start, end) event triples recorded while profiling is on
+  bool profiling = false;
+  struct Mark {
+    int stage;
+    cudaEvent_t a, b;
+  };
+  std::vector<Mark> marks;
+  std::vector<cudaEvent_t> event_pool;
+  cudaEvent_t take_event() {
+    if (!event_pool.empty()) {
+      cudaEvent_t e = event_pool.back();
+      event_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
 };
+
+namespace {
+// RAII stage marker: records an event pair around a stage when profiling is on
+struct StageMark {
+  cleo_b200_ctx* x;
+  int stage;
+  cudaEvent_t a = nullptr;
+  StageMark(cleo_b200_ctx* x_, int st) : x(x_), stage(st) {
+    if (x->profiling) {
+      a = x->take_event();
+      cudaEventRecord(a, x->stream);
+    }
+  }
+  ~StageMark() {
+    if (x->profiling && a) {
+      cudaEvent_t b = x->take_event();
+      cudaEventRecord(b, x->stream);
+      x->marks.push_back({stage, a, b});
+    }
+  }
+};
+}  // namespace
 
 #define CUDA_TRY(expr)                                          \
   do {                                                          \
@@ -629,6 +670,7 @@ int sort_current(cleo_b200_ctx* x) {
     k_scan_add<<<(unsigned)((nh + 255) / 256), 256, 0, s>>>(x->hist, nh, x->tile_sums);
     k_rs_downsweep<<<nt, RS_THREADS, 0, s>>>(kin, vin, d.counters, (int)shift, x->hist, nt, kout,
                                              vout);
+    x->launches += 5;
     std::swap(kin, kout);
     std::swap(vin, vout);
   }
@@ -642,6 +684,7 @@ int sort_current(cleo_b200_ctx* x) {
   k_counts<<<grid_for(d.ngbxs, 256), 256, 0, s>>>(d);
   k_to_grave<<<grid_for(d.capacity, 256), 256, 0, s>>>(d);
   k_grave_commit<<<1, 1, 0, s>>>(d);
+  x->launches += 5;
   CUDA_TRY(cudaGetLastError());
   return CLEO_OK;
 }
@@ -651,15 +694,23 @@ int run_sdm_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
   cudaStream_t s = x->stream;
   const bool did_motion = on_step(d.p.motionstep, t_sdm);
   if (did_motion) {
-    k_motion<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, x->keys[0], x->vals[0]);
+    {
+      StageMark m(x, 0);
+      k_motion<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, x->keys[0], x->vals[0]);
+      x->launches += 1;
+    }
+    StageMark m(x, 1);
     const int rc = sort_current(x);
     if (rc) return rc;
   }
   const bool micro = (d.p.condstep != CLEO_STEP_OFF || d.p.collstep != CLEO_STEP_OFF);
   if (micro || did_motion) {
     const uint32_t blocks = d.ngbxs < (1u << 30) ? d.ngbxs : (1u << 30);
-    if (blocks > 0)
+    if (blocks > 0) {
+      StageMark m(x, 2);
       k_micro<<<blocks, MICRO_THREADS, MICRO_SMEM, s>>>(d, t_sdm, t_sdm_next, did_motion ? 1 : 0);
+      x->launches += 1;
+    }
   }
   CUDA_TRY(cudaGetLastError());
   return CLEO_OK;
@@ -769,12 +820,48 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
 void cleo_b200_destroy(cleo_b200_ctx* x) {
   if (!x) return;
   if (x->stream) cudaStreamSynchronize(x->stream);
+  for (auto& m : x->marks) {
+    cudaEventDestroy(m.a);
+    cudaEventDestroy(m.b);
+  }
+  for (auto e : x->event_pool) cudaEventDestroy(e);
   for (void* p : x->allocs) cudaFree(p);
   if (x->own_stream && x->stream) cudaStreamDestroy(x->stream);
   delete x;
 }
 
 void* cleo_b200_stream(cleo_b200_ctx* x) { return x ? (void*)x->stream : nullptr; }
+
+int cleo_b200_set_profiling(cleo_b200_ctx* x, int enable) {
+  if (!x) return CLEO_ERR_ARGUMENT;
+  x->profiling = enable != 0;
+  return CLEO_OK;
+}
+
+int cleo_b200_stage_times(cleo_b200_ctx* x, double ms[3], uint64_t count[3]) {
+  if (!x || !ms || !count) return CLEO_ERR_ARGUMENT;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  for (int k = 0; k < 3; ++k) {
+    ms[k] = 0.0;
+    count[k] = 0;
+  }
+  for (auto& m : x->marks) {
+    float t = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&t, m.a, m.b));
+    ms[m.stage] += t;
+    count[m.stage] += 1;
+    x->event_pool.push_back(m.a);
+    x->event_pool.push_back(m.b);
+  }
+  x->marks.clear();
+  return CLEO_OK;
+}
+
+int cleo_b200_kernel_launches(cleo_b200_ctx* x, uint64_t* n) {
+  if (!x || !n) return CLEO_ERR_ARGUMENT;
+  *n = x->launches;
+  return CLEO_OK;
+}
 
 int cleo_b200_upload_supers(cleo_b200_ctx* x, const cleo_b200_supers* h, size_t n) {
   if (!x || !h) return CLEO_ERR_ARGUMENT;
@@ -801,6 +888,7 @@ int cleo_b200_upload_supers(cleo_b200_ctx* x, const cleo_b200_supers* h, size_t 
   const uint32_t cnt[4] = {(uint32_t)n, 0, 0, 0};
   CUDA_TRY(cudaMemcpyAsync(x->d.counters, cnt, 16, cudaMemcpyHostToDevice, s));
   k_keys_from_gbx<<<grid_for(x->d.capacity, 256), 256, 0, s>>>(x->d, x->keys[0], x->vals[0]);
+  x->launches += 1;
   const int rc = sort_current(x);  // SupersInDomain ctor: supersindomain.hpp:55-62
   if (rc) return rc;
   CUDA_TRY(cudaStreamSynchronize(s));
@@ -951,6 +1039,7 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_rad
   k_condsolve<<<grid_for(n, 128), 128, 0, x->stream>>>(x->d, (uint32_t)n, d_radius, d_msol, d_temp,
                                                        d_press, d_s_ratio, d_delt, d_radius_out,
                                                        d_niters_out);
+  x->launches += 1;
   CUDA_TRY(cudaGetLastError());
   return CLEO_OK;
 }

@@ -47,29 +47,52 @@ def msol_from_dryradius(rdry):
     return rdry ** 3 * (4.0 * math.pi / 3.0) * Rho_sol
 
 
-def equilibrium_radius(rdry, msol, s_ratio, temp):
+def equilibrium_radius(rdry, msol, s_ratio, temp, iters=44):
     """Stable Kohler equilibrium radius below the critical radius for saturation ratio s.
 
     Solves s - 1 - a/r + b/r^3 = 0 on (r_dry, r_crit] by bisection; supersaturations above the
     critical one are capped just below it, so every droplet starts unactivated.
     """
     a, b = kohler_ab(msol, temp)
+    a = np.broadcast_to(a, rdry.shape)
     rcrit = np.sqrt(3.0 * b / a)
     scrit = 1.0 + np.sqrt(4.0 * a ** 3 / (27.0 * b))
-    s = np.minimum(s_ratio, 1.0 + 0.999 * (scrit - 1.0))
+    sm1 = np.minimum(s_ratio, 1.0 + 0.999 * (scrit - 1.0)) - 1.0
     lo = np.maximum(rdry * (1.0 + 1e-9), 1e-12)
     hi = np.maximum(rcrit, lo)
-
-    def f(r):
-        return s - 1.0 - a / r + b / r ** 3
-
-    for _ in range(80):
-        mid = 0.5 * (lo + hi)
-        fm = f(mid)
-        # f decreases on (r_dry, r_crit): f > 0 means the root lies above mid
-        go_up = fm > 0.0
-        lo = np.where(go_up, mid, lo)
-        hi = np.where(go_up, hi, mid)
+    if lo.size > 1_000_000:
+        try:  # same IEEE element-wise arithmetic, spread over the host cores
+            import torch
+            T = {k: torch.from_numpy(np.array(v, dtype=np.float64, copy=True))
+                 for k, v in (("a", a), ("b", np.broadcast_to(b, lo.shape)), ("sm1", sm1),
+                              ("lo", lo), ("hi", hi))}
+            lo_t, hi_t = T["lo"].clone(), T["hi"].clone()
+            for _ in range(iters):
+                mid = (lo_t + hi_t) * 0.5
+                f = (T["b"] / (mid * mid * mid) - T["a"] / mid) + T["sm1"]
+                up = f > 0.0
+                lo_t = torch.where(up, mid, lo_t)
+                hi_t = torch.where(up, hi_t, mid)
+            return np.maximum(((lo_t + hi_t) * 0.5).numpy(), rdry)
+        except ImportError:
+            pass
+    mid = np.empty_like(lo)
+    f = np.empty_like(lo)
+    tmp = np.empty_like(lo)
+    up = np.empty(lo.shape, dtype=bool)
+    for _ in range(iters):
+        np.add(lo, hi, out=mid)
+        mid *= 0.5
+        np.divide(a, mid, out=f)          # a/r
+        np.multiply(mid, mid, out=tmp)
+        tmp *= mid                        # r^3
+        np.divide(b, tmp, out=tmp)        # b/r^3
+        np.subtract(tmp, f, out=f)
+        f += sm1                          # f = s - 1 - a/r + b/r^3, decreasing on (r_dry, r_crit)
+        np.greater(f, 0.0, out=up)
+        np.copyto(lo, mid, where=up)
+        np.logical_not(up, out=up)
+        np.copyto(hi, mid, where=up)
     r = 0.5 * (lo + hi)
     return np.maximum(r, rdry)
 

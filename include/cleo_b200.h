@@ -232,6 +232,20 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* ctx, size_t n, const double* d_r
 /* The CUDA stream the context enqueues on (cudaStream_t, as void*). */
 void* cleo_b200_stream(cleo_b200_ctx* ctx);
 
+/* Number of kernels the context has launched since it was created (for launch accounting). */
+int cleo_b200_kernel_launches(cleo_b200_ctx* ctx, uint64_t* n);
+
+/*
+ * Per-stage device timing with CUDA events on the context's stream, the counterpart of the
+ * reference's Kokkos profiling regions (sdm_movement_*, timestep_sdm_microphysics;
+ * libs/gridboxes/movesupersindomain.hpp:190-261, libs/runcleo/sdmmethods.hpp:159-216).
+ * cleo_b200_set_profiling(ctx, 1) starts recording; cleo_b200_stage_times synchronises, returns
+ * the summed milliseconds and launch counts of the stages {motion, sort, microphysics} since the
+ * last call, and resets them.
+ */
+int cleo_b200_set_profiling(cleo_b200_ctx* ctx, int enable);
+int cleo_b200_stage_times(cleo_b200_ctx* ctx, double ms[3], uint64_t count[3]);
+
 /* Library version string. */
 const char* cleo_b200_version(void);
 

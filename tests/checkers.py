@@ -119,7 +119,9 @@ def assert_same_domain(a: dict, b: dict, rtol=1e-12, what=""):
         if k.startswith("coord"):
             ok |= err <= 1e-15  # coordinates near zero
         bad = np.nonzero(~ok)[0]
-        assert bad.size == 0, (what, k, bad[:10], x[bad[:5]], y[bad[:5]])
+        rel = err / np.maximum(scale, 1e-300)
+        assert bad.size == 0, (what, k, f"{bad.size} of {nd} beyond rtol; max rel {rel.max():.3e}",
+                               bad[:10], x[bad[:5]], y[bad[:5]])
     ia = np.sort(a["sdid"][nd:])
     ib = np.sort(b["sdid"][nd:])
     assert np.array_equal(ia, ib), (what, "oob ids differ")

@@ -13,13 +13,22 @@ import pytest
 
 import checkers as K
 from cleo_b200 import abi, workloads as W
-from cleo_b200.config import make_params
+from cleo_b200.config import Rho_l, make_params
 from cleo_b200.sdm import CleoError, make_sdm
 from test_oracle import ERRS, VARIANTS, _err_case, golovin_l1
 
 pytestmark = pytest.mark.gpu
 
 RTOL = 1e-12
+
+
+def budget_close(got, exp, what=""):
+    """The cumulative condensed mass per gridbox is a sum of differences of nearly equal masses
+    (and keeps the contributions of droplets that have since left), so it is compared relative to
+    the largest budget of the domain, not element-wise."""
+    scale = float(np.max(np.abs(exp))) if len(exp) else 0.0
+    err = np.abs(got - exp)
+    assert np.all(err <= 1e-12 * scale + 1e-300), (what, float(np.max(err)) / max(scale, 1e-300))
 
 
 @pytest.fixture(scope="module")
@@ -51,7 +60,7 @@ def test_gpu_matches_golden(lib, fname):
     st = g.download_state()
     for f in abi.STATE_FIELDS:
         assert K.max_rel(st[f], exp["state"][f]) <= RTOL, (fname, f)
-    assert K.max_rel(g.download_budgets()[0], exp["cond_mass"]) <= 1e-11
+    budget_close(g.download_budgets()[0], exp["cond_mass"], fname)
 
 
 @pytest.mark.parametrize("name,build,nsteps", VARIANTS, ids=[v[0] for v in VARIANTS])
@@ -64,7 +73,7 @@ def test_gpu_matches_oracle_variants(lib, name, build, nsteps):
         assert K.max_rel(sg[f], so[f]) <= RTOL, (name, f)
     cg, ig = g.download_budgets()
     co, io = o.download_budgets()
-    assert K.max_rel(cg, co) <= 1e-11
+    budget_close(cg, co, name)
     assert np.array_equal(ig, io), (name, "newton iteration counts")
 
 
@@ -74,8 +83,7 @@ def test_gpu_condensation_solve(lib, tol):
     mx, rt, at = tol
     p = make_params(condtstep=1.0, maxniters=mx, rtol=rt, atol=at)
     w = W.condsolve(50000, seed=13)
-    rc, ro, io = K.condsolve(K.oracle_lib(), "oc", p, w)
-    assert rc == 0
+    rc_o, ro, io = K.condsolve(K.oracle_lib(), "oc", p, w)
     grid = W.cartesian_grid((1, 1, 1), (1.0, 1.0, 1.0), nspacedims=0)
     from cleo_b200.sdm import SDM
     s = SDM(p, grid, 1, lib=lib)
@@ -89,7 +97,8 @@ def test_gpu_condensation_solve(lib, tol):
                                    ("radius", "msol", "temp", "press", "s_ratio", "delt")],
         C.c_void_p(out.data_ptr()), C.c_void_p(nit.data_ptr()))
     assert rc == 0
-    s.check()
+    err = s.status()
+    assert err.code == rc_o, (err.code, rc_o)  # same abort site (e.g. NR non-convergence)
     rg = out.cpu().numpy()
     assert K.max_rel(rg, ro) <= RTOL
     assert np.array_equal(nit.cpu().numpy().astype(np.uint32), io)
