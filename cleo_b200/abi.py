@@ -217,7 +217,7 @@ EXPORTED = (
     "cleo_b200_step", "cleo_b200_status", "cleo_b200_domain_nsupers", "cleo_b200_download_supers",
     "cleo_b200_download_state", "cleo_b200_download_budgets", "cleo_b200_condensation_solve",
     "cleo_b200_stream", "cleo_b200_kernel_launches", "cleo_b200_set_profiling",
-    "cleo_b200_stage_times", "cleo_b200_version",
+    "cleo_b200_stage_times", "cleo_b200_sort_by_gridbox_static", "cleo_b200_version",
 )
 
 _LIB = None
@@ -248,6 +248,8 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
     lib.cleo_b200_set_profiling.restype = C.c_int
     lib.cleo_b200_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
     lib.cleo_b200_stage_times.restype = C.c_int
+    lib.cleo_b200_sort_by_gridbox_static.argtypes = [vp, C.c_uint32, C.c_uint32, vp, vp, vp]
+    lib.cleo_b200_sort_by_gridbox_static.restype = C.c_int
     lib.cleo_b200_version.argtypes = []
     lib.cleo_b200_version.restype = C.c_char_p
     if path is None:

@@ -246,6 +246,28 @@ int cleo_b200_kernel_launches(cleo_b200_ctx* ctx, uint64_t* n);
 int cleo_b200_set_profiling(cleo_b200_ctx* ctx, int enable);
 int cleo_b200_stage_times(cleo_b200_ctx* ctx, double ms[3], uint64_t count[3]);
 
+/*
+ * Stable sort of superdroplets by gridbox index that allocates no device memory. No counterpart in
+ * the reference: it is for callers that cannot call cudaMalloc while they run (a host model that
+ * reserves all device memory at start-up and forbids allocation in its time loop, where an
+ * allocation would also synchronise the device, or a caller whose memory belongs to another
+ * framework's pool). It computes what the context's sort computes (sortsupers.hpp:93-226
+ * semantics: keys above ngbxs share the last bucket) with scratch held in a file-scope device
+ * array of about 16.3 MiB, which every GPU that loads the library keeps until the process exits.
+ *   d_sdgbxindex  n gridbox indices (device memory)
+ *   d_order       out: n positions, d_order[j] = position of the j-th superdroplet in sorted order
+ *   d_gstart      out, may be NULL: ngbxs + 2 entries, the first sorted position of each gridbox
+ *                 (entry ngbxs = number of in-domain superdroplets, entry ngbxs + 1 = n)
+ *   stream        cudaStream_t to enqueue on (as void*; NULL = default stream)
+ * n must not exceed 1,048,576 (else CLEO_ERR_CAPACITY). The first call on a device looks up the
+ * scratch array's device address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture. All calls share the one scratch array, so calls whose work
+ * overlaps on the GPU (e.g. on two streams at once) race; each call writes every scratch word it
+ * reads, so nothing needs clearing between calls. Asynchronous on `stream`.
+ */
+int cleo_b200_sort_by_gridbox_static(const uint32_t* d_sdgbxindex, uint32_t n, uint32_t ngbxs,
+                                     uint32_t* d_order, uint32_t* d_gstart, void* stream);
+
 /* Library version string. */
 const char* cleo_b200_version(void);
 
