@@ -40,11 +40,15 @@ NDIMS = (64, 128, 128)
 WORKLOAD = ("uneven3d: 64x128x128 gridboxes of 50 m^3, lognormal counts (median 32, sigma 0.586, "
             "clip 0..2048), ~40M superdroplets; condensation + Long CoalBuRe(ConstNFrags 5, "
             "Straub) + sedimentation (RogersGK), 1 s steps")
-# algorithmic bytes of one k_micro launch: per superdroplet read r, msol, xi, coord3/1/2, id
-# (56 B) and write them back permuted plus sdgbxindex (60 B); per gridbox read volume, press,
-# temp, qvap and write qcond, cond_mass, nr_iters (56 B)
-MICRO_BYTES_PER_SD = 116
-MICRO_BYTES_PER_GBX = 56
+# Algorithmic bytes per launch of the batched kernel groups (each field read once, written once):
+# condensation: per superdroplet read r, msol, xi, sdgbxindex (28 B), write r, dm, its (20 B);
+#   per gridbox read temp, press, qvap, write th_s, th_ff (40 B)
+# collisions: per superdroplet read r, msol, xi, coord3/1/2, id, dm, its (68 B), write the 8
+#   permuted fields (60 B); per gridbox state, budgets, slot, bucket entry (64 B)
+COND_BYTES_PER_SD = 48
+COND_BYTES_PER_GBX = 40
+COLL_BYTES_PER_SD = 128
+COLL_BYTES_PER_GBX = 64
 
 
 def peaks():
@@ -155,6 +159,81 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def measure(lib, wl, mode, steps, warmup, dist, local, e2e=False):
+    """Device-timed steps of one schedule (and optionally the end-to-end loop) on one context."""
+    import torch
+    wl["params"].exec_mode = mode
+    sdm = make_sdm(wl, lib=lib)
+    ctx = sdm.ctx
+    stream = torch.cuda.ExternalStream(lib.cleo_b200_stream(ctx))
+    ngbxs = int(wl["grid"]["ngbxs"])
+    t = 0
+    for _ in range(warmup):
+        sdm.run_step(t * 100, (t + 1) * 100)
+        t += 1
+    sdm.check()
+    nd = C.c_size_t()
+    lib.cleo_b200_domain_nsupers(ctx, C.byref(nd))
+    nsd = int(nd.value)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    lib.cleo_b200_set_profiling(ctx, 1)
+    ms5, cnt5 = (C.c_double * 5)(), (C.c_uint64 * 5)()
+    lib.cleo_b200_stage_times(ctx, ms5, cnt5)  # reset
+    l0 = C.c_uint64()
+    lib.cleo_b200_kernel_launches(ctx, C.byref(l0))
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(steps):
+            sdm.run_step(t * 100, (t + 1) * 100)
+            t += 1
+        ev1.record(stream)
+        ev1.synchronize()
+    barrier()
+    l1 = C.c_uint64()
+    lib.cleo_b200_kernel_launches(ctx, C.byref(l1))
+    lib.cleo_b200_stage_times(ctx, ms5, cnt5)
+    lib.cleo_b200_set_profiling(ctx, 0)
+    sdm.check()
+    names = ("motion", "sort", "microphysics", "condensation", "collisions")
+    out = {"ms": ev0.elapsed_time(ev1), "nsd": nsd, "ngbxs": ngbxs,
+           "stage_ms": {k: ms5[i] / steps for i, k in enumerate(names)},
+           "launches": int(l1.value - l0.value), "clocks": clk.summary()}
+    if e2e:
+        # end-to-end through the public API with pinned host buffers: per step the gridbox
+        # states go host->device and the condensed-mass budget comes back
+        pinned = {f: torch.from_numpy(wl["state"][f].copy()).pin_memory() for f in abi.STATE_FIELDS}
+        st_struct = abi.state_struct({f: pinned[f].numpy() for f in abi.STATE_FIELDS})
+        cm_out = torch.empty(ngbxs, dtype=torch.float64).pin_memory()
+        it_out = torch.empty(ngbxs, dtype=torch.int64).pin_memory()
+        lib.cleo_b200_download_state(ctx, C.byref(st_struct))
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            assert lib.cleo_b200_upload_state(ctx, C.byref(st_struct)) == 0
+            sdm.run_step(t * 100, (t + 1) * 100)
+            t += 1
+            assert lib.cleo_b200_download_budgets(
+                ctx, C.cast(cm_out.data_ptr(), C.POINTER(C.c_double)),
+                C.cast(it_out.data_ptr(), C.POINTER(C.c_uint64))) == 0
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        out["ms_e2e"] = e0.elapsed_time(e1)
+        out["h2d"] = 8 * len(abi.STATE_FIELDS) * ngbxs
+        out["d2h"] = 16 * ngbxs
+        sdm.check()
+    sdm.close()
+    return out
+
+
 def run_ours(args):
     import torch
     rank = int(os.environ.get("RANK", "0"))
@@ -170,97 +249,34 @@ def run_ours(args):
     lib = abi.load_library()
     ndims = tuple(int(x) for x in args.ndims.split(","))
     wl = W.uneven3d(ndims=ndims, seed=3 + rank)  # one independent domain per rank (weak scaling)
-    sdm = make_sdm(wl, lib=lib)
-    ctx = sdm.ctx
-    stream = torch.cuda.ExternalStream(lib.cleo_b200_stream(ctx))
-    ngbxs = int(wl["grid"]["ngbxs"])
-    t = 0
-    for _ in range(args.warmup):
-        sdm.run_step(t * 100, (t + 1) * 100)
-        t += 1
-    sdm.check()
-    nd = C.c_size_t()
-    lib.cleo_b200_domain_nsupers(ctx, C.byref(nd))
-    nsd = int(nd.value)
+    plain_steps = max(2, min(args.steps, 5))
+    plain = measure(lib, wl, abi.EXEC_PLAIN, plain_steps, args.warmup, dist, local)
+    bat = measure(lib, wl, abi.EXEC_BATCHED, args.steps, args.warmup, dist, local, e2e=True)
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    # ---- device-timed region ----
-    lib.cleo_b200_set_profiling(ctx, 1)
-    ms3, cnt3 = (C.c_double * 3)(), (C.c_uint64 * 3)()
-    lib.cleo_b200_stage_times(ctx, ms3, cnt3)  # reset
-    l0 = C.c_uint64()
-    lib.cleo_b200_kernel_launches(ctx, C.byref(l0))
-    barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            sdm.run_step(t * 100, (t + 1) * 100)
-            t += 1
-        ev1.record(stream)
-        ev1.synchronize()
-    barrier()
-    clocks = clk.summary()
-    l1 = C.c_uint64()
-    lib.cleo_b200_kernel_launches(ctx, C.byref(l1))
-    lib.cleo_b200_stage_times(ctx, ms3, cnt3)
-    lib.cleo_b200_set_profiling(ctx, 0)
-    sdm.check()
-    ms = ev0.elapsed_time(ev1)
-    stage_ms = {k: ms3[i] / max(1, cnt3[i]) for i, k in enumerate(("motion", "sort", "microphysics"))}
-
-    # ---- end-to-end region through the public API with pinned host buffers ----
-    pinned = {f: torch.from_numpy(wl["state"][f]).pin_memory() for f in abi.STATE_FIELDS}
-    st_struct = abi.state_struct({f: pinned[f].numpy() for f in abi.STATE_FIELDS})
-    cm_out = torch.empty(ngbxs, dtype=torch.float64).pin_memory()
-    it_out = torch.empty(ngbxs, dtype=torch.int64).pin_memory()
-    h2d = 8 * len(abi.STATE_FIELDS) * ngbxs
-    d2h = 16 * ngbxs
-    # keep the current thermodynamics: read back and re-send it each step
-    lib.cleo_b200_download_state(ctx, C.byref(st_struct))
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        rc = lib.cleo_b200_upload_state(ctx, C.byref(st_struct))
-        assert rc == 0
-        sdm.run_step(t * 100, (t + 1) * 100)
-        t += 1
-        rc = lib.cleo_b200_download_budgets(ctx, C.cast(cm_out.data_ptr(), C.POINTER(C.c_double)),
-                                            C.cast(it_out.data_ptr(), C.POINTER(C.c_uint64)))
-        assert rc == 0
-    e1.record(stream)
-    e1.synchronize()
-    barrier()
-    ms_e2e = e0.elapsed_time(e1)
-    sdm.check()
-
-    # ---- max over ranks ----
-    vals = torch.tensor([ms, ms_e2e, float(nsd), stage_ms["microphysics"]], dtype=torch.float64,
-                        device="cuda")
+    vals = torch.tensor([bat["ms"], bat["ms_e2e"], plain["ms"], float(bat["nsd"]),
+                         float(plain["nsd"])], dtype=torch.float64, device="cuda")
+    mx, sm = vals.clone(), vals.clone()
     if dist is not None:
-        mx = vals.clone()
         dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = vals.clone()
         dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms, ms_e2e = float(mx[0]), float(mx[1])
-        total_sd = float(sm[2])
-    else:
-        total_sd = float(nsd)
+    ms, ms_e2e, ms_plain = float(mx[0]), float(mx[1]), float(mx[2])
+    total_sd, total_sd_plain = float(sm[3]), float(sm[4])
     value = total_sd * args.steps / (ms / 1000.0)
     e2e = total_sd * args.steps / (ms_e2e / 1000.0)
+    value_plain = total_sd_plain * plain_steps / (ms_plain / 1000.0)
 
     if rank == 0:
         peak, peak_kind = peaks()
-        micro_ms = stage_ms["microphysics"]
-        bytes_micro = MICRO_BYTES_PER_SD * nsd + MICRO_BYTES_PER_GBX * ngbxs
-        achieved = bytes_micro / (micro_ms / 1000.0) / 1e9 if micro_ms > 0 else None
+        nsd, ngbxs = bat["nsd"], bat["ngbxs"]
+        st = bat["stage_ms"]
+        # dominant kernel group of the batched step: condensation (pass A + B) or collisions
+        dom = "condensation" if st["condensation"] >= st["collisions"] else "collisions"
+        per_sd = COND_BYTES_PER_SD if dom == "condensation" else COLL_BYTES_PER_SD
+        per_gbx = COND_BYTES_PER_GBX if dom == "condensation" else COLL_BYTES_PER_GBX
+        bytes_dom = per_sd * nsd + per_gbx * ngbxs
+        achieved = bytes_dom / (st[dom] / 1000.0) / 1e9 if st[dom] > 0 else None
         traffic = None
-        tp = os.path.join(ROOT, "profiles", "k_micro_traffic.json")
+        tp = os.path.join(ROOT, "profiles", f"{dom}_traffic.json")
         if os.path.exists(tp):
             with open(tp) as f:
                 tj = json.load(f)
@@ -272,23 +288,27 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "ndims": list(ndims), "ngbxs_per_gpu": ngbxs,
-                       "superdroplets_per_gpu": nsd, "path": "plain (one CTA per gridbox)",
+                       "superdroplets_per_gpu": nsd,
+                       "path": "batched (flat two-pass condensation, bucketed persistent collisions)",
                        "l2": "inputs larger than L2 (2.4 GB SoA per GPU), no flush"},
-            "roofline": {"bound": "hbm", "kernel": "k_micro", "achieved": achieved, "peak": peak,
+            "plain_gpu": {"value": value_plain, "unit": UNIT, "ms_per_step": ms_plain / plain_steps,
+                          "steps": plain_steps, "path": "one CTA per gridbox",
+                          "stages_ms_per_step": plain["stage_ms"]},
+            "speedup_vs_plain_gpu": value / value_plain,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic, "peak_kind": peak_kind,
-                         "bytes_per_launch": bytes_micro, "ms_per_launch": micro_ms},
+                         "bytes_per_launch": bytes_dom, "ms_per_launch": st[dom]},
             "cpu_baseline": {"value": cpu_value, "unit": UNIT, "cores": lcores, "kind": lref,
                              "sample": f"64x16x16 gridboxes of the workload ({cpu_nsd} "
                                        f"superdroplets), 1 step after 1 warm-up"},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
-            "gpu_launches": int(l1.value - l0.value),
-            "clocks": clocks,
-            "stages_ms_per_step": stage_ms,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bat["h2d"],
+                    "d2h_bytes_per_step": bat["d2h"]},
+            "gpu_launches": bat["launches"],
+            "clocks": bat["clocks"],
+            "stages_ms_per_step": st,
         }
         print(json.dumps(out), flush=True)
-    sdm.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

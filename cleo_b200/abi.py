@@ -46,6 +46,7 @@ ENACT_COALESCENCE, ENACT_BREAKUP, ENACT_COALBURE = 0, 1, 2
 NFRAGS_CONST, NFRAGS_CKE = 0, 1
 FLAG_STRAUB, FLAG_TESTIKSTRAUB, FLAG_SZAKALLURBICH, FLAG_CONST = 0, 1, 2, 3
 NRSEED_REFERENCE, NRSEED_MLP = 0, 1
+EXEC_PLAIN, EXEC_BATCHED = 0, 1
 
 _d = C.POINTER(C.c_double)
 _u32 = C.POINTER(C.c_uint32)
@@ -81,6 +82,8 @@ class Params(C.Structure):
         ("seed", C.c_uint64),
         ("motion_tv", C.c_int32),
         ("nr_seed", C.c_int32),
+        ("exec_mode", C.c_int32),
+        ("reserved0", C.c_int32),
     ]
 
     def as_dict(self) -> dict:

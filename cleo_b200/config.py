@@ -66,7 +66,8 @@ def make_params(*, condtstep: float | None = None, colltstep: float | None = Non
                 const_kernel: float = 1.0, nfrags_kind: int = NFRAGS_CONST, nfrags: float = 5.0,
                 nfrags_tv: int = TV_ROGERSGK, flag_kind: int = FLAG_STRAUB,
                 flag_tv: int = TV_ROGERSGK, flag_coaleff: float = 1.0, seed: int = 0,
-                motion_tv: int = TV_NULL, nr_seed: int = NRSEED_REFERENCE) -> Params:
+                motion_tv: int = TV_NULL, nr_seed: int = NRSEED_REFERENCE,
+                exec_mode: int = 1) -> Params:
     """Parameters of one SDM configuration. A timestep of None switches that process off."""
     p = Params()
     p.condstep = STEP_OFF if condtstep is None else realtime2step(condtstep)
@@ -96,6 +97,7 @@ def make_params(*, condtstep: float | None = None, colltstep: float | None = Non
     p.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
     p.motion_tv = int(motion_tv)
     p.nr_seed = int(nr_seed)
+    p.exec_mode = int(exec_mode)
     return p
 
 

@@ -1,0 +1,493 @@
+// batched.cuh — the batched microphysics of one SDM step (exec_mode CLEO_EXEC_BATCHED).
+//
+// Same results as k_micro (one CTA per gridbox), scheduled for B200 occupancy:
+//   k_b_qcond      warp per gridbox: qcond from the moved superdroplets (after the sort)
+//   k_b_thermo     thread per gridbox: psat, supersaturation, diffusion factor, Kelvin factor
+//   k_cond_a       thread per superdroplet: the mandatory two Newton iterations of every
+//                  implicit-Euler solve; solves needing more (sub-stepping, or a restart after two
+//                  unconverged iterations) are appended to a list keyed by their cost
+//   (radix sort of that list by cost, 16-bit keys)
+//   k_cond_b       thread per listed solve, neighbouring lanes of similar cost
+//   k_b_classify   gridboxes into size buckets (warp-aggregated atomics)
+//   k_b_small      persistent, warp per gridbox (n <= 64): reduction of the condensed mass and
+//                  Newton iterations, state update, collisions in registers + per-warp shared memory
+//   k_b_medium     persistent, CTA per gridbox (64 < n <= 1024): the same with shared-memory staging
+//   k_b_large      CTA per gridbox (n > 1024) with global scratch
+// Condensed mass per droplet goes through a scratch array and is summed per gridbox in a fixed
+// order, so budgets and states are deterministic.
+#pragma once
+
+namespace {
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+  return __shfl_sync(0xFFFFFFFFu, v, 0);
+}
+__device__ __forceinline__ uint32_t warp_sum_u(uint32_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+  return __shfl_sync(0xFFFFFFFFu, v, 0);
+}
+
+// warp-aggregated append of `want` lanes to a list counter; returns this lane's slot
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
+  const unsigned m = __ballot_sync(0xFFFFFFFFu, want);
+  const int lane = threadIdx.x & 31;
+  uint32_t base = 0;
+  if (m) {
+    const int leader = __ffs(m) - 1;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(m));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  }
+  return base + __popc(m & ((1u << lane) - 1u));
+}
+
+// ---- effect_on_hydrometeor_states (movesupersindomain.hpp:95-136), warp per gridbox ----
+__global__ void k_b_qcond(DevCtx c) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  for (uint32_t g = warp; g < c.ngbxs; g += nwarps) {
+    const uint32_t base = c.gstart[g], n = c.gcount[g];
+    double m = 0.0;
+    for (uint32_t k = lane; k < n; k += 32) {
+      const Where w{c.err, g, base + k};
+      m += condensate_mass(c.sd.r[base + k], c.sd.msol[base + k], w) * (double)c.sd.xi[base + k];
+    }
+    m = warp_sum_d(m);
+    if (lane == 0) {
+      const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
+      const double rho_cond = m / c.volume[g] * R0cubed_VOL0;
+      c.qcond[g] = rho_cond / dry_air_density(c.press[g], c.temp[g], c.qvap[g]);
+    }
+  }
+}
+
+// ---- per-gridbox thermodynamics of superdroplets_change (condensation.cpp:43-59) ----
+__global__ void k_b_thermo(DevCtx c, BatchScratch b) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x) {
+    if (g == 0) b.ctr[0] = 0;
+    if (c.gcount[g] == 0) continue;
+    const Where w{c.err, g, c.gstart[g]};
+    const double temp = c.temp[g];
+    const double psat = saturation_pressure(temp, w);
+    b.th_s[g] = supersaturation_ratio(c.press[g], c.qvap[g], psat);
+    b.th_ff[g] = diffusion_factor(c.press[g], temp, psat);
+  }
+}
+
+// cost key of a deferred solve: number of sub-steps (0 for a restart of the unique branch)
+__device__ __forceinline__ uint32_t deferred_key(double delt, double mindelt, bool substep) {
+  if (!substep) return 0u;
+  const double ns = ceil(delt / mindelt);
+  return ns >= 65535.0 ? 65535u : (uint32_t)ns;
+}
+
+// ---- pass A: superdrop_mass_change (condensation.cpp:98-112) up to two Newton iterations ----
+__global__ void __launch_bounds__(256)
+k_cond_a(DevCtx c, BatchScratch b) {
+  const cleo_b200_params& p = c.p;
+  const uint32_t n = c.counters[0];
+  const NewtonCfg cfg{p.maxniters, p.rtol, p.atol};
+  for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+    const uint32_t i = i0 + threadIdx.x;
+    bool defer = false;
+    uint32_t key = 0;
+    if (i < n) {
+      const uint32_t g = c.sd.gbx[i];
+      if (g < c.ngbxs) {
+        const Where w{c.err, g, i};
+        const double r = c.sd.r[i], msol = c.sd.msol[i];
+        double akoh, bkoh;
+        kohler_factors(msol, c.temp[g], akoh, bkoh);
+        const double ffactor_fv = b.th_ff[g] / ventilation_factor(r);
+        const OdeConsts o{b.th_s[g], akoh, bkoh, ffactor_fv};
+        const double z0 = initialguess(o, r);
+        const bool ucrit1 = first_unique_criteria(o, r, z0);
+        const double crit = critical_timestep(o);
+        const bool ucrit2 = (p.cond_delt <= crit);
+        uint32_t ni = 0;
+        if (ucrit1 || ucrit2) {
+          bool conv = false;
+          double z = z0;
+          z = nr_iterate(cfg, o, p.cond_delt, r, z, conv, ni);
+          z = nr_iterate(cfg, o, p.cond_delt, r, z, conv, ni);
+          if (conv) {
+            const double rnew = fmax(sqrt(z), dryradius(msol));  // change_radius
+            b.dm[i] = (condensate_mass(rnew, msol, w) - condensate_mass(r, msol, w)) *
+                      (double)c.sd.xi[i];
+            b.its[i] = ni;
+            c.sd.r[i] = rnew;
+          } else {
+            defer = true;  // restart from z0 until converged (impliciteuler.cpp:136-140)
+          }
+        } else {
+          defer = true;
+          key = deferred_key(p.cond_delt, fmax(crit, p.cond_minsubdelt), true);
+        }
+      }
+    }
+    const uint32_t pos = warp_append(&b.ctr[0], defer);
+    if (defer) {
+      b.lkeys[pos] = key;
+      b.lvals[pos] = i;
+    }
+  }
+}
+
+// ---- pass B: the deferred solves, in order of cost ----
+__global__ void __launch_bounds__(256)
+k_cond_b(DevCtx c, BatchScratch b) {
+  const cleo_b200_params& p = c.p;
+  const uint32_t nl = b.ctr[0];
+  const NewtonCfg cfg{p.maxniters, p.rtol, p.atol};
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nl; j += gridDim.x * blockDim.x) {
+    const uint32_t i = b.lvals[j];
+    const uint32_t g = c.sd.gbx[i];
+    const Where w{c.err, g, i};
+    const double r = c.sd.r[i], msol = c.sd.msol[i];
+    double akoh, bkoh;
+    kohler_factors(msol, c.temp[g], akoh, bkoh);
+    uint32_t ni = 0;
+    const double newr = solve_condensation(cfg, p.cond_delt, p.cond_minsubdelt, b.th_s[g], akoh,
+                                           bkoh, b.th_ff[g], r, 0.0, ni, w);
+    const double rnew = fmax(newr, dryradius(msol));
+    b.dm[i] = (condensate_mass(rnew, msol, w) - condensate_mass(r, msol, w)) * (double)c.sd.xi[i];
+    b.its[i] = ni;
+    c.sd.r[i] = rnew;
+  }
+}
+
+// ---- size buckets of the gridboxes that hold superdroplets ----
+__global__ void k_b_classify(DevCtx c, BatchScratch b) {
+  const uint32_t ng = c.ngbxs;
+  for (uint32_t g0 = blockIdx.x * blockDim.x; g0 < ng; g0 += gridDim.x * blockDim.x) {
+    const uint32_t g = g0 + threadIdx.x;
+    const uint32_t n = g < ng ? c.gcount[g] : 0u;
+    const int bk = (n == 0) ? -1 : (n <= SMALL_MAX ? 0 : (n <= MEDIUM_MAX ? 1 : 2));
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const uint32_t pos = warp_append(&b.ctr[1 + q], bk == q);
+      if (bk == q) b.bucket[(size_t)q * ng + pos] = g;
+    }
+  }
+}
+
+// reduction of the condensed mass and iterations of one gridbox + state update and budgets
+// (effect_on_thermodynamic_state, condensation.cpp:72-80 and :126-138; monitor, condensation.hpp:149)
+__device__ __forceinline__ void cond_commit(DevCtx& c, uint32_t g, double totmass,
+                                            unsigned long long totits) {
+  if (c.p.do_alter_thermo) {
+    const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
+    const double totrho = totmass / c.volume[g] * R0cubed_VOL0;
+    const double rho_dry = dry_air_density(c.press[g], c.temp[g], c.qvap[g]);
+    const double dq = totrho / rho_dry;
+    c.qvap[g] -= dq;
+    c.qcond[g] += dq;
+    c.temp[g] += (Latent_v / moist_specifc_heat(c.qvap[g], c.qcond[g])) * dq;
+  }
+  c.cond_mass[g] += totmass;
+  c.nr_iters[g] += totits;
+}
+
+// one pair (2jj, 2jj+1) of the shuffled gridbox: collisions.hpp:140-158
+__device__ __forceinline__ uint32_t collide_pair(const cleo_b200_params& p, Drop& dA, Drop& dB,
+                                                 double scale_p, double VOLUME, uint64_t key,
+                                                 uint64_t slot_pairs, uint32_t jj, const Where& w) {
+  const bool swap = dA.xi < dB.xi;
+  Drop& d1 = swap ? dB : dA;
+  Drop& d2 = swap ? dA : dB;
+  const double prob_jk = pair_prob(p, d1.r, d2.r, VOLUME);
+  const double large_xi = (double)d1.xi;
+  const double prob = scale_p * large_xi * prob_jk;
+  const double phi_coll = cleo_rng_to_unit(cleo_rng_u64(key, slot_pairs + 2ull * jj));
+  const double phi_out = cleo_rng_to_unit(cleo_rng_u64(key, slot_pairs + 2ull * jj + 1));
+  return enact_collision(p, d1, d2, prob, phi_coll, phi_out, w);
+}
+
+// ---- small gridboxes: persistent, one warp per gridbox ----
+__global__ void __launch_bounds__(B_THREADS)
+k_b_small(DevCtx c, BatchScratch b, uint32_t t_sdm, int cond, int coll) {
+  __shared__ double s_r[B_WARPS][SMALL_MAX];
+  __shared__ double s_m[B_WARPS][SMALL_MAX];
+  __shared__ unsigned long long s_x[B_WARPS][SMALL_MAX];
+  __shared__ uint8_t s_p[B_WARPS][SMALL_MAX];
+  __shared__ uint8_t s_j[B_WARPS][SMALL_MAX];
+  const cleo_b200_params& p = c.p;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t count = b.ctr[1];
+  const uint32_t* list = b.bucket;
+  while (true) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(&b.ctr[4], 1u);
+    item = __shfl_sync(0xFFFFFFFFu, item, 0);
+    if (item >= count) break;
+    const uint32_t g = list[item];
+    const uint32_t base = c.gstart[g];
+    uint32_t n = c.gcount[g];
+    if (cond) {
+      double m = 0.0;
+      uint32_t it = 0;
+      for (uint32_t k = lane; k < n; k += 32) {
+        m += b.dm[base + k];
+        it += b.its[base + k];
+      }
+      m = warp_sum_d(m);
+      it = warp_sum_u(it);
+      if (lane == 0) cond_commit(c, g, m, it);
+    }
+    if (!coll) continue;
+    const uint64_t key = cleo_rng_key(p.seed, t_sdm, g);
+    const uint64_t slot = b.slot[g];
+    // stage this gridbox: lane holds k = lane and k = lane + 32
+    for (uint32_t k = lane; k < n; k += 32) {
+      s_r[wib][k] = c.sd.r[base + k];
+      s_m[wib][k] = c.sd.msol[base + k];
+      s_x[wib][k] = c.sd.xi[base + k];
+      s_p[wib][k] = (uint8_t)k;
+      if (k >= 1)
+        s_j[wib][k] = (uint8_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - k)), 0, (uint64_t)k + 1);
+    }
+    __syncwarp();
+    if (lane == 0) {  // Fisher-Yates (shuffle.hpp:80-87)
+      for (uint32_t it = n > 0 ? n - 1 : 0; it > 0; --it) {
+        const uint8_t j = s_j[wib][it];
+        const uint8_t t = s_p[wib][it];
+        s_p[wib][it] = s_p[wib][j];
+        s_p[wib][j] = t;
+      }
+    }
+    __syncwarp();
+    const uint64_t slot_pairs = slot + (n >= 1 ? n - 1 : 0);
+    const uint32_t npairs = n / 2;
+    const double scale_p = (double)n * ((double)n - 1.0) / (2.0 * (double)npairs);
+    const double VOLUME = c.volume[g] * VOL0;
+    uint32_t nnull = 0;
+    if ((uint32_t)lane < npairs) {
+      const uint32_t jj = lane;
+      const uint32_t a = s_p[wib][2 * jj], bb = s_p[wib][2 * jj + 1];
+      const Where w{c.err, g, (uint64_t)base + 2 * jj};
+      Drop dA{s_x[wib][a], s_r[wib][a], s_m[wib][a]};
+      Drop dB{s_x[wib][bb], s_r[wib][bb], s_m[wib][bb]};
+      nnull = collide_pair(p, dA, dB, scale_p, VOLUME, key, slot_pairs, jj, w);
+      s_x[wib][a] = dA.xi; s_r[wib][a] = dA.r; s_m[wib][a] = dA.msol;
+      s_x[wib][bb] = dB.xi; s_r[wib][bb] = dB.r; s_m[wib][bb] = dB.msol;
+    }
+    __syncwarp();
+    const uint32_t totnull = warp_sum_u(nnull);
+    const uint32_t nvalid = n - totnull;
+    // destinations: valid superdroplets in shuffled order, then the nulls (collisions.hpp:240-248)
+    uint32_t src[2], q[2];
+    double c3v[2], c1v[2], c2v[2];
+    unsigned long long idv[2];
+    uint32_t cval = 0, cnull = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const uint32_t k = lane + 32 * h;
+      const bool act = k < n;
+      src[h] = act ? s_p[wib][k] : 0;
+      const bool valid = act && s_x[wib][src[h]] != 0;
+      const unsigned mv = __ballot_sync(0xFFFFFFFFu, valid);
+      const unsigned mn = __ballot_sync(0xFFFFFFFFu, act && !valid);
+      const unsigned lt = (1u << lane) - 1u;
+      q[h] = valid ? cval + __popc(mv & lt) : nvalid + cnull + __popc(mn & lt);
+      cval += __popc(mv);
+      cnull += __popc(mn);
+      if (act) {
+        const uint32_t s = base + src[h];
+        c3v[h] = c.sd.c3[s];
+        c1v[h] = c.sd.c1[s];
+        c2v[h] = c.sd.c2[s];
+        idv[h] = c.sd.id[s];
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const uint32_t k = lane + 32 * h;
+      if (k < n) {
+        const uint32_t o = base + q[h];
+        c.sd.r[o] = s_r[wib][src[h]];
+        c.sd.msol[o] = s_m[wib][src[h]];
+        c.sd.xi[o] = s_x[wib][src[h]];
+        c.sd.gbx[o] = q[h] < nvalid ? g : OOB;
+        c.sd.c3[o] = c3v[h];
+        c.sd.c1[o] = c1v[h];
+        c.sd.c2[o] = c2v[h];
+        c.sd.id[o] = idv[h];
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      c.gcount[g] = nvalid;
+      b.slot[g] = (uint32_t)(slot_pairs + 2ull * npairs);
+    }
+    n = nvalid;
+  }
+}
+
+// ---- medium and large gridboxes: one CTA per gridbox ----
+// medium: staged in shared memory with the non-staged fields permuted through registers;
+// large: staged in global scratch arrays.
+template <bool LARGE>
+__global__ void __launch_bounds__(B_THREADS)
+k_b_cta(DevCtx c, BatchScratch b, uint32_t t_sdm, int cond, int coll) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double shd[32];
+  __shared__ unsigned long long shu[32];
+  __shared__ uint32_t shw[40];
+  __shared__ uint32_t s_item;
+  constexpr uint32_t PT = MEDIUM_MAX / B_THREADS;  // superdroplets per thread (medium)
+  const cleo_b200_params& p = c.p;
+  const int tid = threadIdx.x;
+  const uint32_t q_idx = LARGE ? 2 : 1;
+  const uint32_t count = b.ctr[1 + q_idx];
+  const uint32_t* list = b.bucket + (size_t)q_idx * c.ngbxs;
+  while (true) {
+    if (tid == 0) s_item = atomicAdd(&b.ctr[4 + q_idx], 1u);
+    __syncthreads();
+    const uint32_t item = s_item;
+    __syncthreads();
+    if (item >= count) break;
+    const uint32_t g = list[item];
+    const uint32_t base = c.gstart[g];
+    const uint32_t n = c.gcount[g];
+    if (cond) {
+      double m = 0.0;
+      unsigned long long it = 0;
+      for (uint32_t k = tid; k < n; k += B_THREADS) {
+        m += b.dm[base + k];
+        it += b.its[base + k];
+      }
+      const double totm = block_sum(m, shd);
+      const unsigned long long toti = block_sum(it, shu);
+      if (tid == 0) cond_commit(c, g, totm, toti);
+    }
+    if (!coll) continue;
+    const uint64_t key = cleo_rng_key(p.seed, t_sdm, g);
+    const uint64_t slot = b.slot[g];
+    double* Sr = LARGE ? c.scr_r + base : reinterpret_cast<double*>(smem);
+    double* Sm = LARGE ? c.scr_m + base : reinterpret_cast<double*>(smem) + MEDIUM_MAX;
+    unsigned long long* Sx = LARGE ? c.scr_x + base
+                                   : reinterpret_cast<unsigned long long*>(smem) + 2 * MEDIUM_MAX;
+    uint32_t* P = LARGE ? c.scr_p + base : reinterpret_cast<uint32_t*>(smem + 24 * MEDIUM_MAX);
+    uint32_t* J = LARGE ? c.scr_j + base : reinterpret_cast<uint32_t*>(smem + 28 * MEDIUM_MAX);
+    for (uint32_t k = tid; k < n; k += B_THREADS) {
+      Sr[k] = c.sd.r[base + k];
+      Sm[k] = c.sd.msol[base + k];
+      Sx[k] = c.sd.xi[base + k];
+      P[k] = k;
+      if (k >= 1) J[k] = (uint32_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - k)), 0, (uint64_t)k + 1);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (uint32_t it = n > 0 ? n - 1 : 0; it > 0; --it) {
+        const uint32_t j = J[it];
+        const uint32_t t = P[it];
+        P[it] = P[j];
+        P[j] = t;
+      }
+    }
+    __syncthreads();
+    const uint64_t slot_pairs = slot + (n >= 1 ? n - 1 : 0);
+    const uint32_t npairs = n / 2;
+    const double scale_p = (double)n * ((double)n - 1.0) / (2.0 * (double)npairs);
+    const double VOLUME = c.volume[g] * VOL0;
+    uint32_t nnull = 0;
+    for (uint32_t jj = tid; jj < npairs; jj += B_THREADS) {
+      const uint32_t a = P[2 * jj], bb = P[2 * jj + 1];
+      const Where w{c.err, g, (uint64_t)base + 2 * jj};
+      Drop dA{Sx[a], Sr[a], Sm[a]};
+      Drop dB{Sx[bb], Sr[bb], Sm[bb]};
+      nnull += collide_pair(p, dA, dB, scale_p, VOLUME, key, slot_pairs, jj, w);
+      Sx[a] = dA.xi; Sr[a] = dA.r; Sm[a] = dA.msol;
+      Sx[bb] = dB.xi; Sr[bb] = dB.r; Sm[bb] = dB.msol;
+    }
+    const uint32_t totnull = block_sum(nnull, shw);
+    const uint32_t nvalid = n - totnull;
+    uint32_t cval = 0, cnull = 0;
+    // destination of shuffled position k; J becomes the inverse map q -> source
+    for (uint32_t k0 = 0; k0 < n; k0 += B_THREADS) {
+      const uint32_t k = k0 + tid;
+      const bool act = k < n;
+      const uint32_t src = act ? P[k] : 0;
+      const bool valid = act && Sx[src] != 0;
+      uint32_t tv, tn;
+      const uint32_t ev = block_excl_scan(valid ? 1u : 0u, shw, tv);
+      const uint32_t en = block_excl_scan((act && !valid) ? 1u : 0u, shw, tn);
+      if (act) J[valid ? (cval + ev) : (nvalid + cnull + en)] = src;
+      cval += tv;
+      cnull += tn;
+    }
+    __syncthreads();
+    if (LARGE) {
+      for (uint32_t q = tid; q < n; q += B_THREADS) {
+        const uint32_t s = base + J[q], o = base + q;
+        c.scr_c3[o] = c.sd.c3[s];
+        c.scr_c1[o] = c.sd.c1[s];
+        c.scr_c2[o] = c.sd.c2[s];
+        c.scr_id[o] = c.sd.id[s];
+      }
+      __syncthreads();
+      for (uint32_t q = tid; q < n; q += B_THREADS) {
+        const uint32_t o = base + q;
+        const uint32_t src = J[q];
+        c.sd.r[o] = Sr[src];
+        c.sd.msol[o] = Sm[src];
+        c.sd.xi[o] = Sx[src];
+        c.sd.gbx[o] = q < nvalid ? g : OOB;
+        c.sd.c3[o] = c.scr_c3[o];
+        c.sd.c1[o] = c.scr_c1[o];
+        c.sd.c2[o] = c.scr_c2[o];
+        c.sd.id[o] = c.scr_id[o];
+      }
+    } else {
+      double c3v[PT], c1v[PT], c2v[PT];
+      unsigned long long idv[PT];
+#pragma unroll
+      for (uint32_t h = 0; h < PT; ++h) {
+        const uint32_t q = tid + h * B_THREADS;
+        if (q < n) {
+          const uint32_t s = base + J[q];
+          c3v[h] = c.sd.c3[s];
+          c1v[h] = c.sd.c1[s];
+          c2v[h] = c.sd.c2[s];
+          idv[h] = c.sd.id[s];
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (uint32_t h = 0; h < PT; ++h) {
+        const uint32_t q = tid + h * B_THREADS;
+        if (q < n) {
+          const uint32_t o = base + q;
+          const uint32_t src = J[q];
+          c.sd.r[o] = Sr[src];
+          c.sd.msol[o] = Sm[src];
+          c.sd.xi[o] = Sx[src];
+          c.sd.gbx[o] = q < nvalid ? g : OOB;
+          c.sd.c3[o] = c3v[h];
+          c.sd.c1[o] = c1v[h];
+          c.sd.c2[o] = c2v[h];
+          c.sd.id[o] = idv[h];
+        }
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      c.gcount[g] = nvalid;
+      b.slot[g] = (uint32_t)(slot_pairs + 2ull * npairs);
+    }
+  }
+}
+
+// reset of the per-gridbox slot offsets at the start of an SDM step and of the bucket counters
+__global__ void k_b_reset(DevCtx c, BatchScratch b, int slots) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slots)
+    for (uint32_t g = i; g < c.ngbxs; g += gridDim.x * blockDim.x) b.slot[g] = 0;
+  if (i < 6) b.ctr[1 + i] = 0;
+}
+
+}  // namespace

@@ -1,0 +1,25 @@
+// batched_types.cuh — sizes and scratch of the batched microphysics schedule (batched.cuh).
+#pragma once
+
+#include <cstdint>
+
+namespace {
+
+constexpr uint32_t SMALL_MAX = 64;
+constexpr uint32_t MEDIUM_MAX = 1024;
+constexpr int B_THREADS = 256;
+constexpr int B_WARPS = B_THREADS / 32;
+
+struct BatchScratch {
+  double* th_s;      // per gridbox supersaturation ratio
+  double* th_ff;     // per gridbox diffusion factor
+  double* dm;        // per superdroplet condensed mass x xi
+  uint32_t* its;     // per superdroplet Newton iterations
+  uint32_t* lkeys;   // cost keys of deferred solves
+  uint32_t* lvals;   // positions of deferred solves
+  uint32_t* bucket;  // [3][ngbxs] gridbox lists per size bucket
+  uint32_t* slot;    // per gridbox RNG slot offset within the SDM step
+  uint32_t* ctr;     // [0] deferred solves, [1..3] bucket counts, [4..6] bucket heads
+};
+
+}  // namespace

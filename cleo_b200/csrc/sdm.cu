@@ -69,6 +69,8 @@ struct DevCtx {
 
 }  // namespace
 
+#include "batched_types.cuh"
+
 struct cleo_b200_ctx {
   DevCtx d;
   Fields buf[2];
@@ -79,6 +81,8 @@ struct cleo_b200_ctx {
   // sort scratch
   uint32_t *keys[2], *vals[2], *hist, *tile_sums;
   uint32_t ntiles_max, key_bits;
+  BatchScratch bs{};              // batched-schedule scratch
+  int grid_small = 0, grid_medium = 0, grid_large = 0, grid_flat = 0;
   unsigned long long launches = 0;  // kernels launched by this context
   std::vector<void*> allocs;
   // stage timing: (stage, start, end) event triples recorded while profiling is on
@@ -618,6 +622,8 @@ __global__ void k_condsolve(DevCtx c, uint32_t n, const double* __restrict__ rad
 
 }  // namespace
 
+#include "batched.cuh"
+
 // ------------------------------------------------------------------------------------------
 // host side
 // ------------------------------------------------------------------------------------------
@@ -689,6 +695,74 @@ int sort_current(cleo_b200_ctx* x) {
   return CLEO_OK;
 }
 
+// stable radix sort of (key, value) pairs whose count is *n_ptr (device), over `bits` key bits,
+// from (k0, v0) using (k1, v1) as the other buffer; returns 0 if the result is in (k0, v0)
+int radix_pairs(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1,
+                const uint32_t* n_ptr, uint32_t bits) {
+  cudaStream_t s = x->stream;
+  const uint32_t nt = x->ntiles_max;
+  const uint64_t nh = (uint64_t)256 * nt;
+  const uint32_t nscan_tiles = (uint32_t)((nh + SCAN_TILE - 1) / SCAN_TILE);
+  int cur = 0;
+  uint32_t* K[2] = {k0, k1};
+  uint32_t* V[2] = {v0, v1};
+  for (uint32_t shift = 0; shift < bits; shift += 8) {
+    k_rs_upsweep<<<nt, RS_THREADS, 0, s>>>(K[cur], n_ptr, (int)shift, x->hist, nt);
+    k_scan_tiles<<<nscan_tiles, SCAN_THREADS, 0, s>>>(x->hist, x->hist, nh, x->tile_sums);
+    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(x->tile_sums, nscan_tiles, nullptr);
+    k_scan_add<<<(unsigned)((nh + 255) / 256), 256, 0, s>>>(x->hist, nh, x->tile_sums);
+    k_rs_downsweep<<<nt, RS_THREADS, 0, s>>>(K[cur], V[cur], n_ptr, (int)shift, x->hist, nt,
+                                             K[1 - cur], V[1 - cur]);
+    x->launches += 5;
+    cur = 1 - cur;
+  }
+  return cur;
+}
+
+// the microphysics of one SDM step on the batched schedule (batched.cuh)
+int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, bool did_motion) {
+  DevCtx& d = x->d;
+  BatchScratch& b = x->bs;
+  cudaStream_t s = x->stream;
+  StageMark m(x, 2);
+  const int gg = grid_for(d.ngbxs, 256);
+  if (did_motion) {
+    const size_t warps = d.ngbxs < (size_t)148 * 64 ? d.ngbxs : (size_t)148 * 64;
+    k_b_qcond<<<(unsigned)((warps * 32 + 255) / 256 + 1), 256, 0, s>>>(d);
+    x->launches += 1;
+  }
+  k_b_reset<<<gg, 256, 0, s>>>(d, b, 1);
+  x->launches += 1;
+  uint32_t subt = t_sdm;
+  while (subt < t_sdm_next) {
+    const bool cond = on_step(d.p.condstep, subt);
+    const bool coll = on_step(d.p.collstep, subt);
+    if (cond) {
+      StageMark mc(x, 3);
+      k_b_thermo<<<gg, 256, 0, s>>>(d, b);
+      k_cond_a<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, b);
+      x->launches += 2;
+      const int where = radix_pairs(x, b.lkeys, b.lvals, x->keys[1], x->vals[1], b.ctr, 16);
+      if (where != 0) return CLEO_ERR_CUDA;  // 16 key bits: two passes, result back in place
+      k_cond_b<<<x->grid_flat, 256, 0, s>>>(d, b);
+      x->launches += 1;
+    }
+    if (cond || coll) {
+      StageMark mk(x, 4);
+      k_b_reset<<<1, 32, 0, s>>>(d, b, 0);
+      k_b_classify<<<gg, 256, 0, s>>>(d, b);
+      k_b_small<<<x->grid_small, B_THREADS, 0, s>>>(d, b, t_sdm, cond ? 1 : 0, coll ? 1 : 0);
+      k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_MAX * 32, s>>>(d, b, t_sdm, cond ? 1 : 0,
+                                                                           coll ? 1 : 0);
+      k_b_cta<true><<<x->grid_large, B_THREADS, 0, s>>>(d, b, t_sdm, cond ? 1 : 0, coll ? 1 : 0);
+      x->launches += 5;
+    }
+    subt = min(next_step(d.p.condstep, subt), next_step(d.p.collstep, subt));
+  }
+  CUDA_TRY(cudaGetLastError());
+  return CLEO_OK;
+}
+
 int run_sdm_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
   DevCtx& d = x->d;
   cudaStream_t s = x->stream;
@@ -704,6 +778,7 @@ int run_sdm_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
     if (rc) return rc;
   }
   const bool micro = (d.p.condstep != CLEO_STEP_OFF || d.p.collstep != CLEO_STEP_OFF);
+  if (d.p.exec_mode == CLEO_EXEC_BATCHED) return run_batched_micro(x, t_sdm, t_sdm_next, did_motion);
   if (micro || did_motion) {
     const uint32_t blocks = d.ngbxs < (1u << 30) ? d.ngbxs : (1u << 30);
     if (blocks > 0) {
@@ -778,6 +853,15 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
     rc |= dalloc(x, &x->vals[k], cap);
   }
   rc |= dalloc(x, &x->hist, (size_t)256 * x->ntiles_max);
+  rc |= dalloc(x, &x->bs.th_s, ng);
+  rc |= dalloc(x, &x->bs.th_ff, ng);
+  rc |= dalloc(x, &x->bs.dm, cap);
+  rc |= dalloc(x, &x->bs.its, cap);
+  rc |= dalloc(x, &x->bs.lkeys, cap);
+  rc |= dalloc(x, &x->bs.lvals, cap);
+  rc |= dalloc(x, &x->bs.bucket, 3 * ng);
+  rc |= dalloc(x, &x->bs.slot, ng);
+  rc |= dalloc(x, &x->bs.ctr, 8);
   rc |= dalloc(x, &x->tile_sums, ((size_t)256 * x->ntiles_max + SCAN_TILE - 1) / SCAN_TILE + 1);
   if (rc) {
     cleo_b200_destroy(x);
@@ -812,6 +896,22 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   CUDA_TRY(cudaMemsetAsync(d.gcount, 0, (ng ? ng : 1) * 4, x->stream));
   CUDA_TRY(cudaMemsetAsync(d.err, 0, sizeof(DevError), x->stream));
   CUDA_TRY(cudaFuncSetAttribute(k_micro, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MICRO_SMEM));
+  CUDA_TRY(cudaMemsetAsync(x->bs.ctr, 0, 32, x->stream));
+  CUDA_TRY(cudaMemsetAsync(x->bs.slot, 0, (ng ? ng : 1) * 4, x->stream));
+  {  // persistent grids of the batched kernels: full occupancy on every SM
+    int dev = 0, sms = 148, occ = 1;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small, B_THREADS, 0));
+    x->grid_small = sms * (occ > 0 ? occ : 1);
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<false>, B_THREADS,
+                                                           (size_t)MEDIUM_MAX * 32));
+    x->grid_medium = sms * (occ > 0 ? occ : 1);
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<true>, B_THREADS, 0));
+    x->grid_large = sms * (occ > 0 ? occ : 1);
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cond_b, 256, 0));
+    x->grid_flat = sms * (occ > 0 ? occ : 1);
+  }
   CUDA_TRY(cudaStreamSynchronize(x->stream));
   *out = x;
   return CLEO_OK;
@@ -838,10 +938,10 @@ int cleo_b200_set_profiling(cleo_b200_ctx* x, int enable) {
   return CLEO_OK;
 }
 
-int cleo_b200_stage_times(cleo_b200_ctx* x, double ms[3], uint64_t count[3]) {
+int cleo_b200_stage_times(cleo_b200_ctx* x, double ms[5], uint64_t count[5]) {
   if (!x || !ms || !count) return CLEO_ERR_ARGUMENT;
   CUDA_TRY(cudaStreamSynchronize(x->stream));
-  for (int k = 0; k < 3; ++k) {
+  for (int k = 0; k < 5; ++k) {
     ms[k] = 0.0;
     count[k] = 0;
   }

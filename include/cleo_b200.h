@@ -90,6 +90,10 @@ enum cleo_nrseed {           /* initial guess of the condensation Newton solve *
   CLEO_NRSEED_REFERENCE = 0, /* ImplicitIterations::initialguess, impliciteuler.cpp:156-170 */
   CLEO_NRSEED_MLP = 1        /* surrogate-predicted post-step r^2 */
 };
+enum cleo_exec {             /* how the microphysics of one SDM step is scheduled on the GPU */
+  CLEO_EXEC_PLAIN = 0,       /* one CTA per gridbox does condensation and collisions */
+  CLEO_EXEC_BATCHED = 1      /* flat two-pass condensation + size-bucketed persistent collisions */
+};
 
 #define CLEO_STEP_OFF 0xFFFFFFFFu /* interval value that switches a process off (on_step false) */
 
@@ -127,6 +131,9 @@ typedef struct cleo_b200_params {
   /* motion */
   int32_t motion_tv;        /* terminal velocity subtracted from w (predcorr.hpp:83-105) */
   int32_t nr_seed;          /* enum cleo_nrseed */
+  /* execution (no reference counterpart: results do not depend on it) */
+  int32_t exec_mode;        /* enum cleo_exec */
+  int32_t reserved0;
 } cleo_b200_params;
 
 /*
@@ -240,11 +247,12 @@ int cleo_b200_kernel_launches(cleo_b200_ctx* ctx, uint64_t* n);
  * reference's Kokkos profiling regions (sdm_movement_*, timestep_sdm_microphysics;
  * libs/gridboxes/movesupersindomain.hpp:190-261, libs/runcleo/sdmmethods.hpp:159-216).
  * cleo_b200_set_profiling(ctx, 1) starts recording; cleo_b200_stage_times synchronises, returns
- * the summed milliseconds and launch counts of the stages {motion, sort, microphysics} since the
- * last call, and resets them.
+ * the summed milliseconds and counts of the stages {motion, sort, microphysics, condensation,
+ * collisions} since the last call, and resets them (condensation and collisions are the parts of
+ * microphysics that the batched schedule runs as separate kernels; zero on the plain schedule).
  */
 int cleo_b200_set_profiling(cleo_b200_ctx* ctx, int enable);
-int cleo_b200_stage_times(cleo_b200_ctx* ctx, double ms[3], uint64_t count[3]);
+int cleo_b200_stage_times(cleo_b200_ctx* ctx, double ms[5], uint64_t count[5]);
 
 /*
  * Stable sort of superdroplets by gridbox index that allocates no device memory. No counterpart in

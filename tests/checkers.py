@@ -139,8 +139,12 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def params_from_bytes(b) -> abi.Params:
+    """Params from stored bytes; fields added after a fixture was written keep their zero
+    default (exec_mode 0 = plain)."""
     p = abi.Params()
-    C.memmove(C.byref(p), bytes(np.asarray(b, dtype=np.uint8)), C.sizeof(abi.Params))
+    raw = bytes(np.asarray(b, dtype=np.uint8))
+    n = min(len(raw), C.sizeof(abi.Params))
+    C.memmove(C.byref(p), raw, n)
     return p
 
 

@@ -31,6 +31,15 @@ def budget_close(got, exp, what=""):
     assert np.all(err <= 1e-12 * scale + 1e-300), (what, float(np.max(err)) / max(scale, 1e-300))
 
 
+MODES = [abi.EXEC_PLAIN, abi.EXEC_BATCHED]
+MODE_IDS = ["plain", "batched"]
+
+
+def with_mode(w, mode):
+    w["params"].exec_mode = mode
+    return w
+
+
 @pytest.fixture(scope="module")
 def lib():
     import torch
@@ -49,9 +58,11 @@ def run_pair(lib, w, nsteps):
     return g, o
 
 
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
 @pytest.mark.parametrize("fname", K.step_fixtures())
-def test_gpu_matches_golden(lib, fname):
+def test_gpu_matches_golden(lib, fname, mode):
     w, exp = K.load_step_fixture(os.path.join(K.GOLDEN, fname))
+    with_mode(w, mode)
     g = make_sdm(w, lib=lib)
     for s in range(exp["nsteps"]):
         g.run_step(s * w["tstep"], (s + 1) * w["tstep"])
@@ -63,9 +74,10 @@ def test_gpu_matches_golden(lib, fname):
     budget_close(g.download_budgets()[0], exp["cond_mass"], fname)
 
 
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
 @pytest.mark.parametrize("name,build,nsteps", VARIANTS, ids=[v[0] for v in VARIANTS])
-def test_gpu_matches_oracle_variants(lib, name, build, nsteps):
-    w = build()
+def test_gpu_matches_oracle_variants(lib, name, build, nsteps, mode):
+    w = with_mode(build(), mode)
     g, o = run_pair(lib, w, nsteps)
     K.assert_same_domain(g.download_supers(), o.download_supers(), rtol=RTOL, what=name)
     sg, so = g.download_state(), o.download_state()
@@ -104,9 +116,10 @@ def test_gpu_condensation_solve(lib, tol):
     assert np.array_equal(nit.cpu().numpy().astype(np.uint32), io)
 
 
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
 @pytest.mark.parametrize("name,pov,sov,dov,code", ERRS, ids=[e[0] for e in ERRS])
-def test_gpu_error_codes(lib, name, pov, sov, dov, code):
-    w = _err_case(pov, sov, dov)
+def test_gpu_error_codes(lib, name, pov, sov, dov, code, mode):
+    w = with_mode(_err_case(pov, sov, dov), mode)
     s = make_sdm(w, lib=lib)
     with pytest.raises(CleoError) as ei:
         for k in range(3):
@@ -117,22 +130,25 @@ def test_gpu_error_codes(lib, name, pov, sov, dov, code):
     s.download_supers()
 
 
-def test_gpu_rainshaft_config(lib):
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
+def test_gpu_rainshaft_config(lib, mode):
     """1-D rain shaft at full size (256 boxes x 256 superdroplets), 10 steps."""
-    w = W.rainshaft()
+    w = with_mode(W.rainshaft(), mode)
     g, o = run_pair(lib, w, 10)
     K.assert_same_domain(g.download_supers(), o.download_supers(), rtol=RTOL, what="rainshaft")
 
 
-def test_gpu_uneven3d_medium(lib):
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
+def test_gpu_uneven3d_medium(lib, mode):
     """3-D uneven counts on 32x32x16 boxes (~0.6 M superdroplets), 4 steps."""
-    w = W.uneven3d(ndims=(16, 32, 32), seed=8)
+    w = with_mode(W.uneven3d(ndims=(16, 32, 32), seed=8), mode)
     g, o = run_pair(lib, w, 4)
     K.assert_same_domain(g.download_supers(), o.download_supers(), rtol=RTOL, what="uneven3d")
 
 
-def test_gpu_deterministic(lib):
-    w = W.bubble3d(ndims=(8, 16, 8), seed=9)
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
+def test_gpu_deterministic(lib, mode):
+    w = with_mode(W.bubble3d(ndims=(8, 16, 8), seed=9), mode)
     runs = []
     for _ in range(2):
         g = make_sdm(w, lib=lib)
@@ -142,6 +158,24 @@ def test_gpu_deterministic(lib):
         runs.append(d)
     for k in ("sdid", "xi", "radius", "coord3", "coord1"):
         assert np.array_equal(runs[0][k], runs[1][k]), k
+
+
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
+def test_gpu_all_bucket_sizes(lib, mode):
+    """Gridboxes of 0 .. 3000 superdroplets (every size bucket of the batched schedule)."""
+    w = W.uneven3d(ndims=(4, 4, 4), seed=12)
+    rng = np.random.default_rng(12)
+    counts = rng.integers(0, 80, 64)
+    counts[[3, 17, 40]] = (300, 1024, 3000)
+    counts[[5, 6]] = (0, 1)
+    sd = W.populate(w["grid"], counts, rng, temp=w["state"]["temp"],
+                    s_ratio=np.full(64, 0.99))
+    w["supers"] = sd
+    w["n_sd"] = int(counts.sum())
+    w["params"].exec_mode = mode
+    g, o = run_pair(lib, w, 6)
+    K.assert_same_domain(g.download_supers(), o.download_supers(), rtol=RTOL, what="buckets")
+    budget_close(g.download_budgets()[0], o.download_budgets()[0], "buckets")
 
 
 def test_gpu_golovin_analytic(lib):
