@@ -47,6 +47,8 @@ NFRAGS_CONST, NFRAGS_CKE = 0, 1
 FLAG_STRAUB, FLAG_TESTIKSTRAUB, FLAG_SZAKALLURBICH, FLAG_CONST = 0, 1, 2, 3
 NRSEED_REFERENCE, NRSEED_MLP = 0, 1
 EXEC_PLAIN, EXEC_BATCHED = 0, 1
+MLP_TCGEN05, MLP_MMA_SYNC, MLP_FP32 = 0, 1, 2
+MLP_NFEATURES, MLP_NHIDDEN, MLP_NPARAMS, MLP_NNORM = 7, 64, 4737, 16
 
 _d = C.POINTER(C.c_double)
 _u32 = C.POINTER(C.c_uint32)
@@ -221,6 +223,11 @@ EXPORTED = (
     "cleo_b200_download_state", "cleo_b200_download_budgets", "cleo_b200_condensation_solve",
     "cleo_b200_stream", "cleo_b200_kernel_launches", "cleo_b200_set_profiling",
     "cleo_b200_stage_times", "cleo_b200_sort_by_gridbox_static", "cleo_b200_version",
+    "cleo_b200_mlp_create", "cleo_b200_mlp_destroy", "cleo_b200_mlp_set_params",
+    "cleo_b200_mlp_get_params", "cleo_b200_mlp_features", "cleo_b200_mlp_fit_normalisation",
+    "cleo_b200_mlp_loss_grad", "cleo_b200_mlp_train", "cleo_b200_mlp_infer",
+    "cleo_b200_set_surrogate", "cleo_b200_set_graphs", "cleo_b200_autotune",
+    "cleo_b200_tuned_config",
 )
 
 _LIB = None
@@ -255,6 +262,25 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
     lib.cleo_b200_sort_by_gridbox_static.restype = C.c_int
     lib.cleo_b200_version.argtypes = []
     lib.cleo_b200_version.restype = C.c_char_p
+    fp = C.POINTER(C.c_float)
+    for name, args in (
+            ("mlp_create", [vp, C.c_uint64, C.POINTER(vp)]),
+            ("mlp_destroy", [vp]),
+            ("mlp_set_params", [vp, fp, fp]),
+            ("mlp_get_params", [vp, fp, fp]),
+            ("mlp_features", [vp, C.c_size_t] + [vp] * 10),
+            ("mlp_fit_normalisation", [vp, C.c_size_t, vp, vp]),
+            ("mlp_loss_grad", [vp, C.c_size_t, vp, vp, vp, vp]),
+            ("mlp_train", [vp, C.c_size_t, vp, vp, C.c_uint32, C.c_uint32, C.c_float,
+                           C.c_uint64, vp]),
+            ("mlp_infer", [vp, C.c_size_t, vp, vp, C.c_int]),
+            ("set_surrogate", [vp, vp]),
+            ("set_graphs", [vp, C.c_int]),
+            ("autotune", [vp, C.c_int]),
+            ("tuned_config", [vp, C.POINTER(C.c_int32)])):
+        f = getattr(lib, "cleo_b200_" + name)
+        f.argtypes = args
+        f.restype = C.c_int
     if path is None:
         _LIB = lib
     return lib

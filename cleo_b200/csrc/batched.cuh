@@ -9,10 +9,14 @@
 //   (radix sort of that list by cost, 16-bit keys)
 //   k_cond_b       thread per listed solve, neighbouring lanes of similar cost
 //   k_b_classify   gridboxes into size buckets (warp-aggregated atomics)
-//   k_b_small      persistent, warp per gridbox (n <= 64): reduction of the condensed mass and
-//                  Newton iterations, state update, collisions in registers + per-warp shared memory
-//   k_b_medium     persistent, CTA per gridbox (64 < n <= 1024): the same with shared-memory staging
-//   k_b_large      CTA per gridbox (n > 1024) with global scratch
+//   k_b_small      persistent, warp per gridbox (n <= small_max <= 64): reduction of the condensed
+//                  mass and Newton iterations, state update, collisions in registers + per-warp
+//                  shared memory
+//   k_b_cta<false> persistent, CTA per gridbox (small_max < n <= medium_max <= 1024): the same
+//                  with shared-memory staging
+//   k_b_cta<true>  CTA per gridbox (n > medium_max) with global scratch
+// small_max, medium_max, the pass-A block size and the pass-B grid are chosen by the autotuner
+// (results do not depend on them).
 // Condensed mass per droplet goes through a scratch array and is summed per gridbox in a fixed
 // order, so budgets and states are deterministic.
 #pragma once
@@ -77,6 +81,29 @@ __global__ void k_b_thermo(DevCtx c, BatchScratch b) {
   }
 }
 
+// domain superdroplets -> Newton seed r^2 in b.dm (the surrogate's IO in the batched schedule)
+struct SdmSeedIO {
+  const uint32_t* gbx;
+  const double *r, *msol, *temp, *press, *s_ratio;
+  double delt;
+  uint32_t ngbxs;
+  const uint32_t* nrange;  // counters[0]
+  double* seed;
+  __device__ __forceinline__ bool in_domain(uint32_t i) const {
+    return i < *nrange && gbx[i] < ngbxs;
+  }
+  __device__ __forceinline__ void features(uint32_t i, float x[mlp::NIN]) const {
+    if (!in_domain(i)) return;
+    const uint32_t g = gbx[i];
+    mlp::raw_features(r[i], msol[i], temp[g], press[g], s_ratio[g], delt, x);
+  }
+  __device__ __forceinline__ void store(uint32_t i, float t) const {
+    if (!in_domain(i)) return;
+    const double ri = r[i];
+    seed[i] = ri * ri * exp((double)t);
+  }
+};
+
 // cost key of a deferred solve: number of sub-steps (0 for a restart of the unique branch)
 __device__ __forceinline__ uint32_t deferred_key(double delt, double mindelt, bool substep) {
   if (!substep) return 0u;
@@ -104,17 +131,31 @@ k_cond_a(DevCtx c, BatchScratch b) {
         const double ffactor_fv = b.th_ff[g] / ventilation_factor(r);
         const OdeConsts o{b.th_s[g], akoh, bkoh, ffactor_fv};
         const double z0 = initialguess(o, r);
+        // ucrit1 || ucrit2, the critical timestep only evaluated when ucrit1 fails
         const bool ucrit1 = first_unique_criteria(o, r, z0);
-        const double crit = critical_timestep(o);
-        const bool ucrit2 = (p.cond_delt <= crit);
+        const double crit = ucrit1 ? 0.0 : critical_timestep(o);
         uint32_t ni = 0;
-        if (ucrit1 || ucrit2) {
+        if (ucrit1 || p.cond_delt <= crit) {
           bool conv = false;
-          double z = z0;
-          z = nr_iterate(cfg, o, p.cond_delt, r, z, conv, ni);
-          z = nr_iterate(cfg, o, p.cond_delt, r, z, conv, ni);
+          GEval e = eval_g(o, p.cond_delt, r, z0);
+          bool seeded = false;  // the surrogate's seed, when its residual is the smaller one
+          if (p.nr_seed == CLEO_NRSEED_MLP && seed_ok(b.dm[i])) {
+            const GEval es = eval_g(o, p.cond_delt, r, b.dm[i]);
+            if (fabs(es.g) < fabs(e.g)) {
+              double zs;
+              conv = integrate_seeded(cfg, o, p.cond_delt, r, es, ni, zs) &&
+                     seeded_root_ok(o, ucrit1, zs);
+              e.z = zs;
+              seeded = true;
+              if (!conv) b.dm[i] = -1.0;  // pass B starts from the reference guess
+            }
+          }
+          if (!seeded) {
+            e = nr_iterate(cfg, o, p.cond_delt, r, e, conv, ni);
+            e = nr_iterate(cfg, o, p.cond_delt, r, e, conv, ni);
+          }
           if (conv) {
-            const double rnew = fmax(sqrt(z), dryradius(msol));  // change_radius
+            const double rnew = fmax(sqrt(e.z), dryradius(msol));  // change_radius
             b.dm[i] = (condensate_mass(rnew, msol, w) - condensate_mass(r, msol, w)) *
                       (double)c.sd.xi[i];
             b.its[i] = ni;
@@ -150,8 +191,9 @@ k_cond_b(DevCtx c, BatchScratch b) {
     double akoh, bkoh;
     kohler_factors(msol, c.temp[g], akoh, bkoh);
     uint32_t ni = 0;
+    const double seed = p.nr_seed == CLEO_NRSEED_MLP ? b.dm[i] : 0.0;
     const double newr = solve_condensation(cfg, p.cond_delt, p.cond_minsubdelt, b.th_s[g], akoh,
-                                           bkoh, b.th_ff[g], r, 0.0, ni, w);
+                                           bkoh, b.th_ff[g], r, seed, ni, w);
     const double rnew = fmax(newr, dryradius(msol));
     b.dm[i] = (condensate_mass(rnew, msol, w) - condensate_mass(r, msol, w)) * (double)c.sd.xi[i];
     b.its[i] = ni;
@@ -165,7 +207,7 @@ __global__ void k_b_classify(DevCtx c, BatchScratch b) {
   for (uint32_t g0 = blockIdx.x * blockDim.x; g0 < ng; g0 += gridDim.x * blockDim.x) {
     const uint32_t g = g0 + threadIdx.x;
     const uint32_t n = g < ng ? c.gcount[g] : 0u;
-    const int bk = (n == 0) ? -1 : (n <= SMALL_MAX ? 0 : (n <= MEDIUM_MAX ? 1 : 2));
+    const int bk = (n == 0) ? -1 : (n <= b.small_max ? 0 : (n <= b.medium_max ? 1 : 2));
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       const uint32_t pos = warp_append(&b.ctr[1 + q], bk == q);
@@ -208,7 +250,8 @@ __device__ __forceinline__ uint32_t collide_pair(const cleo_b200_params& p, Drop
 
 // ---- small gridboxes: persistent, one warp per gridbox ----
 __global__ void __launch_bounds__(B_THREADS)
-k_b_small(DevCtx c, BatchScratch b, uint32_t t_sdm, int cond, int coll) {
+k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
+  const uint32_t t_sdm = *b.tsdm;
   __shared__ double s_r[B_WARPS][SMALL_MAX];
   __shared__ double s_m[B_WARPS][SMALL_MAX];
   __shared__ unsigned long long s_x[B_WARPS][SMALL_MAX];
@@ -332,7 +375,8 @@ k_b_small(DevCtx c, BatchScratch b, uint32_t t_sdm, int cond, int coll) {
 // large: staged in global scratch arrays.
 template <bool LARGE>
 __global__ void __launch_bounds__(B_THREADS)
-k_b_cta(DevCtx c, BatchScratch b, uint32_t t_sdm, int cond, int coll) {
+k_b_cta(DevCtx c, BatchScratch b, int cond, int coll) {
+  const uint32_t t_sdm = *b.tsdm;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double shd[32];
   __shared__ unsigned long long shu[32];
@@ -483,6 +527,11 @@ k_b_cta(DevCtx c, BatchScratch b, uint32_t t_sdm, int cond, int coll) {
 }
 
 // reset of the per-gridbox slot offsets at the start of an SDM step and of the bucket counters
+// the device copy of the SDM step time: set before a step whose time the device does not hold,
+// advanced by the last kernel of every step (so one captured step graph serves every step)
+__global__ void k_b_set_t(BatchScratch b, uint32_t t) { *b.tsdm = t; }
+__global__ void k_b_advance_t(BatchScratch b, uint32_t dt) { *b.tsdm += dt; }
+
 __global__ void k_b_reset(DevCtx c, BatchScratch b, int slots) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (slots)

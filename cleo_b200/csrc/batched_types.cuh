@@ -20,6 +20,9 @@ struct BatchScratch {
   uint32_t* bucket;  // [3][ngbxs] gridbox lists per size bucket
   uint32_t* slot;    // per gridbox RNG slot offset within the SDM step
   uint32_t* ctr;     // [0] deferred solves, [1..3] bucket counts, [4..6] bucket heads
+  uint32_t* tsdm;    // the SDM step's start time (keys the injected random numbers)
+  uint32_t small_max;   // gridboxes with 1..small_max superdroplets: warp kernel (<= SMALL_MAX)
+  uint32_t medium_max;  // small_max..medium_max: CTA kernel in shared memory (<= MEDIUM_MAX)
 };
 
 }  // namespace

@@ -16,6 +16,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 
 #if defined(__CUDACC__)
 #define CLEO_MATH_HD __host__ __device__ __forceinline__
@@ -169,13 +170,129 @@ CLEO_MATH_HD double round_dd(dd v) {
   return s.hi;
 }
 
-// exp(x), rounded once from a double-double evaluation
-CLEO_MATH_HD double dexp(double x) {
+// exp(x), rounded once from a double-double evaluation (the second, accurate phase)
+CLEO_MATH_HD double dexp_dd(double x) {
   if (!(x > -707.0 && x < 707.0)) return std::exp(x);
   return round_dd(dd_exp(dd{x, 0.0}));
 }
 
-// pow(x, y) for the exponents CLEO uses, rounded once from a double-double evaluation
+// pow(x, y) for x > 0 normal and y not special, rounded once from a double-double evaluation
+CLEO_MATH_HD double dpow_dd(double x, double y) {
+  const dd z = dd_mul_d(dd_log(x), y);
+  if (!(z.hi > -707.0 && z.hi < 707.0)) return std::pow(x, y);
+  return round_dd(dd_exp(z));
+}
+
+// ---- first phase (Ziv's strategy) ----
+// A cheaper evaluation with relative error below 2^-72 (analysis beside each step), accepted
+// only when that bound cannot move the value across a rounding midpoint; otherwise the accurate
+// phase above decides. Either way the result is the double nearest the true value, so the two
+// phases together return what the accurate phase alone returns.
+constexpr double FAST_ERR = 0x1p-67;  // bound used by the rounding test (about 32x the estimate)
+
+CLEO_MATH_HD uint64_t dbits(double x) {
+#if defined(__CUDA_ARCH__)
+  return (uint64_t)__double_as_longlong(x);
+#else
+  uint64_t b;
+  std::memcpy(&b, &x, sizeof b);
+  return b;
+#endif
+}
+CLEO_MATH_HD double bitsd(uint64_t b) {
+#if defined(__CUDA_ARCH__)
+  return __longlong_as_double((long long)b);
+#else
+  double x;
+  std::memcpy(&x, &b, sizeof x);
+  return x;
+#endif
+}
+
+// ln x for positive normal finite x, relative error below 2^-70 (absolute below 2^-79 plus
+// 2^-100 |exponent|): x = 2^e m, m in [sqrt(1/2), sqrt(2)); rc ~ 1/c for the nearest centre
+// c = i/512, r = m rc - 1 exactly (|r| < 2^-9.4); ln m = -ln(rc) + log1p(r), the series
+// truncated after r^8/8 (remainder below 2^-76 |r|).
+CLEO_MATH_HD dd fast_log(double x) {
+#if defined(__CUDA_ARCH__)
+  using namespace cleo_dd_dev;
+#else
+  using namespace cleo_dd_host;
+#endif
+  int e = 0;
+  double m = std::frexp(x, &e);
+  if (m < 0.70710678118654752440) {
+    m *= 2.0;
+    e -= 1;
+  }
+  const int i = (int)std::rint(m * 512.0);  // 362 .. 724
+  const double* t = cleo_fast_log_tab[i - 362];
+  const dd p = two_prod(m, t[0]);
+  const dd r = two_sum(p.hi - 1.0, p.lo);  // p.hi - 1 is exact (Sterbenz)
+  const double rh = r.hi, rl = r.lo;
+  const dd sq = two_prod(rh, rh);
+  const dd s = two_sum(rh, -0.5 * sq.hi);
+  const double q =
+      CLEO_DD_THIRD_HI +
+      rh * (-0.25 + rh * (CLEO_DD_FIFTH_HI + rh * (-CLEO_DD_INV6_HI +
+                                                   rh * (CLEO_DD_SEVENTH_HI + rh * -0.125))));
+  // r^2/2 = rh^2/2 + rh rl + rl^2/2 (the last below 2^-115 |r|); r^3 q rounded: below 2^-72 |r|
+  const double low = rl - 0.5 * sq.lo - rh * rl + (rh * sq.hi) * q;
+  const dd l1p = fast_two_sum(s.hi, s.lo + low);
+  dd eln2 = two_prod((double)e, CLEO_DD_LN2_HI);
+  eln2.lo += (double)e * CLEO_DD_LN2_LO;
+  return dd_add(eln2, dd_add(dd{t[1], t[2]}, l1p));
+}
+
+// exp of a double-double with |a.hi| < 600, relative error below 2^-72: a = n ln2/512 + r,
+// |r| <= ln2/1024 (2^-10.5), exp(r) - 1 = r + r^2/2 + ... + r^5/120 (remainder below 2^-72).
+CLEO_MATH_HD dd fast_exp(dd a) {
+#if defined(__CUDA_ARCH__)
+  using namespace cleo_dd_dev;
+#else
+  using namespace cleo_dd_host;
+#endif
+  const double nf = std::rint(a.hi * (512.0 * CLEO_DD_INV_LN2));
+  const int n = (int)nf;
+  const int j = n & 511;
+  const int k = (n - j) / 512;
+  const dd p = two_prod(nf, CLEO_DD_LN2_HI * 0x1p-9);
+  dd r = dd_add(a, dd{-p.hi, -p.lo});
+  r = dd_add_d(r, -nf * (CLEO_DD_LN2_LO * 0x1p-9));
+  const double rh = r.hi, rl = r.lo;
+  const double poly =
+      rh * rh * (0.5 + rh * (CLEO_DD_INV6_HI + rh * (CLEO_DD_INV24_HI + rh * CLEO_DD_INV120_HI)));
+  const dd em1 = fast_two_sum(rh, rl + rh * rl + poly);
+  const dd tj{cleo_fast_exp2_tab[j][0], cleo_fast_exp2_tab[j][1]};
+  dd v = dd_add(tj, dd_mul(tj, em1));
+  v.hi = std::ldexp(v.hi, k);
+  v.lo = std::ldexp(v.lo, k);
+  return v;
+}
+
+// true when every value within FAST_ERR |v| of v.hi + v.lo (v positive, normalised, normal)
+// rounds to v.hi
+CLEO_MATH_HD bool fast_round_ok(dd v) {
+  const uint64_t b = dbits(v.hi);
+  const uint64_t ex = (b >> 52) & 0x7FF;
+  if (ex <= 53 || ex >= 0x7FF) return false;
+  const double u = bitsd((ex - 52) << 52);  // spacing of the doubles above v.hi
+  const double d_up = 0.5 * u;
+  const double d_down = ((b & 0xFFFFFFFFFFFFFull) == 0) ? 0.25 * u : 0.5 * u;
+  const double err = FAST_ERR * v.hi;
+  return (v.lo + err < d_up) && (v.lo - err > -d_down);
+}
+
+// exp(x), rounded once (first phase, then the double-double phase when needed)
+CLEO_MATH_HD double dexp(double x) {
+  if (x > -600.0 && x < 600.0) {
+    const dd v = fast_exp(dd{x, 0.0});
+    if (fast_round_ok(v)) return v.hi;
+  }
+  return dexp_dd(x);
+}
+
+// pow(x, y) for the exponents CLEO uses, rounded once
 CLEO_MATH_HD double dpow(double x, double y) {
   if (y == 2.0) return x * x;
   if (y == 0.5 && x >= 0.0) return std::sqrt(x);
@@ -187,9 +304,40 @@ CLEO_MATH_HD double dpow(double x, double y) {
     const dd x2 = two_prod(x, x);
     return round_dd(dd_mul_d(x2, x));
   }
-  const dd z = dd_mul_d(dd_log(x), y);
-  if (!(z.hi > -707.0 && z.hi < 707.0)) return std::pow(x, y);
-  return round_dd(dd_exp(z));
+  const dd z = dd_mul_d(fast_log(x), y);
+  if (z.hi > -600.0 && z.hi < 600.0) {
+    const dd v = fast_exp(z);
+    if (fast_round_ok(v)) return v.hi;
+  }
+  return dpow_dd(x, y);
+}
+
+// dpow(x, y1) and dpow(x, y2) with one logarithm (same results as two dpow calls; for general
+// exponents, i.e. not 0.5, 1, 2 or 3)
+CLEO_MATH_HD void dpow2(double x, double y1, double y2, double& p1, double& p2) {
+  if (!(x > 2.2250738585072014e-308) || !(x < 1.7976931348623157e308)) {
+    p1 = dpow(x, y1);
+    p2 = dpow(x, y2);
+    return;
+  }
+  const dd lx = fast_log(x);
+  const double ys[2] = {y1, y2};
+  double out[2];
+  for (int q = 0; q < 2; ++q) {
+    const dd z = dd_mul_d(lx, ys[q]);
+    out[q] = 0.0;
+    bool done = false;
+    if (z.hi > -600.0 && z.hi < 600.0) {
+      const dd v = fast_exp(z);
+      if (fast_round_ok(v)) {
+        out[q] = v.hi;
+        done = true;
+      }
+    }
+    if (!done) out[q] = dpow_dd(x, ys[q]);
+  }
+  p1 = out[0];
+  p2 = out[1];
 }
 
 }  // namespace cleo

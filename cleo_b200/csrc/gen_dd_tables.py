@@ -42,6 +42,24 @@ def main():
         hi, lo = split(v)
         out.append(f"  {{{hi.hex()}, {lo.hex()}}},")
     out.append("};")
+    # fast first phase of log: centres c = i/512 of the reduced mantissa (i = 362..724), the
+    # double rc = RN(1/c) and -ln(rc) exactly for that double, as (rc, hi, lo)
+    out.append("// fast log: rc = RN(512/i) and -ln(rc) as double-double, i = 362..724")
+    out.append("CLEO_DD_TABLE double cleo_fast_log_tab[363][3] = {")
+    for i in range(362, 725):
+        rc = float(Decimal(512) / Decimal(i))
+        v = -Decimal(rc).ln()
+        hi, lo = split(v)
+        out.append(f"  {{{rc.hex()}, {hi.hex()}, {lo.hex()}}},")
+    out.append("};")
+    # fast first phase of exp: 2^(j/512), j = 0..511
+    out.append("// fast exp: 2^(j/512) for j = 0..511")
+    out.append("CLEO_DD_TABLE double cleo_fast_exp2_tab[512][2] = {")
+    for j in range(512):
+        v = Decimal(2) ** (Decimal(j) / 512)
+        hi, lo = split(v)
+        out.append(f"  {{{hi.hex()}, {lo.hex()}}},")
+    out.append("};")
     # series coefficients needed in double-double
     for name, v in (("THIRD", Decimal(1) / 3), ("FIFTH", Decimal(1) / 5), ("SEVENTH", Decimal(1) / 7),
                     ("INV6", Decimal(1) / 6), ("INV24", Decimal(1) / 24), ("INV120", Decimal(1) / 120)):

@@ -449,8 +449,10 @@ __device__ __forceinline__ double ventilation_factor(double radius) {
   const double A = 1.963;
   const double C2 = 1.069e+3;
   const double B = 0.702;
-  const double a = 1.0 / (C1 * dpow(radius * R0, A));
-  const double b = 1.0 / (C2 * dpow(radius * R0, B));
+  double pa, pb;  // pow(radius * R0, A) and pow(radius * R0, B), one logarithm
+  dpow2(radius * R0, A, B, pa, pb);
+  const double a = 1.0 / (C1 * pa);
+  const double b = 1.0 / (C2 * pb);
   const double vent_factor = 1.0 + 1.0 / (a + b);
   return fmin(vent_factor, vent_factor_max);
 }
@@ -475,60 +477,113 @@ struct NewtonCfg {
 // CLEO_ERR_TIMEOUT, so that no thread can spin for long.
 constexpr uint32_t NR_ITER_CAP = 4u << 20;
 
-__device__ __forceinline__ double ode_gfunc(const OdeConsts& o, double subdelt, double rprev,
-                                            double rsqrd) {  // :270-281
-  const double radius = sqrt(rsqrd);
-  const double alpha = o.s_ratio - 1 - o.akoh / radius + o.bkoh / dpow(radius, 3.0);
+// ode_gfunc (:270-281) at one iterate z = r^2, keeping the terms that ode_gfuncderivative
+// (:291-301) shares at the same z. The reference evaluates g at each new iterate twice (as the
+// convergence check of one iteration and as the numerator of the next) and recomputes sqrt(z),
+// z^(3/2) and akoh/r for g'; one evaluation per iterate gives the same doubles, because each
+// value is the same expression of the same inputs.
+struct GEval {
+  double z, radius, akr, r3, g;
+};
+__device__ __forceinline__ GEval eval_g(const OdeConsts& o, double subdelt, double rprev,
+                                        double rsqrd) {
+  GEval e;
+  e.z = rsqrd;
+  e.radius = sqrt(rsqrd);
+  e.akr = o.akoh / e.radius;
+  e.r3 = dpow(e.radius, 3.0);
+  const double alpha = o.s_ratio - 1 - e.akr + o.bkoh / e.r3;
   const double beta = 2.0 * subdelt / (rsqrd * o.ffactor_fv);
-  const double gamma = dpow(rprev / radius, 2.0);
-  return 1 - gamma - alpha * beta;
+  const double gamma = dpow(rprev / e.radius, 2.0);
+  e.g = 1 - gamma - alpha * beta;
+  return e;
 }
-__device__ __forceinline__ double ode_gfuncderivative(const OdeConsts& o, double subdelt,
-                                                      double rsqrd) {  // :291-301
-  const double radius = sqrt(rsqrd);
-  const double alpha = o.akoh / radius - 3.0 * o.bkoh / dpow(radius, 3.0);
-  const double beta = subdelt / (rsqrd * o.ffactor_fv);
+__device__ __forceinline__ double eval_gprime(const OdeConsts& o, double subdelt, const GEval& e) {
+  const double alpha = e.akr - 3.0 * o.bkoh / e.r3;
+  const double beta = subdelt / (e.z * o.ffactor_fv);
   return 1 - alpha * beta;
 }
 // iterate_rootfinding_algorithm: impliciteuler.cpp:239-255 (+ check_for_convergence, hpp:213-219)
-__device__ __forceinline__ double nr_iterate(const NewtonCfg& c, const OdeConsts& o,
-                                             double subdelt, double rprev, double ziter,
-                                             bool& converged, uint32_t& niters) {
-  const double numerator = ode_gfunc(o, subdelt, rprev, ziter);
-  const double denominator = ode_gfuncderivative(o, subdelt, ziter);
-  ziter = ziter * (1 - numerator / denominator);
+__device__ __forceinline__ GEval nr_iterate(const NewtonCfg& c, const OdeConsts& o,
+                                            double subdelt, double rprev, const GEval& e,
+                                            bool& converged, uint32_t& niters) {
+  const double numerator = e.g;
+  const double denominator = eval_gprime(o, subdelt, e);
+  double ziter = e.z * (1 - numerator / denominator);
   ziter = fmax(ziter, 1e-8);
-  const double newnumerator = ode_gfunc(o, subdelt, rprev, ziter);
-  const double conv = c.rtol * fabs(newnumerator) + c.atol;
-  converged = fabs(newnumerator - numerator) < conv;
+  const GEval next = eval_g(o, subdelt, rprev, ziter);
+  const double conv = c.rtol * fabs(next.g) + c.atol;
+  converged = fabs(next.g - numerator) < conv;
   ++niters;
-  return ziter;
+  return next;
 }
 // integrate_condensation_ode: impliciteuler.cpp:128-141 with newtonraphson_niterations (:181-194)
-// and newtonraphson_untilconverged (:207-227)
-__device__ __forceinline__ double integrate_ode(const NewtonCfg& c, const OdeConsts& o,
-                                                double subdelt, double rprev, double ziter,
-                                                uint32_t& niters, const Where& w) {
+// and newtonraphson_untilconverged (:207-227). e0 is g at the initial guess. Returns 0 or the
+// failure code; z receives the last iterate either way.
+__device__ __forceinline__ int integrate_ode_core(const NewtonCfg& c, const OdeConsts& o,
+                                                  double subdelt, double rprev, const GEval& e0,
+                                                  uint32_t& niters, double& z) {
   bool conv = false;
-  double z = ziter;
-  for (int it = 0; it < 2; ++it) z = nr_iterate(c, o, subdelt, rprev, z, conv, niters);
-  if (conv) return z;
-  z = ziter;
+  GEval e = e0;
+  for (int it = 0; it < 2; ++it) e = nr_iterate(c, o, subdelt, rprev, e, conv, niters);
+  if (conv) {
+    z = e.z;
+    return 0;
+  }
+  e = e0;
   conv = false;
   uint32_t niter = 1;
+  int code = 0;
   while (!conv) {
     if (niter > c.maxniters) {
-      w.fail(CLEO_ERR_NR_NOCONVERGE);
+      code = CLEO_ERR_NR_NOCONVERGE;
       break;
     }
     if (niters >= NR_ITER_CAP) {
-      w.fail(CLEO_ERR_TIMEOUT);
+      code = CLEO_ERR_TIMEOUT;
       break;
     }
-    z = nr_iterate(c, o, subdelt, rprev, z, conv, niters);
+    e = nr_iterate(c, o, subdelt, rprev, e, conv, niters);
     niter += 1;
   }
+  z = e.z;
+  return code;
+}
+__device__ __forceinline__ double integrate_ode(const NewtonCfg& c, const OdeConsts& o,
+                                                double subdelt, double rprev, const GEval& e0,
+                                                uint32_t& niters, const Where& w) {
+  double z;
+  const int code = integrate_ode_core(c, o, subdelt, rprev, e0, niters, z);
+  if (code) w.fail(code);
   return z;
+}
+// a usable seed: finite and positive (NaN compares false)
+__device__ __forceinline__ bool seed_ok(double seed_rsqrd) {
+  return seed_rsqrd > 0.0 && seed_rsqrd <= DBLMAX;
+}
+// Newton iterations from a seed, the convergence test (check_for_convergence) after every one,
+// at most SEED_MAXITERS: a good seed converges in one or two, a poor one is abandoned early
+// (the caller then starts from the reference guess). Returns true when converged.
+constexpr uint32_t SEED_MAXITERS = 6;
+__device__ __forceinline__ bool integrate_seeded(const NewtonCfg& c, const OdeConsts& o,
+                                                 double subdelt, double rprev, GEval e,
+                                                 uint32_t& niters, double& z) {
+  bool conv = false;
+  for (uint32_t k = 0; k < SEED_MAXITERS; ++k) {
+    e = nr_iterate(c, o, subdelt, rprev, e, conv, niters);
+    if (conv) break;
+  }
+  z = e.z;
+  return conv;
+}
+// Whether a root reached from a seed is the root the reference's guess leads to. With
+// h(z) = z g(z) = z - rprev^2 - (2 delt / F)(s - 1 - a/r + b/r^3), h'(z) = 1 - (delt/F) f'(r)/r
+// with f'(r) = a/r^2 - 3b/r^4, whose largest value over r (at r^2 = 5b/a) keeps h' > 0 exactly
+// when delt < 2.5 F/a (5b/a)^1.5, the critical timestep: then the root is unique. Otherwise the
+// direct branch was taken for an unactivated droplet (ucrit1), and h is increasing only on
+// (0, 3b/a], where f' < 0; a seeded root is accepted there, where it is the only one.
+__device__ __forceinline__ bool seeded_root_ok(const OdeConsts& o, bool ucrit1, double z) {
+  return !ucrit1 || z <= 3.0 * o.bkoh / o.akoh;
 }
 __device__ __forceinline__ double initialguess(const OdeConsts& o, double rprev) {  // :156-170
   const double s_act = 1 + sqrt(4.0 * dpow(o.akoh, 3.0) / 27 / o.bkoh);
@@ -554,8 +609,8 @@ __device__ __forceinline__ double critical_timestep(const OdeConsts& o) {  // hp
   const double cuberoot = dpow(5.0 * o.bkoh / o.akoh, 1.5);
   return 2.5 * o.ffactor_fv / o.akoh * cuberoot;
 }
-// solve_condensation: impliciteuler.cpp:35-54 (+ substepping :98-113). seed_rsqrd > 0 replaces
-// the Newton start (not the branch decision) by a predicted r^2.
+// solve_condensation: impliciteuler.cpp:35-54 (+ substepping :98-113). A usable seed_rsqrd
+// replaces the Newton start of the direct branch (not the branch decision) by a predicted r^2.
 __device__ __forceinline__ double solve_condensation(const NewtonCfg& c, double delt,
                                                      double minsubdelt, double s_ratio,
                                                      double akoh, double bkoh, double ffactor,
@@ -564,12 +619,23 @@ __device__ __forceinline__ double solve_condensation(const NewtonCfg& c, double 
   const double ffactor_fv = ffactor / ventilation_factor(rprev);
   const OdeConsts o{s_ratio, akoh, bkoh, ffactor_fv};
   double ziter = initialguess(o, rprev);
+  // ucrit1 || ucrit2: the critical timestep (a general pow) is only needed when ucrit1 fails
   const bool ucrit1 = first_unique_criteria(o, rprev, ziter);
-  const bool ucrit2 = (delt <= critical_timestep(o));
+  const bool direct = ucrit1 || (delt <= critical_timestep(o));
   double rsqrd;
-  if (ucrit1 || ucrit2) {
-    if (seed_rsqrd > 0.0) ziter = seed_rsqrd;
-    rsqrd = integrate_ode(c, o, delt, rprev, ziter, niters, w);
+  if (direct) {
+    const GEval e0 = eval_g(o, delt, rprev, ziter);
+    // a seed is used when its residual is smaller than the reference guess's; a seeded solve
+    // that does not converge within SEED_MAXITERS, or ends on another root, restarts from the
+    // reference's guess
+    bool done = false;
+    if (seed_ok(seed_rsqrd)) {
+      const GEval es = eval_g(o, delt, rprev, seed_rsqrd);
+      if (fabs(es.g) < fabs(e0.g) && integrate_seeded(c, o, delt, rprev, es, niters, rsqrd) &&
+          seeded_root_ok(o, ucrit1, rsqrd))
+        done = true;
+    }
+    if (!done) rsqrd = integrate_ode(c, o, delt, rprev, e0, niters, w);
   } else {
     const double critdelt = critical_timestep(o);
     const double mindelt = fmax(critdelt, minsubdelt);
@@ -580,7 +646,7 @@ __device__ __forceinline__ double solve_condensation(const NewtonCfg& c, double 
         break;
       }
       const double subdelt = fmin(mindelt, remdelt);
-      ziter = integrate_ode(c, o, subdelt, rprev, ziter, niters, w);
+      ziter = integrate_ode(c, o, subdelt, rprev, eval_g(o, subdelt, rprev, ziter), niters, w);
       rprev = dpow(ziter, 0.5);
       remdelt -= subdelt;
     }

@@ -20,9 +20,13 @@
 
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
+#include <string>
 #include <vector>
 
+#include "mlp.cuh"
 #include "physics.cuh"
 #include "sort.cuh"
 
@@ -67,6 +71,19 @@ struct DevCtx {
   DevError* err;
 };
 
+// droplet inputs of cleo_b200_condensation_solve -> Newton seed r^2 (the surrogate's IO)
+struct CondSeedIO {
+  const double *radius, *msol, *temp, *press, *s_ratio, *delt;
+  double* seed;
+  __device__ __forceinline__ void features(uint32_t i, float x[mlp::NIN]) const {
+    mlp::raw_features(radius[i], msol[i], temp[i], press[i], s_ratio[i], delt[i], x);
+  }
+  __device__ __forceinline__ void store(uint32_t i, float t) const {
+    const double r = radius[i];
+    seed[i] = r * r * exp((double)t);
+  }
+};
+
 }  // namespace
 
 #include "batched_types.cuh"
@@ -93,6 +110,38 @@ struct cleo_b200_ctx {
   };
   std::vector<Mark> marks;
   std::vector<cudaEvent_t> event_pool;
+  // launch configuration of the batched schedule (results do not depend on it) and the online
+  // autotuner that chooses it by timing candidates on live steps
+  struct TuneCfg {
+    int cond_block;       // threads per block of pass A
+    int condb_mult;       // pass-B grid = multiple of the resident-CTA count
+    uint32_t small_max;   // bucket thresholds of the collision kernels
+    uint32_t medium_max;
+  };
+  TuneCfg cfg{256, 1, SMALL_MAX, MEDIUM_MAX};
+  std::vector<TuneCfg> cand;
+  std::vector<double> t_cond, t_coll;
+  size_t tune_step = 0, tune_total = 0;
+  std::string tune_key;
+  // CUDA graphs of batched SDM steps, keyed by what decides a step's launch sequence (the
+  // current SoA buffer, motion on/off, the step length and the sub-step pattern)
+  struct StepGraph {
+    std::vector<uint32_t> sig;
+    cudaGraphExec_t exec;
+    int cur_after;
+    unsigned long long nodes;
+  };
+  std::vector<StepGraph> graphs;
+  bool use_graphs = true;
+  uint32_t t_dev = 0xFFFFFFFFu;  // the step time the device word holds (host mirror)
+  void drop_graphs() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+    graphs.clear();
+  }
+  // condensation surrogate (nr_seed = CLEO_NRSEED_MLP) and its seed buffer for condensation_solve
+  const cleo_b200_mlp* mlp = nullptr;
+  double* seed_buf = nullptr;
+  size_t seed_cap = 0;
   cudaEvent_t take_event() {
     if (!event_pool.empty()) {
       cudaEvent_t e = event_pool.back();
@@ -602,8 +651,8 @@ k_micro(DevCtx c, uint32_t t_sdm, uint32_t t_sdm_next, int did_motion) {
 __global__ void k_condsolve(DevCtx c, uint32_t n, const double* __restrict__ radius,
                             const double* __restrict__ msol, const double* __restrict__ temp,
                             const double* __restrict__ press, const double* __restrict__ s_ratio,
-                            const double* __restrict__ delt, double* __restrict__ out,
-                            uint32_t* __restrict__ niters_out) {
+                            const double* __restrict__ delt, const double* __restrict__ seeds,
+                            double* __restrict__ out, uint32_t* __restrict__ niters_out) {
   const NewtonCfg cfg{c.p.maxniters, c.p.rtol, c.p.atol};
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const Where w{c.err, OOB, i};
@@ -614,7 +663,8 @@ __global__ void k_condsolve(DevCtx c, uint32_t n, const double* __restrict__ rad
     kohler_factors(msol[i], T, akoh, bkoh);
     uint32_t ni = 0;
     const double newr = solve_condensation(cfg, delt[i], c.p.cond_minsubdelt, s_ratio[i], akoh,
-                                           bkoh, ffactor, radius[i], 0.0, ni, w);
+                                           bkoh, ffactor, radius[i], seeds ? seeds[i] : 0.0, ni,
+                                           w);
     out[i] = fmax(newr, dryradius(msol[i]));
     if (niters_out) niters_out[i] = ni;
   }
@@ -723,6 +773,8 @@ int radix_pairs(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, uint
 int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, bool did_motion) {
   DevCtx& d = x->d;
   BatchScratch& b = x->bs;
+  b.small_max = x->cfg.small_max;
+  b.medium_max = x->cfg.medium_max;
   cudaStream_t s = x->stream;
   StageMark m(x, 2);
   const int gg = grid_for(d.ngbxs, 256);
@@ -740,25 +792,39 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
     if (cond) {
       StageMark mc(x, 3);
       k_b_thermo<<<gg, 256, 0, s>>>(d, b);
-      k_cond_a<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, b);
-      x->launches += 2;
+      x->launches += 1;
+      if (d.p.nr_seed == CLEO_NRSEED_MLP) {  // surrogate seeds into b.dm (read by pass A / B)
+        mlp::Infer w;
+        if (cleo_mlp_infer_view(x->mlp, &w) != CLEO_OK) return CLEO_ERR_MLP;
+        w.err = reinterpret_cast<uint32_t*>(&d.err->code);
+        const SdmSeedIO io{d.sd.gbx, d.sd.r, d.sd.msol, d.temp, d.press, b.th_s, d.p.cond_delt,
+                           d.ngbxs, d.counters, b.dm};
+        const uint32_t tiles = (d.capacity + mlp::TILE_M - 1) / mlp::TILE_M;
+        mlp::k_mlp_tc<SdmSeedIO><<<tiles < 148u * 4u ? tiles : 148u * 4u, 128, mlp::TC_SMEM, s>>>(
+            w, io, d.capacity);
+        x->launches += 1;
+      }
+      k_cond_a<<<grid_for(d.capacity, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
+      x->launches += 1;
       const int where = radix_pairs(x, b.lkeys, b.lvals, x->keys[1], x->vals[1], b.ctr, 16);
       if (where != 0) return CLEO_ERR_CUDA;  // 16 key bits: two passes, result back in place
-      k_cond_b<<<x->grid_flat, 256, 0, s>>>(d, b);
+      k_cond_b<<<x->grid_flat * x->cfg.condb_mult, 256, 0, s>>>(d, b);
       x->launches += 1;
     }
     if (cond || coll) {
       StageMark mk(x, 4);
       k_b_reset<<<1, 32, 0, s>>>(d, b, 0);
       k_b_classify<<<gg, 256, 0, s>>>(d, b);
-      k_b_small<<<x->grid_small, B_THREADS, 0, s>>>(d, b, t_sdm, cond ? 1 : 0, coll ? 1 : 0);
-      k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_MAX * 32, s>>>(d, b, t_sdm, cond ? 1 : 0,
+      k_b_small<<<x->grid_small, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
+      k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_MAX * 32, s>>>(d, b, cond ? 1 : 0,
                                                                            coll ? 1 : 0);
-      k_b_cta<true><<<x->grid_large, B_THREADS, 0, s>>>(d, b, t_sdm, cond ? 1 : 0, coll ? 1 : 0);
+      k_b_cta<true><<<x->grid_large, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
       x->launches += 5;
     }
     subt = min(next_step(d.p.condstep, subt), next_step(d.p.collstep, subt));
   }
+  k_b_advance_t<<<1, 1, 0, s>>>(b, t_sdm_next - t_sdm);
+  x->launches += 1;
   CUDA_TRY(cudaGetLastError());
   return CLEO_OK;
 }
@@ -791,6 +857,123 @@ int run_sdm_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
   return CLEO_OK;
 }
 
+// ---- autotuner ----
+// Candidate launch configurations are timed on live batched steps (per-stage CUDA events): the
+// condensation options (pass-A block, pass-B grid) and the collision options (bucket
+// thresholds) are scored independently and the fastest of each kept. Chosen configurations are
+// cached per process by GPU name and domain size, so later contexts start from them.
+std::mutex g_tune_mutex;
+std::map<std::string, cleo_b200_ctx::TuneCfg> g_tune_cache;
+
+const cleo_b200_ctx::TuneCfg COND_OPTS[4] = {
+    {128, 1, 0, 0}, {256, 1, 0, 0}, {128, 2, 0, 0}, {256, 2, 0, 0}};
+const cleo_b200_ctx::TuneCfg COLL_OPTS[4] = {
+    {0, 0, 32, 512}, {0, 0, SMALL_MAX, 512}, {0, 0, 32, MEDIUM_MAX}, {0, 0, SMALL_MAX, MEDIUM_MAX}};
+
+std::string tune_key(const cleo_b200_ctx* x) {
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, x->device) != cudaSuccess) return std::string();
+  uint32_t lg = 0;
+  while ((1ull << lg) < (unsigned long long)x->d.capacity) ++lg;
+  return std::string(prop.name) + "|" + std::to_string(x->d.ngbxs) + "|" + std::to_string(lg);
+}
+
+// one tuning step: run the step eagerly with stage events, score the candidate, and when all
+// candidates have been timed choose the fastest
+int run_tuning_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
+  const size_t k = x->tune_step % 4;
+  x->cfg.cond_block = COND_OPTS[k].cond_block;
+  x->cfg.condb_mult = COND_OPTS[k].condb_mult;
+  x->cfg.small_max = COLL_OPTS[k].small_max;
+  x->cfg.medium_max = COLL_OPTS[k].medium_max;
+  const bool prof = x->profiling;
+  const size_t m0 = x->marks.size();
+  x->profiling = true;
+  const int rc = run_sdm_step(x, t_sdm, t_sdm_next);
+  x->profiling = prof;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  double tc = 0.0, tl = 0.0;
+  for (size_t i = m0; i < x->marks.size(); ++i) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, x->marks[i].a, x->marks[i].b);
+    if (x->marks[i].stage == 3) tc += ms;
+    if (x->marks[i].stage == 4) tl += ms;
+    if (!prof) {
+      x->event_pool.push_back(x->marks[i].a);
+      x->event_pool.push_back(x->marks[i].b);
+    }
+  }
+  if (!prof) x->marks.resize(m0);
+  if (rc != CLEO_OK) return rc;
+  x->t_cond[k] += tc;
+  x->t_coll[k] += tl;
+  if (++x->tune_step == x->tune_total) {
+    size_t bc = 0, bl = 0;
+    for (size_t i = 1; i < 4; ++i) {
+      if (x->t_cond[i] < x->t_cond[bc]) bc = i;
+      if (x->t_coll[i] < x->t_coll[bl]) bl = i;
+    }
+    x->cfg = {COND_OPTS[bc].cond_block, COND_OPTS[bc].condb_mult, COLL_OPTS[bl].small_max,
+              COLL_OPTS[bl].medium_max};
+    x->tune_total = 0;
+    x->drop_graphs();
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[x->tune_key] = x->cfg;
+  }
+  return CLEO_OK;
+}
+
+// The launch sequence of one batched SDM step as a CUDA graph: captured the first time a
+// signature is seen, replayed afterwards. The injected random numbers are keyed by the device
+// word bs.tsdm, so a replay needs no parameter update.
+int run_step_graphed(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
+  const cleo_b200_params& p = x->d.p;
+  std::vector<uint32_t> sig;
+  sig.push_back((uint32_t)x->cur);
+  sig.push_back(on_step(p.motionstep, t_sdm) ? 1u : 0u);
+  sig.push_back(t_sdm_next - t_sdm);
+  for (uint32_t subt = t_sdm; subt < t_sdm_next;
+       subt = min(next_step(p.condstep, subt), next_step(p.collstep, subt))) {
+    sig.push_back(subt - t_sdm);
+    sig.push_back((on_step(p.condstep, subt) ? 1u : 0u) | (on_step(p.collstep, subt) ? 2u : 0u));
+  }
+  for (auto& g : x->graphs) {
+    if (g.sig == sig) {
+      CUDA_TRY(cudaGraphLaunch(g.exec, x->stream));
+      x->cur = g.cur_after;
+      x->d.sd = x->buf[x->cur];
+      x->launches += g.nodes;
+      return CLEO_OK;
+    }
+  }
+  if (x->graphs.size() >= 8) x->drop_graphs();
+  const int cur0 = x->cur;
+  const unsigned long long l0 = x->launches;
+  CUDA_TRY(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = run_sdm_step(x, t_sdm, t_sdm_next);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(x->stream, &graph);
+  const unsigned long long nodes = x->launches - l0;
+  x->launches = l0;
+  const int cur_after = x->cur;
+  x->cur = cur0;  // nothing has run yet
+  x->d.sd = x->buf[x->cur];
+  cudaGraphExec_t exec = nullptr;
+  if (rc != CLEO_OK || ce != cudaSuccess || !graph ||
+      cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return rc != CLEO_OK ? rc : CLEO_ERR_CUDA;
+  }
+  cudaGraphDestroy(graph);
+  x->graphs.push_back({sig, exec, cur_after, nodes});
+  CUDA_TRY(cudaGraphLaunch(exec, x->stream));
+  x->cur = cur_after;
+  x->d.sd = x->buf[x->cur];
+  x->launches += nodes;
+  return CLEO_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -804,6 +987,11 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   if (params->condstep != CLEO_STEP_OFF && params->cond_delt < params->cond_minsubdelt)
     return CLEO_ERR_SUBDELT;  // ImplicitEuler ctor, impliciteuler.hpp:320-326
   if (params->condstep == 0 || params->collstep == 0 || params->motionstep == 0)
+    return CLEO_ERR_ARGUMENT;
+  // the surrogate seeds the batched schedule; the plain schedule is the unseeded form
+  if (params->nr_seed == CLEO_NRSEED_MLP && params->exec_mode != CLEO_EXEC_BATCHED)
+    return CLEO_ERR_ARGUMENT;
+  if (params->nr_seed != CLEO_NRSEED_REFERENCE && params->nr_seed != CLEO_NRSEED_MLP)
     return CLEO_ERR_ARGUMENT;
   // a sub-stepping loop needs a positive minimum sub-step, and Newton solves a finite budget
   if (params->condstep != CLEO_STEP_OFF &&
@@ -862,6 +1050,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &x->bs.bucket, 3 * ng);
   rc |= dalloc(x, &x->bs.slot, ng);
   rc |= dalloc(x, &x->bs.ctr, 8);
+  rc |= dalloc(x, &x->bs.tsdm, 1);
   rc |= dalloc(x, &x->tile_sums, ((size_t)256 * x->ntiles_max + SCAN_TILE - 1) / SCAN_TILE + 1);
   if (rc) {
     cleo_b200_destroy(x);
@@ -897,6 +1086,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   CUDA_TRY(cudaMemsetAsync(d.err, 0, sizeof(DevError), x->stream));
   CUDA_TRY(cudaFuncSetAttribute(k_micro, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MICRO_SMEM));
   CUDA_TRY(cudaMemsetAsync(x->bs.ctr, 0, 32, x->stream));
+  CUDA_TRY(cudaMemsetAsync(x->bs.tsdm, 0, 4, x->stream));
   CUDA_TRY(cudaMemsetAsync(x->bs.slot, 0, (ng ? ng : 1) * 4, x->stream));
   {  // persistent grids of the batched kernels: full occupancy on every SM
     int dev = 0, sms = 148, occ = 1;
@@ -912,6 +1102,12 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cond_b, 256, 0));
     x->grid_flat = sms * (occ > 0 ? occ : 1);
   }
+  x->tune_key = tune_key(x);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    const auto it = g_tune_cache.find(x->tune_key);
+    if (it != g_tune_cache.end()) x->cfg = it->second;
+  }
   CUDA_TRY(cudaStreamSynchronize(x->stream));
   *out = x;
   return CLEO_OK;
@@ -925,6 +1121,8 @@ void cleo_b200_destroy(cleo_b200_ctx* x) {
     cudaEventDestroy(m.b);
   }
   for (auto e : x->event_pool) cudaEventDestroy(e);
+  x->drop_graphs();
+  cudaFree(x->seed_buf);
   for (void* p : x->allocs) cudaFree(p);
   if (x->own_stream && x->stream) cudaStreamDestroy(x->stream);
   delete x;
@@ -1012,14 +1210,59 @@ int cleo_b200_upload_state(cleo_b200_ctx* x, const cleo_b200_gbx_state* h) {
 
 int cleo_b200_step(cleo_b200_ctx* x, uint32_t t_mdl, uint32_t t_next) {
   if (!x) return CLEO_ERR_ARGUMENT;
+  if (x->d.p.nr_seed == CLEO_NRSEED_MLP && x->d.p.condstep != CLEO_STEP_OFF && !x->mlp)
+    return CLEO_ERR_MLP;
+  const bool batched = x->d.p.exec_mode == CLEO_EXEC_BATCHED;
   uint32_t t_sdm = t_mdl;
   while (t_sdm < t_next) {
     const uint32_t next_move = next_step(x->d.p.motionstep, t_sdm);
     const uint32_t t_sdm_next = t_next < next_move ? t_next : next_move;
-    const int rc = run_sdm_step(x, t_sdm, t_sdm_next);
+    int rc;
+    if (batched) {
+      if (x->t_dev != t_sdm) {
+        k_b_set_t<<<1, 1, 0, x->stream>>>(x->bs, t_sdm);
+        x->launches += 1;
+      }
+      x->t_dev = 0xFFFFFFFFu;
+      if (x->tune_step < x->tune_total)
+        rc = run_tuning_step(x, t_sdm, t_sdm_next);
+      else
+        rc = (x->use_graphs && !x->profiling) ? run_step_graphed(x, t_sdm, t_sdm_next)
+                                              : run_sdm_step(x, t_sdm, t_sdm_next);
+      if (rc == CLEO_OK) x->t_dev = t_sdm_next;
+    } else {
+      rc = run_sdm_step(x, t_sdm, t_sdm_next);
+    }
     if (rc) return rc;
     t_sdm = t_sdm_next;
   }
+  return CLEO_OK;
+}
+
+int cleo_b200_autotune(cleo_b200_ctx* x, int reps) {
+  if (!x || reps < 1 || reps > 1000 || x->d.p.exec_mode != CLEO_EXEC_BATCHED)
+    return CLEO_ERR_ARGUMENT;
+  x->tune_step = 0;
+  x->tune_total = (size_t)4 * (size_t)reps;
+  x->t_cond.assign(4, 0.0);
+  x->t_coll.assign(4, 0.0);
+  return CLEO_OK;
+}
+
+int cleo_b200_tuned_config(cleo_b200_ctx* x, int32_t cfg[4]) {
+  if (!x || !cfg) return CLEO_ERR_ARGUMENT;
+  cfg[0] = x->cfg.cond_block;
+  cfg[1] = x->cfg.condb_mult;
+  cfg[2] = (int32_t)x->cfg.small_max;
+  cfg[3] = (int32_t)x->cfg.medium_max;
+  return x->tune_step < x->tune_total ? 1 : CLEO_OK;
+}
+
+int cleo_b200_set_graphs(cleo_b200_ctx* x, int on) {
+  if (!x) return CLEO_ERR_ARGUMENT;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  x->use_graphs = on != 0;
+  if (!x->use_graphs) x->drop_graphs();
   return CLEO_OK;
 }
 
@@ -1136,11 +1379,43 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_rad
     return CLEO_ERR_ARGUMENT;
   if (n >= 0xFFFFFFFFull) return CLEO_ERR_CAPACITY;
   if (n == 0) return CLEO_OK;
+  const double* seeds = nullptr;
+  if (x->d.p.nr_seed == CLEO_NRSEED_MLP) {
+    mlp::Infer w;
+    if (cleo_mlp_infer_view(x->mlp, &w) != CLEO_OK) return CLEO_ERR_MLP;
+    if (n > x->seed_cap) {
+      CUDA_TRY(cudaStreamSynchronize(x->stream));
+      cudaFree(x->seed_buf);
+      x->seed_buf = nullptr;
+      x->seed_cap = 0;
+      CUDA_TRY(cudaMalloc(&x->seed_buf, n * sizeof(double)));
+      x->seed_cap = n;
+    }
+    w.err = reinterpret_cast<uint32_t*>(&x->d.err->code);
+    const CondSeedIO io{d_radius, d_msol, d_temp, d_press, d_s_ratio, d_delt, x->seed_buf};
+    const uint32_t tiles = (uint32_t)((n + mlp::TILE_M - 1) / mlp::TILE_M);
+    mlp::k_mlp_tc<CondSeedIO><<<tiles < 148u * 4u ? tiles : 148u * 4u, 128, mlp::TC_SMEM,
+                                x->stream>>>(w, io, (uint32_t)n);
+    x->launches += 1;
+    seeds = x->seed_buf;
+  }
   k_condsolve<<<grid_for(n, 128), 128, 0, x->stream>>>(x->d, (uint32_t)n, d_radius, d_msol, d_temp,
-                                                       d_press, d_s_ratio, d_delt, d_radius_out,
-                                                       d_niters_out);
+                                                       d_press, d_s_ratio, d_delt, seeds,
+                                                       d_radius_out, d_niters_out);
   x->launches += 1;
   CUDA_TRY(cudaGetLastError());
+  return CLEO_OK;
+}
+
+int cleo_b200_set_surrogate(cleo_b200_ctx* x, cleo_b200_mlp* m) {
+  if (!x) return CLEO_ERR_ARGUMENT;
+  if (m) {
+    mlp::Infer w;
+    if (cleo_mlp_infer_view(m, &w) != CLEO_OK) return CLEO_ERR_ARGUMENT;
+  }
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  x->drop_graphs();  // captured steps hold the previous surrogate's weights
+  x->mlp = m;
   return CLEO_OK;
 }
 

@@ -276,6 +276,90 @@ int cleo_b200_stage_times(cleo_b200_ctx* ctx, double ms[5], uint64_t count[5]);
 int cleo_b200_sort_by_gridbox_static(const uint32_t* d_sdgbxindex, uint32_t n, uint32_t ngbxs,
                                      uint32_t* d_order, uint32_t* d_gstart, void* stream);
 
+/*
+ * Condensation surrogate (no counterpart in the reference, whose Newton-Raphson iteration always
+ * starts from ImplicitIterations::initialguess, impliciteuler.cpp:156-170). A 7 -> 64 -> 64 -> 1
+ * GELU multilayer perceptron predicts log(z_new / r^2) of one implicit-Euler condensation step
+ * (z = r^2) from the features log r, log msol, s_ratio - 1, T, p, delt, log(3 b / a)
+ * (dimensionless units). With nr_seed = CLEO_NRSEED_MLP and a surrogate attached to a context,
+ * its prediction replaces the initial guess of the branches whose root is unique (the branch
+ * decision itself is the reference's); a seeded solve that does not converge within maxniters
+ * restarts from the reference's guess. Weights: FP32 master copy for training, BF16 copies with
+ * FP32 accumulation for inference (layer 2 on tcgen05 tensor cores). All calls are on the stream
+ * given at creation and return once their results are ready.
+ */
+typedef struct cleo_b200_mlp cleo_b200_mlp;
+#define CLEO_MLP_NFEATURES 7
+#define CLEO_MLP_NHIDDEN 64
+#define CLEO_MLP_NPARAMS 4737 /* W1[64][7], b1[64], W2[64][64], b2[64], W3[64], b3 */
+#define CLEO_MLP_NNORM 16     /* feature means[7], feature inverse scales[7], target mean, scale */
+enum cleo_mlp_path {
+  CLEO_MLP_TCGEN05 = 0,  /* layer 2 by tcgen05.mma, accumulator in tensor memory */
+  CLEO_MLP_MMA_SYNC = 1, /* layer 2 by warp-level mma.sync m16n8k16 (check path) */
+  CLEO_MLP_FP32 = 2      /* scalar FP32 on the same BF16 operands (check path) */
+};
+/* New model on the current device, Glorot-uniform weights from `seed`, identity standardisation. */
+int cleo_b200_mlp_create(void* stream, uint64_t seed, cleo_b200_mlp** out);
+int cleo_b200_mlp_destroy(cleo_b200_mlp* mlp);
+/* Host arrays of CLEO_MLP_NPARAMS and CLEO_MLP_NNORM floats; set also resets the Adam state. */
+int cleo_b200_mlp_set_params(cleo_b200_mlp* mlp, const float* params, const float* norm);
+int cleo_b200_mlp_get_params(cleo_b200_mlp* mlp, float* params, float* norm);
+/*
+ * Raw features of n droplets (device arrays as cleo_b200_condensation_solve takes them) into
+ * d_features[n][7]. Optional: d_target[n] = log(r_new^2 / r^2) from d_radius_new, and d_direct[n]
+ * = 1 where solve_condensation takes its direct (non-sub-stepping) branch, the branch a seed
+ * applies to.
+ */
+int cleo_b200_mlp_features(cleo_b200_mlp* mlp, size_t n, const double* d_radius,
+                           const double* d_msol, const double* d_temp, const double* d_press,
+                           const double* d_s_ratio, const double* d_delt,
+                           const double* d_radius_new, float* d_features, float* d_target,
+                           uint8_t* d_direct);
+/* Feature and target means and scales from n training pairs (device arrays). */
+int cleo_b200_mlp_fit_normalisation(cleo_b200_mlp* mlp, size_t n, const float* d_features,
+                                    const float* d_target);
+/*
+ * Mean squared error of the standardised target over n samples (n <= 2^24) and its gradient with
+ * respect to the FP32 master parameters: d_grad[CLEO_MLP_NPARAMS], d_loss[1] (device, FP32).
+ */
+int cleo_b200_mlp_loss_grad(cleo_b200_mlp* mlp, size_t n, const float* d_features,
+                            const float* d_target, float* d_grad, float* d_loss);
+/*
+ * `steps` Adam steps (beta 0.9 / 0.999, linear warm-up then cosine decay of `lr`) on minibatches
+ * of `batch` samples (a multiple of 128) drawn uniformly from the n pairs by a counter generator
+ * keyed by `seed`. d_loss_per_step (device, optional) receives each step's minibatch loss.
+ */
+int cleo_b200_mlp_train(cleo_b200_mlp* mlp, size_t n, const float* d_features,
+                        const float* d_target, uint32_t steps, uint32_t batch, float lr,
+                        uint64_t seed, float* d_loss_per_step);
+/* Predicted log(z_new / r^2) of n feature rows into d_out[n] by one of cleo_mlp_path. */
+int cleo_b200_mlp_infer(cleo_b200_mlp* mlp, size_t n, const float* d_features, float* d_out,
+                        int path);
+/* Attach (or detach, with NULL) the surrogate that nr_seed = CLEO_NRSEED_MLP uses. */
+int cleo_b200_set_surrogate(cleo_b200_ctx* ctx, cleo_b200_mlp* mlp);
+
+/*
+ * CUDA graphs for the batched schedule (on by default; no counterpart in the reference). Each
+ * batched SDM step's launch sequence is captured once per distinct pattern (current buffer,
+ * motion, step length, sub-step pattern) and replayed as one graph launch afterwards; results
+ * are the same with graphs on or off. Steps run eagerly while stage profiling is on.
+ */
+int cleo_b200_set_graphs(cleo_b200_ctx* ctx, int on);
+
+/*
+ * Autotuner of the batched schedule (no counterpart in the reference). The next 4 * reps batched
+ * SDM steps run as ordinary steps (same results) while each times one of four candidate launch
+ * configurations per stage: pass-A block size and pass-B grid for condensation, the gridbox-size
+ * thresholds between the warp, shared-memory CTA and global-scratch CTA collision kernels. The
+ * fastest option of each stage is kept, and cached per process by GPU name and domain size so
+ * that later contexts of that size start from it. Steps run eagerly (with a stream
+ * synchronisation each) while tuning.
+ */
+int cleo_b200_autotune(cleo_b200_ctx* ctx, int reps);
+/* Current configuration {pass-A block, pass-B grid multiple, small_max, medium_max}; returns 1
+ * while tuning is still in progress, else CLEO_OK. */
+int cleo_b200_tuned_config(cleo_b200_ctx* ctx, int32_t cfg[4]);
+
 /* Library version string. */
 const char* cleo_b200_version(void);
 

@@ -678,12 +678,15 @@ static double nr_niterations(const implit_t* it, const odeconsts_t* o, double su
 }
 /* newtonraphson_untilconverged: impliciteuler.cpp:207-227 */
 static double nr_untilconverged(const implit_t* it, const odeconsts_t* o, size_t niterslimit,
-                                double subdelt, double rprev, double ziter) {
+                                double subdelt, double rprev, double ziter, int* failed) {
   int is_converged = 0;
   size_t niter = 1;
   while (!is_converged) {
     if (niter > niterslimit) {
-      set_error(CLEO_ERR_NR_NOCONVERGE, g_cur_gbx, g_cur_sd);
+      if (failed)
+        *failed = 1; /* a seeded attempt: the caller restarts from the reference guess */
+      else
+        set_error(CLEO_ERR_NR_NOCONVERGE, g_cur_gbx, g_cur_sd);
       break;
     }
     ziter = iterate_rootfinding(it, o, subdelt, rprev, ziter, &is_converged);
@@ -692,16 +695,20 @@ static double nr_untilconverged(const implit_t* it, const odeconsts_t* o, size_t
   return ziter;
 }
 /* integrate_condensation_ode: impliciteuler.cpp:128-141 */
-static double integrate_condensation_ode(const implit_t* it, const odeconsts_t* o, double subdelt,
-                                         double rprev, double ziter) {
+static double integrate_ode_ex(const implit_t* it, const odeconsts_t* o, double subdelt,
+                               double rprev, double ziter, int* failed) {
   const size_t niters = 2;
   int conv = 0;
   const double res = nr_niterations(it, o, subdelt, rprev, ziter, niters, &conv);
   if (conv) {
     return res;
   } else {
-    return nr_untilconverged(it, o, it->maxniters, subdelt, rprev, ziter);
+    return nr_untilconverged(it, o, it->maxniters, subdelt, rprev, ziter, failed);
   }
+}
+static double integrate_condensation_ode(const implit_t* it, const odeconsts_t* o, double subdelt,
+                                         double rprev, double ziter) {
+  return integrate_ode_ex(it, o, subdelt, rprev, ziter, NULL);
 }
 /* initialguess: impliciteuler.cpp:156-170 */
 static double initialguess(const odeconsts_t* o, double rprev) {
@@ -743,8 +750,9 @@ static double solve_substepping(const implit_t* it, const odeconsts_t* o, double
   }
   return ziter;
 }
-/* solve_condensation: impliciteuler.cpp:35-54. If seed_rsqrd > 0 the Newton iteration (not the
- * branch decision) starts from it instead of the reference initial guess. */
+/* solve_condensation: impliciteuler.cpp:35-54. A finite positive seed_rsqrd starts the Newton
+ * iteration of the direct branch (not the branch decision) instead of the reference initial
+ * guess; a seeded iteration that does not converge within maxniters restarts from that guess. */
 static double solve_condensation(const implit_t* it, double delt, double minsubdelt,
                                  double s_ratio, double akoh, double bkoh, double ffactor,
                                  double rprev, double seed_rsqrd) {
@@ -755,7 +763,17 @@ static double solve_condensation(const implit_t* it, double delt, double minsubd
   const int ucrit2 = (delt <= critical_timestep(&o)); /* second_unique_criteria, impliciteuler.hpp:283-286 */
   double rsqrd = 0.0;
   if (ucrit1 || ucrit2) {
-    if (seed_rsqrd > 0.0) ziter = seed_rsqrd;
+    /* a seed with a smaller residual than the reference guess starts the iteration; its root is
+     * kept when it is the reference's root: unique when delt <= critical timestep, else (an
+     * unactivated droplet) only in (0, 3b/a] where z g(z) increases */
+    if (seed_rsqrd > 0.0 && seed_rsqrd <= DBL_MAX &&
+        fabs(ode_gfunc(&o, delt, rprev, seed_rsqrd)) < fabs(ode_gfunc(&o, delt, rprev, ziter))) {
+      /* Newton from the seed with the convergence test after every iteration, at most 6 */
+      int conv = 0;
+      double z = seed_rsqrd;
+      for (int k = 0; k < 6 && !conv; ++k) z = iterate_rootfinding(it, &o, delt, rprev, z, &conv);
+      if (conv && (!ucrit1 || z <= 3.0 * bkoh / akoh)) return sqrt(z);
+    }
     rsqrd = integrate_condensation_ode(it, &o, delt, rprev, ziter);
   } else {
     rsqrd = solve_substepping(it, &o, delt, minsubdelt, rprev, ziter);

@@ -2,6 +2,8 @@
 
 They must return the correctly rounded result (checked against 60-digit decimal arithmetic) and
 agree with the host libm that CLEO uses, except where the libm itself is not correctly rounded.
+The fast first phase (Ziv's strategy) must return bit for bit what the accurate double-double
+phase alone returns, and its error must stay far inside the bound its rounding test assumes.
 """
 import ctypes as C
 import os
@@ -26,6 +28,14 @@ def lib(tmp_path_factory):
     L.dd_pow.restype = C.c_double
     L.dd_exp.argtypes = [C.c_double]
     L.dd_exp.restype = C.c_double
+    u64, d = C.c_uint64, C.c_double
+    L.dd_compare_pow.argtypes = [u64, u64, d, d, C.POINTER(d), C.c_int, d, d, C.POINTER(u64),
+                                 C.POINTER(u64), C.POINTER(d)]
+    L.dd_compare_exp.argtypes = [u64, u64, d, d, C.POINTER(u64), C.POINTER(u64), C.POINTER(d)]
+    L.dd_compare_pow2.argtypes = [u64, u64, d, d]
+    L.dd_compare_pow2.restype = u64
+    L.dd_fast_pow_maxerr.argtypes = [u64, u64, d, d, d, d]
+    L.dd_fast_pow_maxerr.restype = d
     return L
 
 
@@ -59,3 +69,41 @@ def test_agreement_with_host_libm(lib):
         assert diff.mean() < 0.005, (y, diff.mean())
         ulps = np.abs(mine[diff] - libm[diff]) / np.spacing(np.abs(libm[diff]))
         assert np.all(ulps <= 1.0), (y, ulps.max())
+
+
+FAST_CASES = [  # (x = 2^U[lx0, lx1), y from EXPONENTS or U[y0, y1))
+    (-40.0, 40.0, True, 0.0, 0.0),
+    (-1000.0, 1000.0, False, -0.6, 0.6),
+    (-5.0, 5.0, False, -60.0, 60.0),
+    (-1.0, 1.0, False, -3.0, 3.0),
+]
+
+
+@pytest.mark.parametrize("case", FAST_CASES)
+def test_fast_pow_phase_is_bit_identical(lib, case):
+    lx0, lx1, listed, y0, y1 = case
+    ys = (C.c_double * len(EXPONENTS))(*EXPONENTS) if listed else None
+    mm, df, bad = C.c_uint64(), C.c_uint64(), (C.c_double * 2)()
+    n = 1_000_000
+    lib.dd_compare_pow(11, n, lx0, lx1, ys, len(EXPONENTS) if listed else 0, y0, y1,
+                       C.byref(mm), C.byref(df), bad)
+    assert mm.value == 0, (mm.value, list(bad))
+    assert df.value < 1e-3 * n  # the accurate phase runs rarely
+
+
+def test_fast_exp_phase_is_bit_identical(lib):
+    mm, df, bad = C.c_uint64(), C.c_uint64(), (C.c_double * 2)()
+    for seed, (a, b) in enumerate([(-600.0, 600.0), (-1.0, 1.0), (-30.0, 0.0)]):
+        lib.dd_compare_exp(seed, 1_000_000, a, b, C.byref(mm), C.byref(df), bad)
+        assert mm.value == 0, (a, b, list(bad))
+        assert df.value < 1000
+
+
+def test_fast_phase_error_inside_its_bound(lib):
+    # the rounding test assumes 2^-67; the analysis gives 2^-72
+    for lx0, lx1, y0, y1 in [(-40, 40, -3, 3), (-1000, 1000, -0.5, 0.5), (-5, 5, -60, 60)]:
+        assert lib.dd_fast_pow_maxerr(5, 300_000, lx0, lx1, y0, y1) < 2.0 ** -71
+
+
+def test_pow_pair_matches_two_pows(lib):
+    assert lib.dd_compare_pow2(3, 300_000, 1.963, 0.702) == 0

@@ -1,0 +1,90 @@
+"""CUDA-graph replay of batched SDM steps gives the same results as eager launches and as the
+oracle, for uniform and mixed sub-step patterns (each distinct pattern is its own graph)."""
+import numpy as np
+import pytest
+
+import checkers as K
+from cleo_b200 import abi, workloads as W
+from cleo_b200.config import realtime2step
+from cleo_b200.sdm import make_sdm
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return abi.load_library()
+
+
+def _workload(pattern):
+    w = W.uneven3d(ndims=(8, 12, 10), seed=21)
+    w["params"].exec_mode = abi.EXEC_BATCHED
+    if pattern == "mixed":  # collisions every 2 s, condensation and motion every 1 s
+        w["params"].collstep = realtime2step(2.0)
+        w["params"].coll_delt = 2.0
+    return w
+
+
+@pytest.mark.parametrize("pattern", ["uniform", "mixed"])
+def test_graphs_match_eager_and_oracle(lib, pattern):
+    w = _workload(pattern)
+    runs = {}
+    for name, graphs in (("graph", 1), ("eager", 0)):
+        s = make_sdm(w, lib=lib)
+        assert lib.cleo_b200_set_graphs(s.ctx, graphs) == 0
+        ts = w["tstep"]
+        for k in range(6):
+            s.run_step(k * ts, (k + 1) * ts)
+        s.check()
+        runs[name] = s
+    o = make_sdm(w, lib=K.oracle_lib(), prefix="oc")
+    for k in range(6):
+        o.run_step(k * w["tstep"], (k + 1) * w["tstep"])
+    a, b = runs["graph"].download_supers(), runs["eager"].download_supers()
+    K.assert_same_domain(a, b, rtol=0.0, what="graph vs eager")
+    K.assert_same_domain(a, o.download_supers(), rtol=1e-12, what="graph vs oracle")
+    ca, ia = runs["graph"].download_budgets()
+    cb, ib = runs["eager"].download_budgets()
+    assert np.array_equal(ia, ib) and np.array_equal(ca, cb)
+
+
+def test_graph_step_after_irregular_call(lib):
+    # a call over several SDM steps, then single steps: the device step time stays in sync
+    w = _workload("uniform")
+    ts = w["tstep"]
+    g = make_sdm(w, lib=lib)
+    e = make_sdm(w, lib=lib)
+    lib.cleo_b200_set_graphs(e.ctx, 0)
+    g.run_step(0, 3 * ts)
+    g.run_step(3 * ts, 4 * ts)
+    g.run_step(4 * ts, 5 * ts)
+    for k in range(5):
+        e.run_step(k * ts, (k + 1) * ts)
+    g.check()
+    e.check()
+    K.assert_same_domain(g.download_supers(), e.download_supers(), rtol=0.0, what="irregular")
+
+
+def test_autotune_keeps_results_and_picks_a_candidate(lib):
+    import ctypes as C
+    w = _workload("uniform")
+    ts = w["tstep"]
+    tuned = make_sdm(w, lib=lib)
+    plain = make_sdm(w, lib=lib)
+    assert lib.cleo_b200_autotune(tuned.ctx, 2) == 0
+    cfg = (C.c_int32 * 4)()
+    for k in range(10):
+        tuned.run_step(k * ts, (k + 1) * ts)
+        plain.run_step(k * ts, (k + 1) * ts)
+        rc = lib.cleo_b200_tuned_config(tuned.ctx, cfg)
+        assert rc == (1 if k < 7 else 0)
+    tuned.check()
+    K.assert_same_domain(tuned.download_supers(), plain.download_supers(), rtol=0.0, what="tuned")
+    assert cfg[0] in (128, 256) and cfg[1] in (1, 2)
+    assert cfg[2] in (32, 64) and cfg[3] in (512, 1024)
+    # plain schedule: nothing to tune
+    w["params"].exec_mode = abi.EXEC_PLAIN
+    p = make_sdm(w, lib=lib)
+    assert lib.cleo_b200_autotune(p.ctx, 1) == abi.CODE["CLEO_ERR_ARGUMENT"]
