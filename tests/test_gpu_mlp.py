@@ -23,7 +23,7 @@ from cleo_b200.surrogate import Surrogate, condensation_solve, to_device, train_
 
 pytestmark = pytest.mark.gpu
 
-TIGHT = dict(maxniters=200, rtol=0.0, atol=1e-9)
+TIGHT = dict(maxniters=200, rtol=0.0, atol=1e-8)
 
 
 @pytest.fixture(scope="module")
