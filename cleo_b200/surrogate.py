@@ -174,3 +174,33 @@ def train_surrogate(solver_sdm, n_train: int = 1 << 24, steps: int = 20000, batc
     torch.cuda.synchronize()
     return sur, {"n_pairs": int(tgt.numel()), "n_drawn": n_train,
                  "loss": hist.cpu().numpy(), "feats": feats, "target": tgt}
+
+
+def _main(argv=None):
+    """Time the three inference paths on n droplets of the independent-droplet population with a
+    randomly initialised surrogate: python -m cleo_b200.surrogate --infer N"""
+    import argparse
+    import torch
+    from . import workloads as W
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--infer", type=int, default=1 << 22)
+    ap.add_argument("--repeat", type=int, default=2)
+    a = ap.parse_args(argv)
+    sur = Surrogate(seed=3)
+    f, _, _ = sur.features(to_device(W.condsolve(a.infer, seed=5)), want_direct=False)
+    sur.fit_normalisation(f, torch.randn(a.infer, device="cuda"))
+    for name, path in (("tcgen05", abi.MLP_TCGEN05), ("mma_sync", abi.MLP_MMA_SYNC),
+                       ("fp32", abi.MLP_FP32)):
+        for _ in range(a.repeat):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            sur.infer(f, path)
+            e1.record()
+            e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        print(f"{name}: {ms:.3f} ms, {a.infer / ms / 1e6:.3f} G samples/s")
+    sur.close()
+
+
+if __name__ == "__main__":
+    _main()
