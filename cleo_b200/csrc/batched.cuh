@@ -233,19 +233,36 @@ __device__ __forceinline__ void cond_commit(DevCtx& c, uint32_t g, double totmas
   c.nr_iters[g] += totits;
 }
 
-// one pair (2jj, 2jj+1) of the shuffled gridbox: collisions.hpp:140-158
+// one pair (2jj, 2jj+1) of the shuffled gridbox: collisions.hpp:140-158. tvA, tvB: pair_tv of
+// dA, dB.
 __device__ __forceinline__ uint32_t collide_pair(const cleo_b200_params& p, Drop& dA, Drop& dB,
-                                                 double scale_p, double VOLUME, uint64_t key,
-                                                 uint64_t slot_pairs, uint32_t jj, const Where& w) {
+                                                 double tvA, double tvB, double scale_p,
+                                                 double VOLUME, uint64_t key, uint64_t slot_pairs,
+                                                 uint32_t jj, const Where& w) {
   const bool swap = dA.xi < dB.xi;
   Drop& d1 = swap ? dB : dA;
   Drop& d2 = swap ? dA : dB;
-  const double prob_jk = pair_prob(p, d1.r, d2.r, VOLUME);
+  const double prob_jk =
+      pair_prob_tv(p, d1.r, d2.r, swap ? tvB : tvA, swap ? tvA : tvB, VOLUME);
   const double large_xi = (double)d1.xi;
   const double prob = scale_p * large_xi * prob_jk;
   const double phi_coll = cleo_rng_to_unit(cleo_rng_u64(key, slot_pairs + 2ull * jj));
   const double phi_out = cleo_rng_to_unit(cleo_rng_u64(key, slot_pairs + 2ull * jj + 1));
   return enact_collision(p, d1, d2, prob, phi_coll, phi_out, w);
+}
+
+// Fisher-Yates (shuffle.hpp:80-87) applies swap(p[i], p[J[i]]) for i = n-1 down to 1 to the
+// identity. The element that ends at position k started at the position reached from k by
+// applying the transpositions (s, J[s]) for s = 1, 2, ..., n-1 (the swaps in reverse order), so
+// every thread can find the origin of its own positions without the sequential loop.
+template <class JT>
+__device__ __forceinline__ uint32_t fy_origin(const JT* J, uint32_t n, uint32_t k) {
+  uint32_t pos = k;
+  for (uint32_t s = 1; s < n; ++s) {
+    const uint32_t j = J[s];
+    pos = (pos == s) ? j : ((pos == j) ? s : pos);
+  }
+  return pos;
 }
 
 // ---- small gridboxes: persistent, one warp per gridbox ----
@@ -255,6 +272,7 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
   __shared__ double s_r[B_WARPS][SMALL_MAX];
   __shared__ double s_m[B_WARPS][SMALL_MAX];
   __shared__ unsigned long long s_x[B_WARPS][SMALL_MAX];
+  __shared__ double s_tv[B_WARPS][SMALL_MAX];
   __shared__ uint8_t s_p[B_WARPS][SMALL_MAX];
   __shared__ uint8_t s_j[B_WARPS][SMALL_MAX];
   const cleo_b200_params& p = c.p;
@@ -285,22 +303,16 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
     const uint64_t slot = b.slot[g];
     // stage this gridbox: lane holds k = lane and k = lane + 32
     for (uint32_t k = lane; k < n; k += 32) {
-      s_r[wib][k] = c.sd.r[base + k];
+      const double rk = c.sd.r[base + k];
+      s_r[wib][k] = rk;
       s_m[wib][k] = c.sd.msol[base + k];
       s_x[wib][k] = c.sd.xi[base + k];
-      s_p[wib][k] = (uint8_t)k;
+      s_tv[wib][k] = pair_tv(p, rk);
       if (k >= 1)
         s_j[wib][k] = (uint8_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - k)), 0, (uint64_t)k + 1);
     }
     __syncwarp();
-    if (lane == 0) {  // Fisher-Yates (shuffle.hpp:80-87)
-      for (uint32_t it = n > 0 ? n - 1 : 0; it > 0; --it) {
-        const uint8_t j = s_j[wib][it];
-        const uint8_t t = s_p[wib][it];
-        s_p[wib][it] = s_p[wib][j];
-        s_p[wib][j] = t;
-      }
-    }
+    for (uint32_t k = lane; k < n; k += 32) s_p[wib][k] = (uint8_t)fy_origin(s_j[wib], n, k);
     __syncwarp();
     const uint64_t slot_pairs = slot + (n >= 1 ? n - 1 : 0);
     const uint32_t npairs = n / 2;
@@ -313,7 +325,8 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
       const Where w{c.err, g, (uint64_t)base + 2 * jj};
       Drop dA{s_x[wib][a], s_r[wib][a], s_m[wib][a]};
       Drop dB{s_x[wib][bb], s_r[wib][bb], s_m[wib][bb]};
-      nnull = collide_pair(p, dA, dB, scale_p, VOLUME, key, slot_pairs, jj, w);
+      nnull = collide_pair(p, dA, dB, s_tv[wib][a], s_tv[wib][bb], scale_p, VOLUME, key,
+                           slot_pairs, jj, w);
       s_x[wib][a] = dA.xi; s_r[wib][a] = dA.r; s_m[wib][a] = dA.msol;
       s_x[wib][bb] = dB.xi; s_r[wib][bb] = dB.r; s_m[wib][bb] = dB.msol;
     }
@@ -417,20 +430,30 @@ k_b_cta(DevCtx c, BatchScratch b, int cond, int coll) {
                                    : reinterpret_cast<unsigned long long*>(smem) + 2 * MEDIUM_MAX;
     uint32_t* P = LARGE ? c.scr_p + base : reinterpret_cast<uint32_t*>(smem + 24 * MEDIUM_MAX);
     uint32_t* J = LARGE ? c.scr_j + base : reinterpret_cast<uint32_t*>(smem + 28 * MEDIUM_MAX);
+    // Simmel terminal velocities once per droplet (medium: shared memory after the five staged
+    // arrays; large: computed per pair)
+    double* Stv = LARGE ? nullptr : reinterpret_cast<double*>(smem + 32 * MEDIUM_MAX);
     for (uint32_t k = tid; k < n; k += B_THREADS) {
-      Sr[k] = c.sd.r[base + k];
+      const double rk = c.sd.r[base + k];
+      Sr[k] = rk;
       Sm[k] = c.sd.msol[base + k];
       Sx[k] = c.sd.xi[base + k];
-      P[k] = k;
+      if (!LARGE) Stv[k] = pair_tv(p, rk);
       if (k >= 1) J[k] = (uint32_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - k)), 0, (uint64_t)k + 1);
     }
     __syncthreads();
-    if (tid == 0) {
-      for (uint32_t it = n > 0 ? n - 1 : 0; it > 0; --it) {
-        const uint32_t j = J[it];
-        const uint32_t t = P[it];
-        P[it] = P[j];
-        P[j] = t;
+    if (n <= FY_PARALLEL_MAX) {  // every thread traces its own positions
+      for (uint32_t k = tid; k < n; k += B_THREADS) P[k] = fy_origin(J, n, k);
+    } else {
+      for (uint32_t k = tid; k < n; k += B_THREADS) P[k] = k;
+      __syncthreads();
+      if (tid == 0) {
+        for (uint32_t it = n > 0 ? n - 1 : 0; it > 0; --it) {
+          const uint32_t j = J[it];
+          const uint32_t t = P[it];
+          P[it] = P[j];
+          P[j] = t;
+        }
       }
     }
     __syncthreads();
@@ -444,7 +467,9 @@ k_b_cta(DevCtx c, BatchScratch b, int cond, int coll) {
       const Where w{c.err, g, (uint64_t)base + 2 * jj};
       Drop dA{Sx[a], Sr[a], Sm[a]};
       Drop dB{Sx[bb], Sr[bb], Sm[bb]};
-      nnull += collide_pair(p, dA, dB, scale_p, VOLUME, key, slot_pairs, jj, w);
+      const double tvA = LARGE ? pair_tv(p, dA.r) : Stv[a];
+      const double tvB = LARGE ? pair_tv(p, dB.r) : Stv[bb];
+      nnull += collide_pair(p, dA, dB, tvA, tvB, scale_p, VOLUME, key, slot_pairs, jj, w);
       Sx[a] = dA.xi; Sr[a] = dA.r; Sm[a] = dA.msol;
       Sx[bb] = dB.xi; Sr[bb] = dB.r; Sm[bb] = dB.msol;
     }

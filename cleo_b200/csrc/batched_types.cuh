@@ -7,6 +7,8 @@ namespace {
 
 constexpr uint32_t SMALL_MAX = 64;
 constexpr uint32_t MEDIUM_MAX = 1024;
+constexpr uint32_t MEDIUM_SMEM = 40 * MEDIUM_MAX;  // r, msol, xi, P, J, Simmel velocity
+constexpr uint32_t FY_PARALLEL_MAX = 256;  // gridboxes up to this size shuffle in parallel
 constexpr int B_THREADS = 256;
 constexpr int B_WARPS = B_THREADS / 32;
 

@@ -20,8 +20,10 @@
 
 #if defined(__CUDACC__)
 #define CLEO_MATH_HD __host__ __device__ __forceinline__
+#define CLEO_MATH_SLOW static __host__ __device__ __noinline__  // the rarely taken accurate phase
 #else
 #define CLEO_MATH_HD static inline
+#define CLEO_MATH_SLOW static
 #endif
 
 // one copy of the tables for device code (global memory, read through the L1 cache: lanes index
@@ -171,13 +173,13 @@ CLEO_MATH_HD double round_dd(dd v) {
 }
 
 // exp(x), rounded once from a double-double evaluation (the second, accurate phase)
-CLEO_MATH_HD double dexp_dd(double x) {
+CLEO_MATH_SLOW double dexp_dd(double x) {
   if (!(x > -707.0 && x < 707.0)) return std::exp(x);
   return round_dd(dd_exp(dd{x, 0.0}));
 }
 
 // pow(x, y) for x > 0 normal and y not special, rounded once from a double-double evaluation
-CLEO_MATH_HD double dpow_dd(double x, double y) {
+CLEO_MATH_SLOW double dpow_dd(double x, double y) {
   const dd z = dd_mul_d(dd_log(x), y);
   if (!(z.hi > -707.0 && z.hi < 707.0)) return std::pow(x, y);
   return round_dd(dd_exp(z));

@@ -180,24 +180,37 @@ __device__ __forceinline__ double long_kerneleff(double ra, double rb, double co
   }
   return colleff * coaleff;
 }
-__device__ __forceinline__ double prob_hydrodynamic(double r1, double r2, double eff, double DELT,
+// tv1, tv2: the Simmel terminal velocities of r1, r2 (computed by the caller, possibly once per
+// droplet for all its pairs: the same function of the same radius)
+__device__ __forceinline__ double prob_hydrodynamic(double r1, double r2, double tv1, double tv2,
+                                                    double eff, double DELT,
                                                     double VOLUME) {  // hydrodynamicprob.hpp:49-66
   const double prob_jk_const = PI * R0 * R0 * W0;
   const double DELT_DELVOL = DELT / VOLUME;
   const double sumr = r1 + r2;
   const double sumrsqrd = sumr * sumr;
-  const double vdiff = fabs(tv_simmel(r1) - tv_simmel(r2));
+  const double vdiff = fabs(tv1 - tv2);
   const double hydro_kernel = prob_jk_const * eff * sumrsqrd * vdiff;
   return hydro_kernel * DELT_DELVOL;
 }
-__device__ __forceinline__ double pair_prob(const cleo_b200_params& p, double r1, double r2,
-                                            double VOLUME) {
+// pair probability; tv1, tv2 = tv_simmel(r1), tv_simmel(r2) when p.coll_prob is CLEO_PROB_LONG
+__device__ __forceinline__ double pair_prob_tv(const cleo_b200_params& p, double r1, double r2,
+                                               double tv1, double tv2, double VOLUME) {
   switch (p.coll_prob) {
     case CLEO_PROB_GOLOVIN: return prob_golovin(r1, r2, p.coll_delt, VOLUME);
     case CLEO_PROB_LONG:
-      return prob_hydrodynamic(r1, r2, long_kerneleff(r1, r2, p.coaleff), p.coll_delt, VOLUME);
+      return prob_hydrodynamic(r1, r2, tv1, tv2, long_kerneleff(r1, r2, p.coaleff), p.coll_delt,
+                               VOLUME);
     default: return p.const_kernel * p.coll_delt / VOLUME;  // constprob.hpp:44-48
   }
+}
+// the pair-probability terminal velocity of one droplet (0 when the kernel needs none)
+__device__ __forceinline__ double pair_tv(const cleo_b200_params& p, double r) {
+  return p.coll_prob == CLEO_PROB_LONG ? tv_simmel(r) : 0.0;
+}
+__device__ __forceinline__ double pair_prob(const cleo_b200_params& p, double r1, double r2,
+                                            double VOLUME) {
+  return pair_prob_tv(p, r1, r2, pair_tv(p, r1), pair_tv(p, r2), VOLUME);
 }
 
 // ---- collision kinetics: collisionkinetics.cpp:31-67, coalescence_efficiency.cpp:27-38 ----

@@ -816,7 +816,7 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       k_b_reset<<<1, 32, 0, s>>>(d, b, 0);
       k_b_classify<<<gg, 256, 0, s>>>(d, b);
       k_b_small<<<x->grid_small, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
-      k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_MAX * 32, s>>>(d, b, cond ? 1 : 0,
+      k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_SMEM, s>>>(d, b, cond ? 1 : 0,
                                                                            coll ? 1 : 0);
       k_b_cta<true><<<x->grid_large, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
       x->launches += 5;
@@ -1095,7 +1095,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small, B_THREADS, 0));
     x->grid_small = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<false>, B_THREADS,
-                                                           (size_t)MEDIUM_MAX * 32));
+                                                           (size_t)MEDIUM_SMEM));
     x->grid_medium = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<true>, B_THREADS, 0));
     x->grid_large = sms * (occ > 0 ? occ : 1);
