@@ -225,8 +225,8 @@ def measure(lib, wl, mode, steps, warmup, dist, local, e2e=False, surrogate=None
     out = {"ms": ev0.elapsed_time(ev1), "nsd": nsd, "ngbxs": ngbxs,
            "stage_ms": {k: ms5[i] / profile_steps for i, k in enumerate(names)},
            "launches": int(l1.value - l0.value), "clocks": clk.summary(),
-           "tuned": {"cond_block": cfg[0], "condb_grid_mult": cfg[1], "small_max": cfg[2],
-                     "medium_max": cfg[3]}}
+           "tuned": {"cond_block": cfg[0], "cond_ctas_per_sm": cfg[1], "small_max": cfg[2],
+                     "small_ctas_per_sm": cfg[3]}}
     if e2e:
         # end-to-end through the public API with pinned host buffers: per step the gridbox
         # states go host->device and the condensed-mass budget comes back

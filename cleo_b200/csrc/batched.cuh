@@ -15,8 +15,8 @@
 //   k_b_cta<false> persistent, CTA per gridbox (small_max < n <= medium_max <= 1024): the same
 //                  with shared-memory staging
 //   k_b_cta<true>  CTA per gridbox (n > medium_max) with global scratch
-// small_max, medium_max, the pass-A block size and the pass-B grid are chosen by the autotuner
-// (results do not depend on them).
+// small_max, the pass-A block size, the resident-CTA targets (register budgets) of pass A and of
+// the warp kernel are chosen by the autotuner (results do not depend on them).
 // Condensed mass per droplet goes through a scratch array and is summed per gridbox in a fixed
 // order, so budgets and states are deterministic.
 #pragma once
@@ -112,7 +112,8 @@ __device__ __forceinline__ uint32_t deferred_key(double delt, double mindelt, bo
 }
 
 // ---- pass A: superdrop_mass_change (condensation.cpp:98-112) up to two Newton iterations ----
-__global__ void __launch_bounds__(256)
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB)
 k_cond_a(DevCtx c, BatchScratch b) {
   const cleo_b200_params& p = c.p;
   const uint32_t n = c.counters[0];
@@ -266,7 +267,8 @@ __device__ __forceinline__ uint32_t fy_origin(const JT* J, uint32_t n, uint32_t 
 }
 
 // ---- small gridboxes: persistent, one warp per gridbox ----
-__global__ void __launch_bounds__(B_THREADS)
+template <int MINB>
+__global__ void __launch_bounds__(B_THREADS, MINB)
 k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
   const uint32_t t_sdm = *b.tsdm;
   __shared__ double s_r[B_WARPS][SMALL_MAX];
@@ -279,12 +281,14 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t count = b.ctr[1];
   const uint32_t* list = b.bucket;
-  while (true) {
-    uint32_t item = 0;
-    if (lane == 0) item = atomicAdd(&b.ctr[4], 1u);
-    item = __shfl_sync(0xFFFFFFFFu, item, 0);
-    if (item >= count) break;
-    const uint32_t g = list[item];
+  // static assignment (item = warp + k * warps): no shared counter, and the next gridbox's list
+  // entry is loaded a whole gridbox ahead
+  const uint32_t nwarps = gridDim.x * B_WARPS;
+  uint32_t item = blockIdx.x * B_WARPS + wib;
+  uint32_t g_next = item < count ? list[item] : 0u;
+  for (; item < count; item += nwarps) {
+    const uint32_t g = g_next;
+    if (item + nwarps < count) g_next = list[item + nwarps];
     const uint32_t base = c.gstart[g];
     uint32_t n = c.gcount[g];
     if (cond) {

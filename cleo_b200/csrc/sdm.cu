@@ -99,7 +99,7 @@ struct cleo_b200_ctx {
   uint32_t *keys[2], *vals[2], *hist, *tile_sums;
   uint32_t ntiles_max, key_bits;
   BatchScratch bs{};              // batched-schedule scratch
-  int grid_small = 0, grid_medium = 0, grid_large = 0, grid_flat = 0;
+  int grid_small = 0, grid_small3 = 0, grid_medium = 0, grid_large = 0, grid_flat = 0;
   unsigned long long launches = 0;  // kernels launched by this context
   std::vector<void*> allocs;
   // stage timing: (stage, start, end) event triples recorded while profiling is on
@@ -114,11 +114,11 @@ struct cleo_b200_ctx {
   // autotuner that chooses it by timing candidates on live steps
   struct TuneCfg {
     int cond_block;       // threads per block of pass A
-    int condb_mult;       // pass-B grid = multiple of the resident-CTA count
-    uint32_t small_max;   // bucket thresholds of the collision kernels
-    uint32_t medium_max;
+    int cond_minb;        // pass-A variant: resident 256-thread CTAs per SM it is compiled for
+    uint32_t small_max;   // gridboxes up to this size go to the warp kernel
+    int small_minb;       // warp-kernel variant: resident CTAs per SM it is compiled for
   };
-  TuneCfg cfg{256, 1, SMALL_MAX, MEDIUM_MAX};
+  TuneCfg cfg{256, 3, SMALL_MAX, 2};
   std::vector<TuneCfg> cand;
   std::vector<double> t_cond, t_coll;
   size_t tune_step = 0, tune_total = 0;
@@ -226,7 +226,8 @@ __device__ __forceinline__ bool beyond_domainboundary(uint32_t gbxindex, uint32_
 // PredCorr::operator() (predcorr.hpp:156-171), cfl_criteria, PredCorrMotion::superdrop_gbx
 // (predcorrmotion.hpp:85-106) with get_no_decomposition_bounding_gridbox (cartesianmaps.cpp:278)
 // and CartesianCheckBounds. Writes the sort key min(gbx, ngbxs) and the position.
-__global__ void k_motion(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+__global__ void __launch_bounds__(256, 3)
+k_motion(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
   const uint32_t n = c.counters[0];
   const uint32_t ng = c.ngbxs;
   const double delt = c.p.motion_delt;
@@ -774,7 +775,7 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
   DevCtx& d = x->d;
   BatchScratch& b = x->bs;
   b.small_max = x->cfg.small_max;
-  b.medium_max = x->cfg.medium_max;
+  b.medium_max = MEDIUM_MAX;
   cudaStream_t s = x->stream;
   StageMark m(x, 2);
   const int gg = grid_for(d.ngbxs, 256);
@@ -804,18 +805,24 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
             w, io, d.capacity);
         x->launches += 1;
       }
-      k_cond_a<<<grid_for(d.capacity, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
+      if (x->cfg.cond_minb == 4)
+        k_cond_a<4><<<grid_for(d.capacity, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
+      else
+        k_cond_a<3><<<grid_for(d.capacity, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
       x->launches += 1;
       const int where = radix_pairs(x, b.lkeys, b.lvals, x->keys[1], x->vals[1], b.ctr, 16);
       if (where != 0) return CLEO_ERR_CUDA;  // 16 key bits: two passes, result back in place
-      k_cond_b<<<x->grid_flat * x->cfg.condb_mult, 256, 0, s>>>(d, b);
+      k_cond_b<<<x->grid_flat * 2, 256, 0, s>>>(d, b);
       x->launches += 1;
     }
     if (cond || coll) {
       StageMark mk(x, 4);
       k_b_reset<<<1, 32, 0, s>>>(d, b, 0);
       k_b_classify<<<gg, 256, 0, s>>>(d, b);
-      k_b_small<<<x->grid_small, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
+      if (x->cfg.small_minb == 3)
+        k_b_small<3><<<x->grid_small3, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
+      else
+        k_b_small<2><<<x->grid_small, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
       k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_SMEM, s>>>(d, b, cond ? 1 : 0,
                                                                            coll ? 1 : 0);
       k_b_cta<true><<<x->grid_large, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
@@ -866,9 +873,9 @@ std::mutex g_tune_mutex;
 std::map<std::string, cleo_b200_ctx::TuneCfg> g_tune_cache;
 
 const cleo_b200_ctx::TuneCfg COND_OPTS[4] = {
-    {128, 1, 0, 0}, {256, 1, 0, 0}, {128, 2, 0, 0}, {256, 2, 0, 0}};
+    {128, 3, 0, 0}, {256, 3, 0, 0}, {128, 4, 0, 0}, {256, 4, 0, 0}};
 const cleo_b200_ctx::TuneCfg COLL_OPTS[4] = {
-    {0, 0, 32, 512}, {0, 0, SMALL_MAX, 512}, {0, 0, 32, MEDIUM_MAX}, {0, 0, SMALL_MAX, MEDIUM_MAX}};
+    {0, 0, 32, 2}, {0, 0, SMALL_MAX, 2}, {0, 0, 32, 3}, {0, 0, SMALL_MAX, 3}};
 
 std::string tune_key(const cleo_b200_ctx* x) {
   cudaDeviceProp prop;
@@ -883,9 +890,9 @@ std::string tune_key(const cleo_b200_ctx* x) {
 int run_tuning_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
   const size_t k = x->tune_step % 4;
   x->cfg.cond_block = COND_OPTS[k].cond_block;
-  x->cfg.condb_mult = COND_OPTS[k].condb_mult;
+  x->cfg.cond_minb = COND_OPTS[k].cond_minb;
   x->cfg.small_max = COLL_OPTS[k].small_max;
-  x->cfg.medium_max = COLL_OPTS[k].medium_max;
+  x->cfg.small_minb = COLL_OPTS[k].small_minb;
   const bool prof = x->profiling;
   const size_t m0 = x->marks.size();
   x->profiling = true;
@@ -913,8 +920,8 @@ int run_tuning_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
       if (x->t_cond[i] < x->t_cond[bc]) bc = i;
       if (x->t_coll[i] < x->t_coll[bl]) bl = i;
     }
-    x->cfg = {COND_OPTS[bc].cond_block, COND_OPTS[bc].condb_mult, COLL_OPTS[bl].small_max,
-              COLL_OPTS[bl].medium_max};
+    x->cfg = {COND_OPTS[bc].cond_block, COND_OPTS[bc].cond_minb, COLL_OPTS[bl].small_max,
+              COLL_OPTS[bl].small_minb};
     x->tune_total = 0;
     x->drop_graphs();
     std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -1092,8 +1099,10 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
     int dev = 0, sms = 148, occ = 1;
     CUDA_TRY(cudaGetDevice(&dev));
     CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small, B_THREADS, 0));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<2>, B_THREADS, 0));
     x->grid_small = sms * (occ > 0 ? occ : 1);
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<3>, B_THREADS, 0));
+    x->grid_small3 = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<false>, B_THREADS,
                                                            (size_t)MEDIUM_SMEM));
     x->grid_medium = sms * (occ > 0 ? occ : 1);
@@ -1252,9 +1261,9 @@ int cleo_b200_autotune(cleo_b200_ctx* x, int reps) {
 int cleo_b200_tuned_config(cleo_b200_ctx* x, int32_t cfg[4]) {
   if (!x || !cfg) return CLEO_ERR_ARGUMENT;
   cfg[0] = x->cfg.cond_block;
-  cfg[1] = x->cfg.condb_mult;
+  cfg[1] = x->cfg.cond_minb;
   cfg[2] = (int32_t)x->cfg.small_max;
-  cfg[3] = (int32_t)x->cfg.medium_max;
+  cfg[3] = x->cfg.small_minb;
   return x->tune_step < x->tune_total ? 1 : CLEO_OK;
 }
 

@@ -349,15 +349,16 @@ int cleo_b200_set_graphs(cleo_b200_ctx* ctx, int on);
 /*
  * Autotuner of the batched schedule (no counterpart in the reference). The next 4 * reps batched
  * SDM steps run as ordinary steps (same results) while each times one of four candidate launch
- * configurations per stage: pass-A block size and pass-B grid for condensation, the gridbox-size
- * thresholds between the warp, shared-memory CTA and global-scratch CTA collision kernels. The
- * fastest option of each stage is kept, and cached per process by GPU name and domain size so
- * that later contexts of that size start from it. Steps run eagerly (with a stream
- * synchronisation each) while tuning.
+ * configurations per stage: for condensation pass A, the block size (128 or 256) and the
+ * compiled variant's resident-CTA target (3 or 4 per SM, i.e. its register budget); for
+ * collisions, the largest gridbox of the warp-per-gridbox kernel (32 or 64) and that kernel's
+ * resident-CTA target (2 or 3). The fastest option of each stage is kept, and cached per process
+ * by GPU name and domain size so that later contexts of that size start from it. Steps run
+ * eagerly (with a stream synchronisation each) while tuning.
  */
 int cleo_b200_autotune(cleo_b200_ctx* ctx, int reps);
-/* Current configuration {pass-A block, pass-B grid multiple, small_max, medium_max}; returns 1
- * while tuning is still in progress, else CLEO_OK. */
+/* Current configuration {pass-A block, pass-A CTA target, warp-kernel gridbox limit, warp-kernel
+ * CTA target}; returns 1 while tuning is still in progress, else CLEO_OK. */
 int cleo_b200_tuned_config(cleo_b200_ctx* ctx, int32_t cfg[4]);
 
 /* Library version string. */
