@@ -495,8 +495,11 @@ constexpr uint32_t NR_ITER_CAP = 4u << 20;
 // convergence check of one iteration and as the numerator of the next) and recomputes sqrt(z),
 // z^(3/2) and akoh/r for g'; one evaluation per iterate gives the same doubles, because each
 // value is the same expression of the same inputs.
+// g's beta is (2 subdelt) / (z F) and g''s is subdelt / (z F) with the same rounded product z F;
+// scaling by 2 commutes with rounding to nearest (no overflow or underflow at these magnitudes),
+// so the first is exactly twice the second and one division serves both.
 struct GEval {
-  double z, radius, akr, r3, g;
+  double z, radius, akr, r3, q, g;
 };
 __device__ __forceinline__ GEval eval_g(const OdeConsts& o, double subdelt, double rprev,
                                         double rsqrd) {
@@ -506,22 +509,22 @@ __device__ __forceinline__ GEval eval_g(const OdeConsts& o, double subdelt, doub
   e.akr = o.akoh / e.radius;
   e.r3 = dpow(e.radius, 3.0);
   const double alpha = o.s_ratio - 1 - e.akr + o.bkoh / e.r3;
-  const double beta = 2.0 * subdelt / (rsqrd * o.ffactor_fv);
+  e.q = subdelt / (rsqrd * o.ffactor_fv);
+  const double beta = 2.0 * e.q;
   const double gamma = dpow(rprev / e.radius, 2.0);
   e.g = 1 - gamma - alpha * beta;
   return e;
 }
-__device__ __forceinline__ double eval_gprime(const OdeConsts& o, double subdelt, const GEval& e) {
+__device__ __forceinline__ double eval_gprime(const OdeConsts& o, const GEval& e) {
   const double alpha = e.akr - 3.0 * o.bkoh / e.r3;
-  const double beta = subdelt / (e.z * o.ffactor_fv);
-  return 1 - alpha * beta;
+  return 1 - alpha * e.q;
 }
 // iterate_rootfinding_algorithm: impliciteuler.cpp:239-255 (+ check_for_convergence, hpp:213-219)
 __device__ __forceinline__ GEval nr_iterate(const NewtonCfg& c, const OdeConsts& o,
                                             double subdelt, double rprev, const GEval& e,
                                             bool& converged, uint32_t& niters) {
   const double numerator = e.g;
-  const double denominator = eval_gprime(o, subdelt, e);
+  const double denominator = eval_gprime(o, e);
   double ziter = e.z * (1 - numerator / denominator);
   ziter = fmax(ziter, 1e-8);
   const GEval next = eval_g(o, subdelt, rprev, ziter);

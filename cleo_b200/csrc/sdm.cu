@@ -142,6 +142,17 @@ struct cleo_b200_ctx {
   const cleo_b200_mlp* mlp = nullptr;
   double* seed_buf = nullptr;
   size_t seed_cap = 0;
+  // two-pass condensation_solve scratch (deferred-solve list and its radix sort)
+  struct CsScratch {
+    size_t cap = 0;
+    uint32_t *k0 = nullptr, *v0 = nullptr, *k1 = nullptr, *v1 = nullptr;
+    uint32_t *hist = nullptr, *tsums = nullptr, *ctr = nullptr;
+    uint32_t nt = 0;
+  } cs;
+  void free_cs() {
+    for (uint32_t* q : {cs.k0, cs.v0, cs.k1, cs.v1, cs.hist, cs.tsums, cs.ctr}) cudaFree(q);
+    cs = CsScratch();
+  }
   cudaEvent_t take_event() {
     if (!event_pool.empty()) {
       cudaEvent_t e = event_pool.back();
@@ -675,6 +686,111 @@ __global__ void k_condsolve(DevCtx c, uint32_t n, const double* __restrict__ rad
 
 #include "batched.cuh"
 
+namespace {
+
+// Two-pass form of the batch solve (the batched schedule), as k_cond_a / k_cond_b do for the
+// SDM step: pass A finishes every direct solve that converges within its first two iterations
+// (or within the seeded attempt) and lists the rest, keyed by sub-step count; pass B solves the
+// listed ones after the list has been sorted by that key, so that neighbouring lanes carry
+// similar work. Iterations spent in pass A on an abandoned seed are carried in niters_out.
+__device__ __forceinline__ uint32_t cs_warp_append(uint32_t* ctr, bool flag) {
+  const unsigned m = __ballot_sync(0xFFFFFFFFu, flag);
+  uint32_t base = 0;
+  const int lane = threadIdx.x & 31;
+  if (lane == 0 && m) base = atomicAdd(ctr, (uint32_t)__popc(m));
+  base = __shfl_sync(0xFFFFFFFFu, base, 0);
+  return base + __popc(m & ((1u << lane) - 1u));
+}
+__global__ void __launch_bounds__(256, 3)
+k_cs_a(DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __restrict__ msol,
+       const double* __restrict__ temp, const double* __restrict__ press,
+       const double* __restrict__ s_ratio, const double* __restrict__ delt,
+       double* __restrict__ seeds, double* __restrict__ out, uint32_t* __restrict__ niters_out,
+       uint32_t* __restrict__ lkeys, uint32_t* __restrict__ lvals, uint32_t* __restrict__ ctr) {
+  const NewtonCfg cfg{c.p.maxniters, c.p.rtol, c.p.atol};
+  for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+    const uint32_t i = i0 + threadIdx.x;
+    bool defer = false;
+    uint32_t key = 0;
+    if (i < n) {
+      const Where w{c.err, OOB, i};
+      const double T = temp[i], r = radius[i], dt = delt[i];
+      const double psat = saturation_pressure(T, w);
+      const double ffactor = diffusion_factor(press[i], T, psat);
+      double akoh, bkoh;
+      kohler_factors(msol[i], T, akoh, bkoh);
+      const OdeConsts o{s_ratio[i], akoh, bkoh, ffactor / ventilation_factor(r)};
+      const double z0 = initialguess(o, r);
+      const bool ucrit1 = first_unique_criteria(o, r, z0);
+      const double crit = ucrit1 ? 0.0 : critical_timestep(o);
+      uint32_t ni = 0, carried = 0;
+      if (ucrit1 || dt <= crit) {
+        bool conv = false, seeded = false;
+        GEval e = eval_g(o, dt, r, z0);
+        if (seeds && seed_ok(seeds[i])) {
+          const GEval es = eval_g(o, dt, r, seeds[i]);
+          if (fabs(es.g) < fabs(e.g)) {
+            double zs;
+            conv = integrate_seeded(cfg, o, dt, r, es, ni, zs) && seeded_root_ok(o, ucrit1, zs);
+            e.z = zs;
+            seeded = true;
+            if (!conv) {
+              seeds[i] = -1.0;  // pass B starts from the reference guess
+              carried = ni;
+            }
+          }
+        }
+        if (!seeded) {
+          e = nr_iterate(cfg, o, dt, r, e, conv, ni);
+          e = nr_iterate(cfg, o, dt, r, e, conv, ni);
+        }
+        if (conv) {
+          out[i] = fmax(sqrt(e.z), dryradius(msol[i]));
+          if (niters_out) niters_out[i] = ni;
+        } else {
+          defer = true;  // restart until converged (impliciteuler.cpp:136-140)
+        }
+      } else {
+        defer = true;
+        key = deferred_key(dt, fmax(crit, c.p.cond_minsubdelt), true);
+      }
+      if (defer && niters_out) niters_out[i] = carried;
+    }
+    const uint32_t pos = cs_warp_append(ctr, defer);
+    if (defer) {
+      lkeys[pos] = key;
+      lvals[pos] = i;
+    }
+  }
+}
+__global__ void __launch_bounds__(256)
+k_cs_b(DevCtx c, const double* __restrict__ radius, const double* __restrict__ msol,
+       const double* __restrict__ temp, const double* __restrict__ press,
+       const double* __restrict__ s_ratio, const double* __restrict__ delt,
+       const double* __restrict__ seeds, double* __restrict__ out,
+       uint32_t* __restrict__ niters_out, const uint32_t* __restrict__ lvals,
+       const uint32_t* __restrict__ ctr) {
+  const NewtonCfg cfg{c.p.maxniters, c.p.rtol, c.p.atol};
+  const uint32_t nl = *ctr;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nl; j += gridDim.x * blockDim.x) {
+    const uint32_t i = lvals[j];
+    const Where w{c.err, OOB, i};
+    const double T = temp[i];
+    const double psat = saturation_pressure(T, w);
+    const double ffactor = diffusion_factor(press[i], T, psat);
+    double akoh, bkoh;
+    kohler_factors(msol[i], T, akoh, bkoh);
+    uint32_t ni = 0;
+    const double newr = solve_condensation(cfg, delt[i], c.p.cond_minsubdelt, s_ratio[i], akoh,
+                                           bkoh, ffactor, radius[i], seeds ? seeds[i] : 0.0, ni,
+                                           w);
+    out[i] = fmax(newr, dryradius(msol[i]));
+    if (niters_out) niters_out[i] += ni;
+  }
+}
+
+}  // namespace
+
 // ------------------------------------------------------------------------------------------
 // host side
 // ------------------------------------------------------------------------------------------
@@ -748,26 +864,32 @@ int sort_current(cleo_b200_ctx* x) {
 
 // stable radix sort of (key, value) pairs whose count is *n_ptr (device), over `bits` key bits,
 // from (k0, v0) using (k1, v1) as the other buffer; returns 0 if the result is in (k0, v0)
-int radix_pairs(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1,
-                const uint32_t* n_ptr, uint32_t bits) {
+// with explicit digit-table scratch for nt tiles (hist: 256 nt words, tile_sums: enough for the
+// scan of the table)
+int radix_pairs_on(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1,
+                   const uint32_t* n_ptr, uint32_t bits, uint32_t* hist, uint32_t* tile_sums,
+                   uint32_t nt) {
   cudaStream_t s = x->stream;
-  const uint32_t nt = x->ntiles_max;
   const uint64_t nh = (uint64_t)256 * nt;
   const uint32_t nscan_tiles = (uint32_t)((nh + SCAN_TILE - 1) / SCAN_TILE);
   int cur = 0;
   uint32_t* K[2] = {k0, k1};
   uint32_t* V[2] = {v0, v1};
   for (uint32_t shift = 0; shift < bits; shift += 8) {
-    k_rs_upsweep<<<nt, RS_THREADS, 0, s>>>(K[cur], n_ptr, (int)shift, x->hist, nt);
-    k_scan_tiles<<<nscan_tiles, SCAN_THREADS, 0, s>>>(x->hist, x->hist, nh, x->tile_sums);
-    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(x->tile_sums, nscan_tiles, nullptr);
-    k_scan_add<<<(unsigned)((nh + 255) / 256), 256, 0, s>>>(x->hist, nh, x->tile_sums);
-    k_rs_downsweep<<<nt, RS_THREADS, 0, s>>>(K[cur], V[cur], n_ptr, (int)shift, x->hist, nt,
+    k_rs_upsweep<<<nt, RS_THREADS, 0, s>>>(K[cur], n_ptr, (int)shift, hist, nt);
+    k_scan_tiles<<<nscan_tiles, SCAN_THREADS, 0, s>>>(hist, hist, nh, tile_sums);
+    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(tile_sums, nscan_tiles, nullptr);
+    k_scan_add<<<(unsigned)((nh + 255) / 256), 256, 0, s>>>(hist, nh, tile_sums);
+    k_rs_downsweep<<<nt, RS_THREADS, 0, s>>>(K[cur], V[cur], n_ptr, (int)shift, hist, nt,
                                              K[1 - cur], V[1 - cur]);
     x->launches += 5;
     cur = 1 - cur;
   }
   return cur;
+}
+int radix_pairs(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1,
+                const uint32_t* n_ptr, uint32_t bits) {
+  return radix_pairs_on(x, k0, v0, k1, v1, n_ptr, bits, x->hist, x->tile_sums, x->ntiles_max);
 }
 
 // the microphysics of one SDM step on the batched schedule (batched.cuh)
@@ -1132,6 +1254,7 @@ void cleo_b200_destroy(cleo_b200_ctx* x) {
   for (auto e : x->event_pool) cudaEventDestroy(e);
   x->drop_graphs();
   cudaFree(x->seed_buf);
+  x->free_cs();
   for (void* p : x->allocs) cudaFree(p);
   if (x->own_stream && x->stream) cudaStreamDestroy(x->stream);
   delete x;
@@ -1408,9 +1531,47 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_rad
     x->launches += 1;
     seeds = x->seed_buf;
   }
-  k_condsolve<<<grid_for(n, 128), 128, 0, x->stream>>>(x->d, (uint32_t)n, d_radius, d_msol, d_temp,
-                                                       d_press, d_s_ratio, d_delt, seeds,
-                                                       d_radius_out, d_niters_out);
+  if (x->d.p.exec_mode != CLEO_EXEC_BATCHED) {
+    k_condsolve<<<grid_for(n, 128), 128, 0, x->stream>>>(x->d, (uint32_t)n, d_radius, d_msol,
+                                                         d_temp, d_press, d_s_ratio, d_delt,
+                                                         seeds, d_radius_out, d_niters_out);
+    x->launches += 1;
+    CUDA_TRY(cudaGetLastError());
+    return CLEO_OK;
+  }
+  // two-pass form: scratch for the deferred list of up to n solves and its 16-bit radix sort
+  auto& cs = x->cs;
+  if (n > cs.cap) {
+    CUDA_TRY(cudaStreamSynchronize(x->stream));
+    x->free_cs();
+    const uint32_t nt = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
+    const uint64_t nh = (uint64_t)256 * nt;
+    const size_t nsums = (size_t)((nh + SCAN_TILE - 1) / SCAN_TILE) + 1;
+    bool ok = true;
+    for (uint32_t** q : {&cs.k0, &cs.v0, &cs.k1, &cs.v1})
+      ok = ok && cudaMalloc(q, n * sizeof(uint32_t)) == cudaSuccess;
+    ok = ok && cudaMalloc(&cs.hist, nh * sizeof(uint32_t)) == cudaSuccess;
+    ok = ok && cudaMalloc(&cs.tsums, nsums * sizeof(uint32_t)) == cudaSuccess;
+    ok = ok && cudaMalloc(&cs.ctr, sizeof(uint32_t)) == cudaSuccess;
+    if (!ok) {
+      x->free_cs();
+      cudaGetLastError();
+      return CLEO_ERR_CUDA;
+    }
+    cs.cap = n;
+    cs.nt = nt;
+  }
+  CUDA_TRY(cudaMemsetAsync(cs.ctr, 0, sizeof(uint32_t), x->stream));
+  k_cs_a<<<grid_for(n, 256), 256, 0, x->stream>>>(
+      x->d, (uint32_t)n, d_radius, d_msol, d_temp, d_press, d_s_ratio, d_delt,
+      seeds ? x->seed_buf : nullptr, d_radius_out, d_niters_out, cs.k0, cs.v0, cs.ctr);
+  x->launches += 1;
+  const int where = radix_pairs_on(x, cs.k0, cs.v0, cs.k1, cs.v1, cs.ctr, 16, cs.hist, cs.tsums,
+                                   cs.nt);
+  if (where != 0) return CLEO_ERR_CUDA;  // two 8-bit passes leave the result in (k0, v0)
+  k_cs_b<<<x->grid_flat * 2, 256, 0, x->stream>>>(x->d, d_radius, d_msol, d_temp, d_press,
+                                                  d_s_ratio, d_delt, seeds, d_radius_out,
+                                                  d_niters_out, cs.v0, cs.ctr);
   x->launches += 1;
   CUDA_TRY(cudaGetLastError());
   return CLEO_OK;
