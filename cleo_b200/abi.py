@@ -48,6 +48,7 @@ FLAG_STRAUB, FLAG_TESTIKSTRAUB, FLAG_SZAKALLURBICH, FLAG_CONST = 0, 1, 2, 3
 NRSEED_REFERENCE, NRSEED_MLP = 0, 1
 EXEC_PLAIN, EXEC_BATCHED = 0, 1
 MLP_TCGEN05, MLP_MMA_SYNC, MLP_FP32 = 0, 1, 2
+MONITOR_MASSMOMENTS, MONITOR_RAINMASSMOMENTS, MONITOR_PRECIPITATION = 1, 2, 4
 MLP_NFEATURES, MLP_NHIDDEN, MLP_NPARAMS, MLP_NNORM = 7, 64, 4737, 16
 
 _d = C.POINTER(C.c_double)
@@ -85,7 +86,7 @@ class Params(C.Structure):
         ("motion_tv", C.c_int32),
         ("nr_seed", C.c_int32),
         ("exec_mode", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("monitors", C.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -104,6 +105,7 @@ class Grid(C.Structure):
         ("back3", _u32), ("fwd3", _u32),
         ("back1", _u32), ("fwd1", _u32),
         ("back2", _u32), ("fwd2", _u32),
+        ("gbxarea", _d),
     ]
 
 
@@ -180,11 +182,44 @@ def grid_struct(g: dict) -> Grid:
         setattr(gr, f, ptr(g[f], C.c_double))
     for f in ("back3", "fwd3", "back1", "fwd1", "back2", "fwd2"):
         setattr(gr, f, ptr(g[f], C.c_uint32))
+    if g.get("gbxarea") is not None:
+        gr.gbxarea = ptr(g["gbxarea"], C.c_double)
     return gr
+
+
+_f32 = C.POINTER(C.c_float)
+MONITOR_FIELDS = (("mom0_micro", np.uint64), ("mom0_motion", np.uint64),
+                  ("rain_mom0_micro", np.uint64), ("rain_mom0_motion", np.uint64),
+                  ("mom1_micro", np.float32), ("mom2_micro", np.float32),
+                  ("mom1_motion", np.float32), ("mom2_motion", np.float32),
+                  ("rain_mom1_micro", np.float32), ("rain_mom2_micro", np.float32),
+                  ("rain_mom1_motion", np.float32), ("rain_mom2_motion", np.float32),
+                  ("precip", np.float64))
+
+
+class Monitors(C.Structure):
+    """cleo_b200_monitors (host pointers; owner keeps the arrays alive)."""
+
+    _fields_ = [(name, {np.uint64: _u64, np.float32: _f32, np.float64: _d}[dt])
+                for name, dt in MONITOR_FIELDS]
+
+
+def monitors_struct(arrs: dict) -> Monitors:
+    m = Monitors()
+    ct = {np.uint64: C.c_uint64, np.float32: C.c_float, np.float64: C.c_double}
+    for name, dt in MONITOR_FIELDS:
+        setattr(m, name, ptr(arrs[name], ct[dt]))
+    return m
 
 
 def declare_api(lib: C.CDLL, prefix: str) -> C.CDLL:
     """Declare argtypes/restype of the context API ``<prefix>_create`` ... on ``lib``."""
+    for name, args in (("monitors_begin", [C.c_void_p]),
+                       ("download_monitors", [C.c_void_p, C.POINTER(Monitors), C.c_int])):
+        f = getattr(lib, f"{prefix}_{name}", None)
+        if f is not None:
+            f.argtypes = args
+            f.restype = C.c_int
     vp = C.c_void_p
     f = getattr(lib, f"{prefix}_create")
     f.argtypes = [C.POINTER(Params), C.POINTER(Grid), C.c_size_t, C.POINTER(vp)]
@@ -227,7 +262,7 @@ EXPORTED = (
     "cleo_b200_mlp_get_params", "cleo_b200_mlp_features", "cleo_b200_mlp_fit_normalisation",
     "cleo_b200_mlp_loss_grad", "cleo_b200_mlp_train", "cleo_b200_mlp_infer",
     "cleo_b200_set_surrogate", "cleo_b200_set_graphs", "cleo_b200_autotune",
-    "cleo_b200_tuned_config",
+    "cleo_b200_tuned_config", "cleo_b200_monitors_begin", "cleo_b200_download_monitors",
 )
 
 _LIB = None

@@ -161,4 +161,7 @@ def cartesian_grid(ndims, spacing_m, nspacedims: int = 3, origin_m=(0.0, 0.0, 0.
     for k in ("back3", "fwd3", "back1", "fwd1", "back2", "fwd2"):
         g[k] = np.ascontiguousarray(g[k], dtype=np.uint32)
     g["volume_m3"] = float(spacing_m[0] * spacing_m[1] * spacing_m[2])
+    # horizontal area from the gridbox extents, as a gridfile holds them for every model
+    # dimension (GbxBoundsFromBinary::gbxarea, gbx_bounds_from_binary.cpp:206-215)
+    g["gbxarea"] = np.full(ngbxs, (spacing_m[1] / COORD0) * (spacing_m[2] / COORD0))
     return g

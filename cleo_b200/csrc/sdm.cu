@@ -64,6 +64,13 @@ struct DevCtx {
   uint32_t* gstart;  // ngbxs + 2
   uint32_t* gcount;  // ngbxs
   uint32_t* counters;  // [0] nrange, [1] ndomain, [2] ngrave
+  // SDMMonitor members (allocated when params.monitors != 0): mass-moment changes
+  // [all, rain][after microphysics, after motion], the previous moments, precipitation
+  unsigned long long* mm0[2][2];
+  float *mm1[2][2], *mm2[2][2];
+  unsigned long long* prev0[2];
+  float *prev1[2], *prev2[2];
+  double *precip, *precip_c, *gbxarea;  // per gridbox, per superdroplet, per gridbox
   // scratch
   double *scr_r, *scr_m, *scr_c3, *scr_c1, *scr_c2;
   unsigned long long *scr_x, *scr_id;
@@ -284,6 +291,12 @@ k_motion(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
     cfl = (fabs(delta2) <= fabs(byh - byl)) && cfl;
     if (!cfl) w.fail(CLEO_ERR_CFL);
     double n3 = c3 + delta3, n1 = c1 + delta1, n2 = c2 + delta2;
+    // monitor_precipitation (monitor_precipitation_observer.hpp:97-107): the contribution of a
+    // superdroplet below its gridbox's lower bound, added per gridbox in order by k_mon_precip
+    if (c.precip_c)
+      c.precip_c[i] = (n3 < bzl) ? condensate_mass(c.sd.r[i], c.sd.msol[i], w) *
+                                       (double)c.sd.xi[i] / Rho_l / c.gbxarea[g]
+                                 : 0.0;
     // change_if_coord3nghbr: finite z, coordinate unchanged at the edge (cartesianmaps.cpp:184-213)
     uint32_t idx = g;
     int flag = flag_sdgbxindex(idx, ng, bzl, bzh, n3);
@@ -682,6 +695,66 @@ __global__ void k_condsolve(DevCtx c, uint32_t n, const double* __restrict__ rad
   }
 }
 
+// ---- SDMMonitor members: one thread per gridbox, sums in the superdroplets' order ----
+// calculate_massmoments / calculate_rainmassmoments (massmoments_observer.cpp:38-113)
+__device__ __forceinline__ void mon_moments(const DevCtx& c, uint32_t g, int rain,
+                                            unsigned long long& m0, float& m1, float& m2) {
+  const double rlim = 40e-6 / R0;
+  const uint32_t base = c.gstart[g], n = c.gcount[g];
+  unsigned long long a0 = 0;
+  float a1 = 0.0f, a2 = 0.0f;
+  for (uint32_t k = base; k < base + n; ++k) {
+    const double r = c.sd.r[k];
+    const unsigned long long x = c.sd.xi[k];
+    const bool binary = rain ? (r >= rlim) : true;
+    a0 += x * (unsigned long long)binary;
+    const double mass = sd_mass(r, c.sd.msol[k]);
+    const double xi = (double)x;
+    a1 += (float)(xi * mass * (double)binary);
+    a2 += (float)(xi * mass * mass * (double)binary);
+  }
+  m0 = a0;
+  m1 = a1;
+  m2 = a2;
+}
+// fetch_delta_massmoments (monitor_massmoments_change.hpp:99-121); which = 0 after
+// microphysics, 1 after motion; begin != 0: before_timestepping (moments become the baseline)
+__global__ void k_mon_mm(DevCtx c, int which, int begin) {
+  const int mask = c.p.monitors;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs;
+       g += gridDim.x * blockDim.x) {
+    for (int rain = 0; rain < 2; ++rain) {
+      if (!begin && !(mask & (rain ? CLEO_MONITOR_RAINMASSMOMENTS : CLEO_MONITOR_MASSMOMENTS)))
+        continue;
+      unsigned long long m0;
+      float m1, m2;
+      mon_moments(c, g, rain, m0, m1, m2);
+      if (!begin) {
+        c.mm0[rain][which][g] += m0 - c.prev0[rain][g];
+        c.mm1[rain][which][g] += m1 - c.prev1[rain][g];
+        c.mm2[rain][which][g] += m2 - c.prev2[rain][g];
+      }
+      c.prev0[rain][g] = m0;
+      c.prev1[rain][g] = m1;
+      c.prev2[rain][g] = m2;
+    }
+  }
+}
+// the precipitation contributions of each gridbox's superdroplets, in their order (the
+// reference adds them one by one as it moves the gridbox's superdroplets)
+__global__ void k_mon_precip(DevCtx c) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs;
+       g += gridDim.x * blockDim.x) {
+    const uint32_t base = c.gstart[g], n = c.gcount[g];
+    double acc = c.precip[g];
+    for (uint32_t k = base; k < base + n; ++k) {
+      const double v = c.precip_c[k];
+      if (v > 0.0) acc += v;
+    }
+    c.precip[g] = acc;
+  }
+}
+
 }  // namespace
 
 #include "batched.cuh"
@@ -962,18 +1035,36 @@ int run_sdm_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
   DevCtx& d = x->d;
   cudaStream_t s = x->stream;
   const bool did_motion = on_step(d.p.motionstep, t_sdm);
+  const int gg = grid_for(d.ngbxs, 256);
+  const bool mon_mm =
+      (d.p.monitors & (CLEO_MONITOR_MASSMOMENTS | CLEO_MONITOR_RAINMASSMOMENTS)) != 0;
   if (did_motion) {
     {
       StageMark m(x, 0);
       k_motion<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, x->keys[0], x->vals[0]);
       x->launches += 1;
+      if (d.p.monitors & CLEO_MONITOR_PRECIPITATION) {  // before the sort moves the droplets
+        k_mon_precip<<<gg, 256, 0, s>>>(d);
+        x->launches += 1;
+      }
     }
     StageMark m(x, 1);
     const int rc = sort_current(x);
     if (rc) return rc;
+    if (mon_mm) {  // monitor_motion (movesupersindomain.hpp:297)
+      k_mon_mm<<<gg, 256, 0, s>>>(d, 1, 0);
+      x->launches += 1;
+    }
   }
   const bool micro = (d.p.condstep != CLEO_STEP_OFF || d.p.collstep != CLEO_STEP_OFF);
-  if (d.p.exec_mode == CLEO_EXEC_BATCHED) return run_batched_micro(x, t_sdm, t_sdm_next, did_motion);
+  if (d.p.exec_mode == CLEO_EXEC_BATCHED) {
+    const int rc = run_batched_micro(x, t_sdm, t_sdm_next, did_motion);
+    if (rc == CLEO_OK && mon_mm) {  // monitor_microphysics (sdmmethods.hpp:76)
+      k_mon_mm<<<gg, 256, 0, s>>>(d, 0, 0);
+      x->launches += 1;
+    }
+    return rc;
+  }
   if (micro || did_motion) {
     const uint32_t blocks = d.ngbxs < (1u << 30) ? d.ngbxs : (1u << 30);
     if (blocks > 0) {
@@ -981,6 +1072,10 @@ int run_sdm_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
       k_micro<<<blocks, MICRO_THREADS, MICRO_SMEM, s>>>(d, t_sdm, t_sdm_next, did_motion ? 1 : 0);
       x->launches += 1;
     }
+  }
+  if (mon_mm) {
+    k_mon_mm<<<gg, 256, 0, s>>>(d, 0, 0);
+    x->launches += 1;
   }
   CUDA_TRY(cudaGetLastError());
   return CLEO_OK;
@@ -1181,6 +1276,21 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &x->bs.ctr, 8);
   rc |= dalloc(x, &x->bs.tsdm, 1);
   rc |= dalloc(x, &x->tile_sums, ((size_t)256 * x->ntiles_max + SCAN_TILE - 1) / SCAN_TILE + 1);
+  if (params->monitors) {
+    for (int r = 0; r < 2; ++r) {
+      for (int w = 0; w < 2; ++w) {
+        rc |= dalloc(x, &d.mm0[r][w], ng);
+        rc |= dalloc(x, &d.mm1[r][w], ng);
+        rc |= dalloc(x, &d.mm2[r][w], ng);
+      }
+      rc |= dalloc(x, &d.prev0[r], ng);
+      rc |= dalloc(x, &d.prev1[r], ng);
+      rc |= dalloc(x, &d.prev2[r], ng);
+    }
+    rc |= dalloc(x, &d.precip, ng);
+    rc |= dalloc(x, &d.gbxarea, ng);
+    if (params->monitors & CLEO_MONITOR_PRECIPITATION) rc |= dalloc(x, &d.precip_c, cap);
+  }
   if (rc) {
     cleo_b200_destroy(x);
     return CLEO_ERR_CUDA;
@@ -1217,6 +1327,20 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   CUDA_TRY(cudaMemsetAsync(x->bs.ctr, 0, 32, x->stream));
   CUDA_TRY(cudaMemsetAsync(x->bs.tsdm, 0, 4, x->stream));
   CUDA_TRY(cudaMemsetAsync(x->bs.slot, 0, (ng ? ng : 1) * 4, x->stream));
+  if (params->monitors) {  // gridbox areas (GbxBoundsFromBinary::gbxarea) and zeroed monitors
+    std::vector<double> area(ng ? ng : 1, 0.0);
+    for (uint32_t i = 0; i < ng; ++i)
+      area[i] = grid->gbxarea ? grid->gbxarea[i]
+                              : (grid->coord1hi[i] - grid->coord1lo[i]) *
+                                    (grid->coord2hi[i] - grid->coord2lo[i]);
+    CUDA_TRY(cudaMemcpyAsync(d.gbxarea, area.data(), ng * 8, cudaMemcpyHostToDevice, x->stream));
+    CUDA_TRY(cudaStreamSynchronize(x->stream));  // area is a host temporary
+    const int rc2 = cleo_b200_monitors_begin(x);
+    if (rc2 != CLEO_OK) {
+      cleo_b200_destroy(x);
+      return rc2;
+    }
+  }
   {  // persistent grids of the batched kernels: full occupancy on every SM
     int dev = 0, sms = 148, occ = 1;
     CUDA_TRY(cudaGetDevice(&dev));
@@ -1491,6 +1615,60 @@ int cleo_b200_download_state(cleo_b200_ctx* x, cleo_b200_gbx_state* h) {
     if (!dst[k]) return CLEO_ERR_ARGUMENT;
     CUDA_TRY(cudaMemcpy(dst[k], src[k], ng * 8, cudaMemcpyDeviceToHost));
   }
+  return CLEO_OK;
+}
+
+int cleo_b200_monitors_begin(cleo_b200_ctx* x) {
+  if (!x) return CLEO_ERR_ARGUMENT;
+  const DevCtx& d = x->d;
+  if (!d.precip) return CLEO_OK;  // no monitors selected
+  const size_t ng = d.ngbxs ? d.ngbxs : 1;
+  k_mon_mm<<<grid_for(d.ngbxs, 256), 256, 0, x->stream>>>(d, 0, 1);
+  x->launches += 1;
+  for (int r = 0; r < 2; ++r)
+    for (int w = 0; w < 2; ++w) {
+      CUDA_TRY(cudaMemsetAsync(d.mm0[r][w], 0, ng * 8, x->stream));
+      CUDA_TRY(cudaMemsetAsync(d.mm1[r][w], 0, ng * 4, x->stream));
+      CUDA_TRY(cudaMemsetAsync(d.mm2[r][w], 0, ng * 4, x->stream));
+    }
+  CUDA_TRY(cudaMemsetAsync(d.precip, 0, ng * 8, x->stream));
+  CUDA_TRY(cudaGetLastError());
+  return CLEO_OK;
+}
+
+int cleo_b200_download_monitors(cleo_b200_ctx* x, cleo_b200_monitors* o, int reset) {
+  if (!x || !o) return CLEO_ERR_ARGUMENT;
+  const DevCtx& d = x->d;
+  const size_t ng = d.ngbxs;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  uint64_t* h0[2][2] = {{o->mom0_micro, o->mom0_motion}, {o->rain_mom0_micro, o->rain_mom0_motion}};
+  float* h1[2][2] = {{o->mom1_micro, o->mom1_motion}, {o->rain_mom1_micro, o->rain_mom1_motion}};
+  float* h2[2][2] = {{o->mom2_micro, o->mom2_motion}, {o->rain_mom2_micro, o->rain_mom2_motion}};
+  for (int r = 0; r < 2; ++r)
+    for (int w = 0; w < 2; ++w) {
+      if (!d.precip) {  // no monitors selected: nothing accumulated
+        if (h0[r][w]) memset(h0[r][w], 0, ng * 8);
+        if (h1[r][w]) memset(h1[r][w], 0, ng * 4);
+        if (h2[r][w]) memset(h2[r][w], 0, ng * 4);
+        continue;
+      }
+      if (h0[r][w]) CUDA_TRY(cudaMemcpy(h0[r][w], d.mm0[r][w], ng * 8, cudaMemcpyDeviceToHost));
+      if (h1[r][w]) CUDA_TRY(cudaMemcpy(h1[r][w], d.mm1[r][w], ng * 4, cudaMemcpyDeviceToHost));
+      if (h2[r][w]) CUDA_TRY(cudaMemcpy(h2[r][w], d.mm2[r][w], ng * 4, cudaMemcpyDeviceToHost));
+      if (reset) {
+        CUDA_TRY(cudaMemsetAsync(d.mm0[r][w], 0, ng * 8, x->stream));
+        CUDA_TRY(cudaMemsetAsync(d.mm1[r][w], 0, ng * 4, x->stream));
+        CUDA_TRY(cudaMemsetAsync(d.mm2[r][w], 0, ng * 4, x->stream));
+      }
+    }
+  if (o->precip) {
+    if (d.precip)
+      CUDA_TRY(cudaMemcpy(o->precip, d.precip, ng * 8, cudaMemcpyDeviceToHost));
+    else
+      memset(o->precip, 0, ng * 8);
+  }
+  if (reset && d.precip) CUDA_TRY(cudaMemsetAsync(d.precip, 0, ng * 8, x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
   return CLEO_OK;
 }
 

@@ -126,6 +126,18 @@ class SDM:
                                                 abi.ptr(it, C.c_uint64)), "in download_budgets")
         return cm, it
 
+    def monitors_begin(self):
+        """before_timestepping of the SDMMonitor members selected by params.monitors."""
+        self._check(self._f("monitors_begin")(self._ctx), "in monitors_begin")
+
+    def download_monitors(self, reset: bool = False) -> dict:
+        """Accumulated mass-moment changes (micro/motion, all/rain) and precipitation."""
+        out = {name: np.zeros(self.ngbxs, dtype=dt) for name, dt in abi.MONITOR_FIELDS}
+        m = abi.monitors_struct(out)
+        self._check(self._f("download_monitors")(self._ctx, C.byref(m), int(bool(reset))),
+                    "in download_monitors")
+        return out
+
 
 def make_sdm(workload: dict, lib=None, prefix="cleo_b200", params=None) -> SDM:
     """Create, upload supers and states of a workload dict (see :mod:`cleo_b200.workloads`)."""

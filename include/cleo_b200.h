@@ -95,6 +95,12 @@ enum cleo_exec {             /* how the microphysics of one SDM step is schedule
   CLEO_EXEC_BATCHED = 1      /* flat two-pass condensation + size-bucketed persistent collisions */
 };
 
+enum cleo_monitor {          /* SDMMonitor members (libs/observers/sdmmonitor/) */
+  CLEO_MONITOR_MASSMOMENTS = 1,     /* MonitorMassMomentsChange<MonitorMassMomentsChangeViews> */
+  CLEO_MONITOR_RAINMASSMOMENTS = 2, /* MonitorMassMomentsChange<MonitorRainMassMomentsChangeViews> */
+  CLEO_MONITOR_PRECIPITATION = 4    /* MonitorPrecipitation */
+};
+
 #define CLEO_STEP_OFF 0xFFFFFFFFu /* interval value that switches a process off (on_step false) */
 
 /*
@@ -133,7 +139,8 @@ typedef struct cleo_b200_params {
   int32_t nr_seed;          /* enum cleo_nrseed */
   /* execution (no reference counterpart: results do not depend on it) */
   int32_t exec_mode;        /* enum cleo_exec */
-  int32_t reserved0;
+  /* SDMMonitor members to run (libs/observers/sdmmonitor/): a bitmask of enum cleo_monitor */
+  int32_t monitors;
 } cleo_b200_params;
 
 /*
@@ -148,6 +155,9 @@ typedef struct cleo_b200_grid {
   uint32_t ndims[3]; /* number of gridboxes along [coord3, coord1, coord2] */
   const double *coord3lo, *coord3hi, *coord1lo, *coord1hi, *coord2lo, *coord2hi;
   const uint32_t *back3, *fwd3, *back1, *fwd1, *back2, *fwd2;
+  /* horizontal area of each gridbox (GbxBoundsFromBinary::gbxarea,
+   * gbx_bounds_from_binary.cpp:206-215), used by the precipitation monitor; may be NULL */
+  const double* gbxarea;
 } cleo_b200_grid;
 
 /* Per-gridbox thermodynamic State (state.hpp:33-120) as SoA arrays of length ngbxs. */
@@ -275,6 +285,30 @@ int cleo_b200_stage_times(cleo_b200_ctx* ctx, double ms[5], uint64_t count[5]);
  */
 int cleo_b200_sort_by_gridbox_static(const uint32_t* d_sdgbxindex, uint32_t n, uint32_t ngbxs,
                                      uint32_t* d_order, uint32_t* d_gstart, void* stream);
+
+/*
+ * SDMMonitor members selected by params.monitors, per gridbox (host arrays of ngbxs, any may be
+ * NULL). Mass moments (calculate_massmoments / calculate_rainmassmoments,
+ * massmoments_observer.cpp:38-113): mom0 = sum xi (u64), mom1 = sum (float)(xi m), mom2 = sum
+ * (float)(xi m m) over the gridbox's superdroplets (rain: radius >= 40 um), summed in the
+ * superdroplets' order; the changes accumulated after each SDM step's microphysics and after each
+ * motion step (MonitorMassMomentsChange::monitor_microphysics / monitor_motion,
+ * monitor_massmoments_change.hpp:99-121, 287-305). Precipitation: condensate mass x xi / rho_l /
+ * gridbox area of superdroplets that cross their gridbox's lower coord3 bound during motion
+ * (MonitorPrecipitation::monitor_precipitation, monitor_precipitation_observer.hpp:97-107).
+ */
+typedef struct cleo_b200_monitors {
+  uint64_t *mom0_micro, *mom0_motion, *rain_mom0_micro, *rain_mom0_motion;
+  float *mom1_micro, *mom2_micro, *mom1_motion, *mom2_motion;
+  float *rain_mom1_micro, *rain_mom2_micro, *rain_mom1_motion, *rain_mom2_motion;
+  double* precip;
+} cleo_b200_monitors;
+/* before_timestepping of the monitors: the current moments become the baseline of the
+ * accumulated changes, and all accumulations restart from zero. */
+int cleo_b200_monitors_begin(cleo_b200_ctx* ctx);
+/* Copy the accumulated changes and precipitation to the host; reset != 0 then zeroes them
+ * (reset_monitor; the baselines stay). */
+int cleo_b200_download_monitors(cleo_b200_ctx* ctx, cleo_b200_monitors* out, int reset);
 
 /*
  * Condensation surrogate (no counterpart in the reference, whose Newton-Raphson iteration always

@@ -93,6 +93,14 @@ struct oc_ctx {
   size_t* refs0; /* SupersInGbx refs per gridbox, relative to the domain start */
   size_t* refs1;
   size_t* counts;
+  /* SDMMonitor members (params.monitors): [0] all droplets, [1] raindrops; changes after
+   * microphysics ([.][0]) and after motion ([.][1]); the previous moments; precipitation */
+  double* gbxarea;
+  uint64_t* mm0[2][2];
+  float *mm1[2][2], *mm2[2][2];
+  uint64_t* prev0[2];
+  float *prev1[2], *prev2[2];
+  double* precip;
   /* errors */
   cleo_b200_error err;
 };
@@ -962,6 +970,11 @@ static void move_superdrop(const oc_ctx* c, uint32_t g, sd_t* drop) {
   drop->c3 += delta3;
   drop->c1 += delta1;
   drop->c2 += delta2;
+  /* monitor_precipitation: monitor_precipitation_observer.hpp:97-107 */
+  if ((c->p.monitors & CLEO_MONITOR_PRECIPITATION) && drop->c3 < bz.lo) {
+    const double m = condensate_mass(drop->r, drop->msol) * (double)drop->xi / Rho_l / c->gbxarea[g];
+    c->precip[g] += m;
+  }
   /* superdrop_gbx: predcorrmotion.hpp:85-106 -> get_no_decomposition_bounding_gridbox,
    * cartesianmaps.cpp:278-286 */
   double n3 = drop->c3, n1 = drop->c1, n2 = drop->c2;
@@ -1056,6 +1069,88 @@ static uint32_t next_step(uint32_t interval, uint32_t t) {
 /* ------------------------------------------------------------------------------------------ */
 /* the SDM step: sdmmethods.hpp:54-93, 184-230, 319-332; movesupersindomain.hpp:234-301         */
 /* ------------------------------------------------------------------------------------------ */
+/* ------------------------------------------------------------------------------------------ */
+/* SDMMonitor members: monitor_massmoments_change.hpp, monitor_precipitation_observer.hpp     */
+/* ------------------------------------------------------------------------------------------ */
+/* calculate_massmoments / calculate_rainmassmoments: massmoments_observer.cpp:38-113, the
+ * reduction in the superdroplets' order (Kokkos' serial order) */
+static void massmoments(const sd_t* supers, size_t n, int rain, uint64_t* m0, float* m1,
+                        float* m2) {
+  const double rlim = 40e-6 / R0;
+  uint64_t a0 = 0;
+  float a1 = 0.0f, a2 = 0.0f;
+  for (size_t kk = 0; kk < n; ++kk) {
+    const sd_t* drop = &supers[kk];
+    const int binary = rain ? (drop->r >= rlim) : 1;
+    a0 += (uint64_t)(drop->xi * (uint64_t)binary);
+    const double mass = sd_mass(drop->r, drop->msol);
+    const double xi = (double)drop->xi;
+    a1 += (float)(xi * mass * (double)binary);
+    a2 += (float)(xi * mass * mass * (double)binary);
+  }
+  *m0 = a0;
+  *m1 = a1;
+  *m2 = a2;
+}
+/* fetch_delta_massmoments: monitor_massmoments_change.hpp:99-121 (which = 0 after microphysics,
+ * 1 after motion) */
+static void monitor_massmoments(oc_ctx* c, uint32_t g, const sd_t* supers, size_t n, int which) {
+  for (int rain = 0; rain < 2; ++rain) {
+    if (!(c->p.monitors & (rain ? CLEO_MONITOR_RAINMASSMOMENTS : CLEO_MONITOR_MASSMOMENTS)))
+      continue;
+    uint64_t m0;
+    float m1, m2;
+    massmoments(supers, n, rain, &m0, &m1, &m2);
+    c->mm0[rain][which][g] += m0 - c->prev0[rain][g];
+    c->mm1[rain][which][g] += m1 - c->prev1[rain][g];
+    c->mm2[rain][which][g] += m2 - c->prev2[rain][g];
+    c->prev0[rain][g] = m0;
+    c->prev1[rain][g] = m1;
+    c->prev2[rain][g] = m2;
+  }
+}
+static void monitor_motion(oc_ctx* c) { /* MonitorMassMomentsChange::monitor_motion :295-305 */
+  for (uint32_t g = 0; g < c->ngbxs; ++g)
+    monitor_massmoments(c, g, &c->sd[c->refs0[g]], c->refs1[g] - c->refs0[g], 1);
+}
+
+int oc_monitors_begin(oc_ctx* c) { /* before_timestepping: :75-82, reset_monitor */
+  for (int rain = 0; rain < 2; ++rain) {
+    for (uint32_t g = 0; g < c->ngbxs; ++g) {
+      massmoments(&c->sd[c->refs0[g]], c->refs1[g] - c->refs0[g], rain, &c->prev0[rain][g],
+                  &c->prev1[rain][g], &c->prev2[rain][g]);
+      for (int w = 0; w < 2; ++w) {
+        c->mm0[rain][w][g] = 0;
+        c->mm1[rain][w][g] = 0.0f;
+        c->mm2[rain][w][g] = 0.0f;
+      }
+    }
+  }
+  memset(c->precip, 0, sizeof(double) * (c->ngbxs ? c->ngbxs : 1));
+  return CLEO_OK;
+}
+
+int oc_download_monitors(oc_ctx* c, cleo_b200_monitors* o, int reset) {
+  const size_t n = c->ngbxs;
+  uint64_t* d0[2][2] = {{o->mom0_micro, o->mom0_motion}, {o->rain_mom0_micro, o->rain_mom0_motion}};
+  float* d1[2][2] = {{o->mom1_micro, o->mom1_motion}, {o->rain_mom1_micro, o->rain_mom1_motion}};
+  float* d2[2][2] = {{o->mom2_micro, o->mom2_motion}, {o->rain_mom2_micro, o->rain_mom2_motion}};
+  for (int r = 0; r < 2; ++r)
+    for (int w = 0; w < 2; ++w) {
+      if (d0[r][w]) memcpy(d0[r][w], c->mm0[r][w], n * 8);
+      if (d1[r][w]) memcpy(d1[r][w], c->mm1[r][w], n * 4);
+      if (d2[r][w]) memcpy(d2[r][w], c->mm2[r][w], n * 4);
+      if (reset) {
+        memset(c->mm0[r][w], 0, n * 8);
+        memset(c->mm1[r][w], 0, n * 4);
+        memset(c->mm2[r][w], 0, n * 4);
+      }
+    }
+  if (o->precip) memcpy(o->precip, c->precip, n * 8);
+  if (reset) memset(c->precip, 0, n * 8);
+  return CLEO_OK;
+}
+
 int oc_step(oc_ctx* c, uint32_t t_mdl, uint32_t t_next) {
   const cleo_b200_params* p = &c->p;
   g_err = &c->err;
@@ -1076,6 +1171,7 @@ int oc_step(oc_ctx* c, uint32_t t_mdl, uint32_t t_next) {
       }
       sort_and_set_refs(c); /* CartesianTransportAcrossDomain on 1 process: sort_totsupers */
       effect_on_qcond(c);
+      monitor_motion(c); /* movesupersindomain.hpp:297 */
     }
 
     /* sdm_microphysics: sdmmethods.hpp:184-230 */
@@ -1097,6 +1193,7 @@ int oc_step(oc_ctx* c, uint32_t t_mdl, uint32_t t_next) {
         const uint32_t b = next_step(p->collstep, subt);
         subt = (a < b) ? a : b;
       }
+      monitor_massmoments(c, g, supers, n, 0); /* monitor_microphysics, sdmmethods.hpp:76 */
       if (n != nbefore) any_change = 1;
     }
     if (any_change) sort_and_set_refs(c);
@@ -1148,6 +1245,21 @@ int oc_create(const cleo_b200_params* p, const cleo_b200_grid* g, size_t capacit
   c->refs0 = (size_t*)calloc(n ? n : 1, sizeof(size_t));
   c->refs1 = (size_t*)calloc(n ? n : 1, sizeof(size_t));
   c->counts = (size_t*)calloc(n + 1, sizeof(size_t));
+  c->gbxarea = (double*)calloc(n ? n : 1, sizeof(double));
+  for (size_t i = 0; i < n; ++i)
+    c->gbxarea[i] = g->gbxarea ? g->gbxarea[i]
+                               : (g->coord1hi[i] - g->coord1lo[i]) * (g->coord2hi[i] - g->coord2lo[i]);
+  for (int r = 0; r < 2; ++r) {
+    for (int w = 0; w < 2; ++w) {
+      c->mm0[r][w] = (uint64_t*)calloc(n ? n : 1, 8);
+      c->mm1[r][w] = (float*)calloc(n ? n : 1, 4);
+      c->mm2[r][w] = (float*)calloc(n ? n : 1, 4);
+    }
+    c->prev0[r] = (uint64_t*)calloc(n ? n : 1, 8);
+    c->prev1[r] = (float*)calloc(n ? n : 1, 4);
+    c->prev2[r] = (float*)calloc(n ? n : 1, 4);
+  }
+  c->precip = (double*)calloc(n ? n : 1, sizeof(double));
   c->err.code = CLEO_OK;
   c->err.gbxindex = OOB;
   *out = c;
@@ -1163,6 +1275,13 @@ void oc_destroy(oc_ctx* c) {
   uint32_t* uu[] = {c->back3, c->fwd3, c->back1, c->fwd1, c->back2, c->fwd2};
   for (size_t i = 0; i < sizeof(uu) / sizeof(uu[0]); ++i) free(uu[i]);
   free(c->nr_iters); free(c->sd); free(c->tmp); free(c->refs0); free(c->refs1); free(c->counts);
+  free(c->gbxarea); free(c->precip);
+  for (int r = 0; r < 2; ++r) {
+    for (int w = 0; w < 2; ++w) {
+      free(c->mm0[r][w]); free(c->mm1[r][w]); free(c->mm2[r][w]);
+    }
+    free(c->prev0[r]); free(c->prev1[r]); free(c->prev2[r]);
+  }
   free(c);
 }
 

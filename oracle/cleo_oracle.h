@@ -30,6 +30,8 @@ int oc_status(oc_ctx* c, cleo_b200_error* err);
 int oc_download_supers(oc_ctx* c, cleo_b200_supers* h, size_t* n_domain, size_t* n_total);
 int oc_download_state(oc_ctx* c, cleo_b200_gbx_state* h);
 int oc_download_budgets(oc_ctx* c, double* cond_mass, uint64_t* nr_iters);
+int oc_monitors_begin(oc_ctx* c);
+int oc_download_monitors(oc_ctx* c, cleo_b200_monitors* out, int reset);
 
 /* Batch of independent implicit-Euler condensation solves (host arrays). */
 int oc_condensation_solve(const cleo_b200_params* p, size_t n, const double* radius,

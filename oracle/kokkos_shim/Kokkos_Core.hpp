@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <tuple>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
@@ -72,9 +73,12 @@ namespace Kokkos {
 
 /* ---------------------------------------------------------------- spaces, pair, misc */
 struct HostSpace {};
+struct LayoutRight {};
+struct LayoutLeft {};
 struct Serial {
   using memory_space = HostSpace;
   using execution_space = Serial;
+  using array_layout = LayoutRight;
 };
 using DefaultExecutionSpace = Serial;
 using DefaultHostExecutionSpace = Serial;
@@ -148,6 +152,10 @@ template <class T, class U>
 inline T atomic_fetch_add(T* p, U v) {
   return __atomic_fetch_add(p, static_cast<T>(v), __ATOMIC_RELAXED);
 }
+template <class T, class U>
+inline void atomic_add(T* p, U v) {  // integer or floating point
+  std::atomic_ref<T>(*p).fetch_add(static_cast<T>(v), std::memory_order_relaxed);
+}
 
 /* ---------------------------------------------------------------- views */
 template <class DataType>
@@ -195,6 +203,7 @@ class View {
   bool is_allocated() const { return ptr_ != nullptr; }
   const std::shared_ptr<void>& owner() const { return own_; }
   std::string label() const { return ""; }
+  void reallocate(size_t n) { allocate(n); }  // contents not kept (Kokkos::realloc)
 
  private:
   void allocate(size_t n) {
@@ -210,6 +219,11 @@ class View {
   template <class D, class... P>
   friend class View;
 };
+
+template <class D, class... P>
+void realloc(View<D, P...>& v, size_t n) {
+  v.reallocate(n);
+}
 
 /* Subview of a 1-D view by an index range is a 1-D view of the same type. */
 template <class V, class... Args>
@@ -438,6 +452,19 @@ void parallel_reduce(const TeamThreadRangeBoundaries<M>& r, const F& f, T& resul
   T acc = T{};
   for (size_t i = r.begin_; i < r.end_; ++i) f(i, acc);
   result = acc;
+}
+/* several sum reductions at once, accumulated in index order */
+template <class M, class F, class T1, class T2, class... Ts>
+void parallel_reduce(const TeamThreadRangeBoundaries<M>& r, const F& f, T1& r1, T2& r2,
+                     Ts&... rs) {
+  T1 a1{};
+  T2 a2{};
+  std::tuple<Ts...> as{};
+  for (size_t i = r.begin_; i < r.end_; ++i)
+    std::apply([&](auto&... a) { f(i, a1, a2, a...); }, as);
+  r1 = a1;
+  r2 = a2;
+  std::apply([&](auto&... a) { ((rs = a), ...); }, as);
 }
 template <class E, class F>
 void parallel_reduce(const std::string&, const TeamPolicy<E>& p, const F& f, const LOr<bool>& red) {

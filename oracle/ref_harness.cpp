@@ -25,6 +25,8 @@
 #include "cartesiandomain/movement/cartesian_motion.hpp"
 #include "cartesiandomain/movement/cartesian_movement.hpp"
 #include "gridboxes/boundary_conditions.hpp"
+#include "observers/sdmmonitor/monitor_massmoments_change.hpp"
+#include "observers/sdmmonitor/monitor_precipitation_observer.hpp"
 #include "runcleo/sdmmethods.hpp"
 #include "superdrops/collisions/breakup.hpp"
 #include "superdrops/collisions/breakup_nfrags.hpp"
@@ -118,18 +120,44 @@ struct AnyEnact {
   }
 };
 
-/* ---- monitor that accumulates the condensed mass per gridbox (condensation.hpp:149) ---- */
+/* ---- SDMMonitor: the condensed mass per gridbox (condensation.hpp:149) plus the reference's
+ * own MonitorMassMomentsChange (all droplets, raindrops) and MonitorPrecipitation, each active
+ * when selected by params.monitors ---- */
+using MassMomsMo = MonitorMassMomentsChange<MonitorMassMomentsChangeViews>;
+using RainMassMomsMo = MonitorMassMomentsChange<MonitorRainMassMomentsChangeViews>;
 struct BudgetMonitor {
   Kokkos::View<double*> cond_mass;
-  void reset_monitor() const {}
-  KOKKOS_FUNCTION void before_timestepping(const TeamMember&, const viewd_constsupers) const {}
+  int mask;
+  MassMomsMo mm;
+  RainMassMomsMo rmm;
+  MonitorPrecipitation pr;
+  BudgetMonitor(Kokkos::View<double*> cm, int m, size_t ngbxs)
+      : cond_mass(cm), mask(m), mm(ngbxs), rmm(ngbxs), pr(ngbxs) {}
+  void reset_monitor() const {
+    mm.reset_monitor();
+    rmm.reset_monitor();
+    pr.reset_monitor();
+  }
+  KOKKOS_FUNCTION void before_timestepping(const TeamMember& tm,
+                                           const subviewd_constsupers s) const {
+    if (mask & CLEO_MONITOR_MASSMOMENTS) mm.before_timestepping(tm, s);
+    if (mask & CLEO_MONITOR_RAINMASSMOMENTS) rmm.before_timestepping(tm, s);
+  }
   KOKKOS_FUNCTION void monitor_condensation(const TeamMember& tm, const double d) const {
     cond_mass(tm.league_rank()) += d;
   }
-  KOKKOS_FUNCTION void monitor_microphysics(const TeamMember&, const viewd_constsupers) const {}
-  void monitor_motion(const auto, const auto) const {}
-  KOKKOS_FUNCTION void monitor_precipitation(const TeamMember&, const unsigned int, const auto&,
-                                             Superdrop&) const {}
+  KOKKOS_FUNCTION void monitor_microphysics(const TeamMember& tm, const viewd_constsupers s) const {
+    if (mask & CLEO_MONITOR_MASSMOMENTS) mm.monitor_microphysics(tm, s);
+    if (mask & CLEO_MONITOR_RAINMASSMOMENTS) rmm.monitor_microphysics(tm, s);
+  }
+  void monitor_motion(const viewd_constgbx d_gbxs, const subviewd_constsupers ds) const {
+    if (mask & CLEO_MONITOR_MASSMOMENTS) mm.monitor_motion(d_gbxs, ds);
+    if (mask & CLEO_MONITOR_RAINMASSMOMENTS) rmm.monitor_motion(d_gbxs, ds);
+  }
+  KOKKOS_FUNCTION void monitor_precipitation(const TeamMember& tm, const unsigned int gi,
+                                             const auto& maps, Superdrop& d) const {
+    if (mask & CLEO_MONITOR_PRECIPITATION) pr.monitor_precipitation(tm, gi, maps, d);
+  }
 };
 struct BudgetObserver {
   BudgetMonitor mo;
@@ -176,6 +204,7 @@ struct ref_ctx {
   dualview_gbx gbxs;
   std::unique_ptr<SupersInDomain> allsupers;
   Kokkos::View<double*> cond_mass;
+  std::unique_ptr<BudgetMonitor> mon;
   cleo_b200_error err{CLEO_OK, 0xFFFFFFFFu, 0};
 };
 
@@ -216,7 +245,10 @@ int ref_create(const cleo_b200_params* p, const cleo_b200_grid* g, size_t capaci
       b3.insert(i, g->back3[i]); f3.insert(i, g->fwd3[i]);
       b1.insert(i, g->back1[i]); f1.insert(i, g->fwd1[i]);
       b2.insert(i, g->back2[i]); f2.insert(i, g->fwd2[i]);
-      areas.insert(i, 0.0); vols.insert(i, 0.0);
+      const double area = g->gbxarea ? g->gbxarea[i]
+                                     : (g->coord1hi[i] - g->coord1lo[i]) *
+                                           (g->coord2hi[i] - g->coord2lo[i]);
+      areas.insert(i, area); vols.insert(i, 0.0);
     }
     c->gbxmaps.set_coord3bounds_via_copy(h3);
     c->gbxmaps.set_coord1bounds_via_copy(h1);
@@ -251,7 +283,8 @@ int ref_create(const cleo_b200_params* p, const cleo_b200_grid* g, size_t capaci
     const MoveT movesupers = cartesian_movement(c->gbxmaps, motion, NullBoundaryConditions{});
 
     c->cond_mass = Kokkos::View<double*>("cond_mass", g->ngbxs);
-    BudgetObserver obs{BudgetMonitor{c->cond_mass}};
+    c->mon = std::make_unique<BudgetMonitor>(c->cond_mass, P.monitors, g->ngbxs);
+    BudgetObserver obs{*c->mon};
     const unsigned int couplstep = P.motionstep == CLEO_STEP_OFF ? 1u : P.motionstep;
     c->sdm = std::make_unique<SDM>(couplstep, c->gbxmaps, microphys, movesupers, obs);
     c->gbxs = dualview_gbx("gbxs", g->ngbxs);
@@ -358,6 +391,47 @@ int ref_download_state(ref_ctx* c, cleo_b200_gbx_state* h) {
     h->uvel_lo[ii] = s.uvel.first; h->uvel_hi[ii] = s.uvel.second;
     h->vvel_lo[ii] = s.vvel.first; h->vvel_hi[ii] = s.vvel.second;
   }
+  return CLEO_OK;
+}
+
+/* before_timestepping of the monitors over every gridbox (as DoSDMMonitorObs does,
+ * do_sdmmonitor_obs.hpp) and reset_monitor */
+int ref_monitors_begin(ref_ctx* c) {
+  try {
+    const auto d_gbxs = c->gbxs.view_device();
+    const auto domainsupers = c->allsupers->domain_supers_readonly();
+    const BudgetMonitor mon = *c->mon;
+    Kokkos::parallel_for(
+        "monitors_begin", TeamPolicy(c->ngbxs, Kokkos::AUTO()),
+        [=](const TeamMember& tm) {
+          const auto ii = tm.league_rank();
+          mon.before_timestepping(tm, d_gbxs(ii).supersingbx.readonly(domainsupers));
+        });
+    mon.reset_monitor();
+  } catch (const kokkos_shim::Abort& e) {
+    return code_of(e.what());
+  }
+  return CLEO_OK;
+}
+
+int ref_download_monitors(ref_ctx* c, cleo_b200_monitors* o, int reset) {
+  const BudgetMonitor& m = *c->mon;
+  for (unsigned int ii = 0; ii < c->ngbxs; ++ii) {
+    if (o->mom0_micro) o->mom0_micro[ii] = m.mm.microphysics_moms.d_delta_mom0(ii);
+    if (o->mom1_micro) o->mom1_micro[ii] = m.mm.microphysics_moms.d_delta_mom1(ii);
+    if (o->mom2_micro) o->mom2_micro[ii] = m.mm.microphysics_moms.d_delta_mom2(ii);
+    if (o->mom0_motion) o->mom0_motion[ii] = m.mm.motion_moms.d_delta_mom0(ii);
+    if (o->mom1_motion) o->mom1_motion[ii] = m.mm.motion_moms.d_delta_mom1(ii);
+    if (o->mom2_motion) o->mom2_motion[ii] = m.mm.motion_moms.d_delta_mom2(ii);
+    if (o->rain_mom0_micro) o->rain_mom0_micro[ii] = m.rmm.microphysics_moms.d_delta_mom0(ii);
+    if (o->rain_mom1_micro) o->rain_mom1_micro[ii] = m.rmm.microphysics_moms.d_delta_mom1(ii);
+    if (o->rain_mom2_micro) o->rain_mom2_micro[ii] = m.rmm.microphysics_moms.d_delta_mom2(ii);
+    if (o->rain_mom0_motion) o->rain_mom0_motion[ii] = m.rmm.motion_moms.d_delta_mom0(ii);
+    if (o->rain_mom1_motion) o->rain_mom1_motion[ii] = m.rmm.motion_moms.d_delta_mom1(ii);
+    if (o->rain_mom2_motion) o->rain_mom2_motion[ii] = m.rmm.motion_moms.d_delta_mom2(ii);
+    if (o->precip) o->precip[ii] = m.pr.d_data(ii);
+  }
+  if (reset) m.reset_monitor();
   return CLEO_OK;
 }
 

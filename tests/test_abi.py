@@ -34,7 +34,7 @@ def test_struct_sizes_match_header_layout():
     # cleo_b200_params: 4 u32 + 4 f64 + (i32,u32) + 2 f64 + 2 i32 + 2 f64 + 2 i32 + f64
     #                   + 2 i32 + f64 + u64 + 2 i32 + 2 i32
     assert C.sizeof(abi.Params) == 16 + 32 + 8 + 16 + 8 + 16 + 8 + 8 + 8 + 8 + 8 + 8 + 8
-    assert C.sizeof(abi.Grid) == 4 + 12 + 12 * 8
+    assert C.sizeof(abi.Grid) == 4 + 12 + 13 * 8
     assert C.sizeof(abi.Supers) == 8 * 8
     assert C.sizeof(abi.GbxState) == 11 * 8
     assert C.sizeof(abi.Error) == 16
