@@ -67,7 +67,7 @@ def make_params(*, condtstep: float | None = None, colltstep: float | None = Non
                 nfrags_tv: int = TV_ROGERSGK, flag_kind: int = FLAG_STRAUB,
                 flag_tv: int = TV_ROGERSGK, flag_coaleff: float = 1.0, seed: int = 0,
                 motion_tv: int = TV_NULL, nr_seed: int = NRSEED_REFERENCE,
-                exec_mode: int = 1) -> Params:
+                exec_mode: int = 1, monitors: int = 0) -> Params:
     """Parameters of one SDM configuration. A timestep of None switches that process off."""
     p = Params()
     p.condstep = STEP_OFF if condtstep is None else realtime2step(condtstep)
@@ -98,6 +98,7 @@ def make_params(*, condtstep: float | None = None, colltstep: float | None = Non
     p.motion_tv = int(motion_tv)
     p.nr_seed = int(nr_seed)
     p.exec_mode = int(exec_mode)
+    p.monitors = int(monitors)
     return p
 
 

@@ -16,6 +16,7 @@
  * coalbure.hpp:173-185) and Condensation through its own factory (condensation.hpp:242-253).
  */
 #include <cfloat>
+#include <filesystem>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -25,6 +26,9 @@
 #include "cartesiandomain/movement/cartesian_motion.hpp"
 #include "cartesiandomain/movement/cartesian_movement.hpp"
 #include "gridboxes/boundary_conditions.hpp"
+#include "coupldyn_fromfile/fromfile_cartesian_dynamics.hpp"
+#include "initialise/gbx_bounds_from_binary.hpp"
+#include "initialise/init_all_supers_from_binary.hpp"
 #include "observers/sdmmonitor/monitor_massmoments_change.hpp"
 #include "observers/sdmmonitor/monitor_precipitation_observer.hpp"
 #include "runcleo/sdmmethods.hpp"
@@ -432,6 +436,82 @@ int ref_download_monitors(ref_ctx* c, cleo_b200_monitors* o, int reset) {
     if (o->precip) o->precip[ii] = m.pr.d_data(ii);
   }
   if (reset) m.reset_monitor();
+  return CLEO_OK;
+}
+
+/* ---- CLEO's binary initialisation and coupled-dynamics readers ---- */
+/* GbxBoundsFromBinary (gbx_bounds_from_binary.cpp): bounds [6 per gridbox], area, volume */
+int ref_read_gridfile(const char* path, size_t ngbxs, unsigned int nspacedims, double* bounds,
+                      double* areas, double* vols) {
+  try {
+    const GbxBoundsFromBinary gfb(ngbxs, nspacedims, std::filesystem::path(path));
+    for (unsigned int i = 0; i < ngbxs; ++i) {
+      const auto b3 = gfb.get_coord3gbxbounds(i), b1 = gfb.get_coord1gbxbounds(i),
+                 b2 = gfb.get_coord2gbxbounds(i);
+      const double b[6] = {b3.first, b3.second, b1.first, b1.second, b2.first, b2.second};
+      for (int k = 0; k < 6; ++k) bounds[6 * i + k] = b[k];
+      areas[i] = gfb.gbxarea(i);
+      vols[i] = gfb.gbxvol(i);
+    }
+  } catch (const std::exception&) {
+    return CLEO_ERR_ARGUMENT;
+  }
+  return CLEO_OK;
+}
+
+/* InitAllSupersFromBinary (init_all_supers_from_binary.cpp) */
+int ref_read_initsupers(const char* path, size_t maxnsupers, unsigned int nspacedims,
+                        uint32_t* gbx, uint64_t* xi, double* radius, double* msol, double* c3,
+                        double* c1, double* c2) {
+  try {
+    const InitAllSupersFromBinary init(maxnsupers, std::filesystem::path(path), nspacedims);
+    const InitSupersData d = init.fetch_data();
+    for (size_t k = 0; k < maxnsupers; ++k) {
+      gbx[k] = d.sdgbxindexes.at(k);
+      xi[k] = d.xis.at(k);
+      radius[k] = d.radii.at(k);
+      msol[k] = d.msols.at(k);
+      c3[k] = k < d.coord3s.size() ? d.coord3s[k] : 0.0;
+      c1[k] = k < d.coord1s.size() ? d.coord1s[k] : 0.0;
+      c2[k] = k < d.coord2s.size() ? d.coord2s[k] : 0.0;
+    }
+  } catch (const std::exception&) {
+    return CLEO_ERR_ARGUMENT;
+  }
+  return CLEO_OK;
+}
+
+/* CartesianDynamics (fromfile_cartesian_dynamics.cpp) after `step` increments, read the way
+ * FromFileComms::update_gridbox_state does (fromfilecomms.cpp:40-52). paths: press, temp,
+ * qvap, qcond, wvel, uvel, vvel. out: press, temp, qvap, qcond, wlo, whi, ulo, uhi, vlo, vhi. */
+int ref_fromfile_state(const char* const* paths, unsigned int nspacedims, const uint64_t* ndims,
+                       unsigned int nsteps, unsigned int step, double* const* out) {
+  try {
+    OptionalConfigParams::FromFileDynamicsParams cfg;
+    cfg.nspacedims = nspacedims;
+    cfg.press = paths[0];
+    cfg.temp = paths[1];
+    cfg.qvap = paths[2];
+    cfg.qcond = paths[3];
+    cfg.wvel = paths[4];
+    cfg.uvel = paths[5];
+    cfg.vvel = paths[6];
+    CartesianDynamics dyn(cfg, {ndims[0], ndims[1], ndims[2]}, nsteps);
+    for (unsigned int s = 0; s < step; ++s) dyn.increment_position();
+    const size_t ng = ndims[0] * ndims[1] * ndims[2];
+    for (size_t ii = 0; ii < ng; ++ii) {
+      out[0][ii] = dyn.get_press(ii);
+      out[1][ii] = dyn.get_temp(ii);
+      out[2][ii] = dyn.get_qvap(ii);
+      out[3][ii] = dyn.get_qcond(ii);
+      const auto w = dyn.get_wvel(ii), u = dyn.get_uvel(ii), v = dyn.get_vvel(ii);
+      out[4][ii] = w.first; out[5][ii] = w.second;
+      out[6][ii] = u.first; out[7][ii] = u.second;
+      out[8][ii] = v.first; out[9][ii] = v.second;
+    }
+  } catch (const std::exception&) {
+    return CLEO_ERR_ARGUMENT;
+  }
   return CLEO_OK;
 }
 

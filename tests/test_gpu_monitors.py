@@ -58,3 +58,24 @@ def test_gpu_monitors_off(lib):
     _, outs = run_monitored(lib, "cleo_b200", w, 2, mask=0)
     for f, _ in abi.MONITOR_FIELDS:
         assert not np.any(outs[-1][f])
+
+
+@pytest.mark.parametrize("mode", [abi.EXEC_PLAIN, abi.EXEC_BATCHED], ids=["plain", "batched"])
+def test_gpu_domain_from_files(lib, mode, monkeypatch):
+    """The GPU path set up and driven from CLEO's binary files matches the oracle."""
+    import test_binaryio as TB
+    from cleo_b200 import config
+    orig = config.make_params
+
+    def with_mode(**kw):
+        p = orig(**kw)
+        p.exec_mode = mode
+        return p
+
+    monkeypatch.setattr(TB, "make_params", with_mode)
+    g = TB.run_from_files(lib, "cleo_b200")
+    o = TB.run_from_files(K.oracle_lib(), "oc")
+    K.assert_same_domain(g.download_supers(), o.download_supers(), rtol=1e-12, what="files")
+    mg, mo = g.download_monitors(), o.download_monitors()
+    for f, dt in abi.MONITOR_FIELDS:
+        close_monitor(mg[f], mo[f], dt, ("files", f))
