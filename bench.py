@@ -40,6 +40,17 @@ NDIMS = (64, 128, 128)
 WORKLOAD = ("uneven3d: 64x128x128 gridboxes of 50 m^3, lognormal counts (median 32, sigma 0.586, "
             "clip 0..2048), ~40M superdroplets; condensation + Long CoalBuRe(ConstNFrags 5, "
             "Straub) + sedimentation (RogersGK), 1 s steps")
+# the largest configuration: the coupled bubble shape on one GPU
+BUBBLE_NDIMS = (128, 256, 256)
+BUBBLE = ("bubble3d: 128x256x256 gridboxes of 25 m^3, lognormal counts (median 16, sigma 0.9005, "
+          "mean 24), ~200M superdroplets; prescribed divergence-free 2-D flow (w_max 2 m/s) + "
+          "sedimentation, condensation, Long CoalBuRe(ConstNFrags 5, Straub), 1 s steps")
+
+
+def make_workload(kind, ndims, seed):
+    if kind == "bubble3d":
+        return W.bubble3d(ndims=ndims, seed=seed)
+    return W.uneven3d(ndims=ndims, seed=seed)
 # Algorithmic bytes per launch of the batched kernel groups (each field read once, written once):
 # condensation: per superdroplet read r, msol, xi, sdgbxindex (28 B), write r, dm, its (20 B);
 #   per gridbox read temp, press, qvap, write th_s, th_ff (40 B)
@@ -121,9 +132,9 @@ def reference_lib():
     return K.oracle_lib(), "oc", "port", 1
 
 
-def cpu_sample(steps, warmup, lib, prefix):
+def cpu_sample(steps, warmup, lib, prefix, kind="uneven3d"):
     """SD-steps/s of a CPU implementation on a sub-grid of the workload (same per-box physics)."""
-    w = W.uneven3d(ndims=(64, 16, 16), seed=3)
+    w = make_workload(kind, (64, 16, 16), 3)
     s = make_sdm(w, lib=lib, prefix=prefix)
     t = 0
     for _ in range(warmup):
@@ -145,14 +156,15 @@ def run_reference(args):
     lib, prefix, kind, cores = reference_lib()
     steps = max(1, min(args.steps, 3))
     warm = 1
-    value, nsd, dt = cpu_sample(steps, warm, lib, prefix)
+    value, nsd, dt = cpu_sample(steps, warm, lib, prefix, args.workload)
     sample = (f"64x16x16 gridboxes of the workload ({nsd} superdroplets), {steps} steps after "
               f"{warm} warm-up, {cores} host threads")
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
            "n_gpus": args.gpus, "steps": steps, "warmup": warm,
            "ms_per_step": 1000.0 * dt / steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "sample": sample},
+           "config": {"workload": BUBBLE if args.workload == "bubble3d" else WORKLOAD,
+                      "sample": sample},
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                             "sample": sample},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -406,7 +418,8 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     lib = abi.load_library()
     ndims = tuple(int(x) for x in args.ndims.split(","))
-    wl = W.uneven3d(ndims=ndims, seed=replicas.domain_seed(3, rank))  # one domain per rank
+    # one domain per rank
+    wl = make_workload(args.workload, ndims, replicas.domain_seed(3, rank))
     plain_steps = max(2, min(args.steps, 5))
     plain = measure(lib, wl, abi.EXEC_PLAIN, plain_steps, args.warmup, dist, local)
     bat = measure(lib, wl, abi.EXEC_BATCHED, args.steps, args.warmup, dist, local, e2e=True,
@@ -440,19 +453,20 @@ def run_ours(args):
             matched = measure_matched(lib, wl, sur, args.steps, args.warmup, local)
             sur.close()
         lc, lprefix, lref, lcores = reference_lib()
-        cpu_value, cpu_nsd, cpu_dt = cpu_sample(1, 1, lc, lprefix)
+        cpu_value, cpu_nsd, cpu_dt = cpu_sample(1, 1, lc, lprefix, args.workload)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "ndims": list(ndims), "ngbxs_per_gpu": ngbxs,
+            "config": {"workload": BUBBLE if args.workload == "bubble3d" else WORKLOAD,
+                       "ndims": list(ndims), "ngbxs_per_gpu": ngbxs,
                        "superdroplets_per_gpu": nsd,
                        "path": "batched (flat two-pass condensation, bucketed persistent "
                                "collisions), one CUDA graph per step, autotuned launch shapes",
                        "autotuned": bat["tuned"], "graphs": True,
                        "newton_seed": "reference guess (the reference's tolerances: maxniters "
                                       "50, atol 0.01)",
-                       "l2": "inputs larger than L2 (2.4 GB SoA per GPU), no flush"},
+                       "l2": "inputs larger than L2 (SoA of 60 B per superdroplet), no flush"},
             "plain_gpu": {"value": value_plain, "unit": UNIT, "ms_per_step": ms_plain / plain_steps,
                           "steps": plain_steps, "path": "one CTA per gridbox",
                           "stages_ms_per_step": plain["stage_ms"]},
@@ -485,10 +499,16 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ndims", default=",".join(str(n) for n in NDIMS))
+    ap.add_argument("--workload", default="uneven3d", choices=["uneven3d", "bubble3d"],
+                    help="uneven3d: the 3-D uneven-count configuration (default); bubble3d: "
+                         "the ~200M-superdroplet coupled bubble shape")
+    ap.add_argument("--ndims", default=None)
     ap.add_argument("--no-surrogate", dest="surrogate", action="store_false",
                     help="skip the surrogate training / seeded-solve section")
     args = ap.parse_args()
+    if args.ndims is None:
+        args.ndims = ",".join(str(n) for n in (BUBBLE_NDIMS if args.workload == "bubble3d"
+                                                else NDIMS))
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

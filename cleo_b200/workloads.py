@@ -61,9 +61,10 @@ def equilibrium_radius(rdry, msol, s_ratio, temp, iters=44):
     lo = np.maximum(rdry * (1.0 + 1e-9), 1e-12)
     hi = np.maximum(rcrit, lo)
     if lo.size > 1_000_000:
-        try:  # same IEEE element-wise arithmetic, spread over the host cores
+        try:  # same IEEE element-wise arithmetic, on the GPU when there is one, else host cores
             import torch
-            T = {k: torch.from_numpy(np.array(v, dtype=np.float64, copy=True))
+            dev = "cuda" if torch.cuda.is_available() else "cpu"
+            T = {k: torch.from_numpy(np.array(v, dtype=np.float64, copy=True)).to(dev)
                  for k, v in (("a", a), ("b", np.broadcast_to(b, lo.shape)), ("sm1", sm1),
                               ("lo", lo), ("hi", hi))}
             lo_t, hi_t = T["lo"].clone(), T["hi"].clone()
@@ -73,7 +74,7 @@ def equilibrium_radius(rdry, msol, s_ratio, temp, iters=44):
                 up = f > 0.0
                 lo_t = torch.where(up, mid, lo_t)
                 hi_t = torch.where(up, hi_t, mid)
-            return np.maximum(((lo_t + hi_t) * 0.5).numpy(), rdry)
+            return np.maximum(((lo_t + hi_t) * 0.5).cpu().numpy(), rdry)
         except ImportError:
             pass
     mid = np.empty_like(lo)
