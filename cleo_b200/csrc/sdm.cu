@@ -71,6 +71,10 @@ struct DevCtx {
   unsigned long long* prev0[2];
   float *prev1[2], *prev2[2];
   double *precip, *precip_c, *gbxarea;  // per gridbox, per superdroplet, per gridbox
+  // incremental re-sort after motion: mover flags then their exclusive scan (capacity + 1),
+  // per gridbox the valid superdroplets that leave, the arrivals and the arrivals from lower
+  // positions, the stayers, and the new gridbox starts (ngbxs + 2)
+  uint32_t *mv_scan, *mv_leave, *mv_arrive, *mv_below, *mv_stay, *gstart_new, *mv_mstart;
   // scratch
   double *scr_r, *scr_m, *scr_c3, *scr_c1, *scr_c2;
   unsigned long long *scr_x, *scr_id;
@@ -104,6 +108,7 @@ struct cleo_b200_ctx {
   int device = 0;
   // sort scratch
   uint32_t *keys[2], *vals[2], *hist, *tile_sums;
+  uint32_t *mv_tsums = nullptr, *mv_count = nullptr;  // incremental re-sort scratch
   uint32_t ntiles_max, key_bits;
   BatchScratch bs{};              // batched-schedule scratch
   int grid_small = 0, grid_small3 = 0, grid_medium = 0, grid_large = 0, grid_flat = 0;
@@ -245,15 +250,16 @@ __device__ __forceinline__ bool beyond_domainboundary(uint32_t gbxindex, uint32_
 // (predcorrmotion.hpp:85-106) with get_no_decomposition_bounding_gridbox (cartesianmaps.cpp:278)
 // and CartesianCheckBounds. Writes the sort key min(gbx, ngbxs) and the position.
 __global__ void __launch_bounds__(256, 3)
-k_motion(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+k_motion(DevCtx c, uint32_t* __restrict__ keys) {
   const uint32_t n = c.counters[0];
   const uint32_t ng = c.ngbxs;
   const double delt = c.p.motion_delt;
+  if (blockIdx.x == 0 && threadIdx.x == 0) c.mv_scan[n] = 0;  // the scan's total lands here
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t g = c.sd.gbx[i];
-    vals[i] = i;
     if (g >= ng) {  // null superdroplet left by collisions: out of the domain
       keys[i] = ng;
+      c.mv_scan[i] = 1;  // a mover, but not one of its range's gcount valid superdroplets
       continue;
     }
     const Where w{c.err, g, i};
@@ -365,8 +371,93 @@ k_motion(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
       bad |= (n2 < l) | (n2 >= h);
       if (bad) w.fail(CLEO_ERR_OUT_OF_BOX);
     }
-    keys[i] = idx < ng ? idx : ng;
+    const uint32_t key = idx < ng ? idx : ng;
+    keys[i] = key;
+    // a superdroplet that changes gridbox (or leaves the domain) moves in the re-sort
+    const bool mover = key != g;
+    c.mv_scan[i] = mover ? 1u : 0u;
+    if (mover) {
+      atomicAdd(&c.mv_leave[g], 1u);
+      if (key < ng) {
+        atomicAdd(&c.mv_arrive[key], 1u);
+        if (i < c.gstart[key]) atomicAdd(&c.mv_below[key], 1u);
+      }
+    }
   }
+}
+
+// ---- incremental re-sort (stable by gridbox, equal to the full radix sort) ----
+// Before motion, gridbox g's superdroplets occupy [gstart[g], gstart[g + 1]): its gcount[g] valid
+// ones first, then the nulls its collisions left. In a stable sort by the new keys, gridbox k
+// receives, in order: the movers into k from positions before its range, its stayers (valid,
+// key unchanged: gcount[k] less the valid ones that left), the movers into k from positions
+// after it; out-of-domain ones and nulls follow all gridboxes in position order. Only the
+// movers are sorted.
+__global__ void k_mv_list(DevCtx c, const uint32_t* __restrict__ keys, uint32_t* __restrict__ mk,
+                          uint32_t* __restrict__ mvp) {
+  const uint32_t n = c.counters[0];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t p = c.mv_scan[i];
+    if (c.mv_scan[i + 1] != p) {  // a mover: the exclusive scan steps over it
+      mk[p] = keys[i];
+      mvp[p] = i;
+    }
+  }
+}
+__global__ void k_mv_counts(DevCtx c) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x) {
+    const uint32_t stay = c.gcount[g] - c.mv_leave[g];
+    c.mv_stay[g] = stay;
+    c.gstart_new[g] = stay + c.mv_arrive[g];  // scanned in place to the new starts
+  }
+}
+__global__ void k_mv_ends(DevCtx c) {  // after the scan: gstart_new[ngbxs] = in-domain count
+  c.gstart_new[c.ngbxs + 1] = c.counters[0];
+}
+__global__ void k_mv_count(DevCtx c, uint32_t* __restrict__ count) {  // number of movers
+  *count = c.mv_scan[c.counters[0]];
+}
+__global__ void k_mv_arrivals(DevCtx c) {  // to be scanned: first sorted mover of each key
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x)
+    c.mv_mstart[g] = c.mv_arrive[g];
+}
+__device__ __forceinline__ void mv_copy(const Fields& s, const Fields& d, uint32_t i, uint32_t o) {
+  d.gbx[o] = s.gbx[i];
+  d.c3[o] = s.c3[i];
+  d.c1[o] = s.c1[i];
+  d.c2[o] = s.c2[i];
+  d.xi[o] = s.xi[i];
+  d.r[o] = s.r[i];
+  d.msol[o] = s.msol[i];
+  d.id[o] = s.id[i];
+}
+__global__ void k_mv_stayers(DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ keys) {
+  const uint32_t n = c.counters[0];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t m = c.mv_scan[i];
+    if (c.mv_scan[i + 1] != m) continue;
+    const uint32_t g = keys[i];
+    const uint32_t g0 = c.gstart[g];
+    const uint32_t o = c.gstart_new[g] + c.mv_below[g] + (i - g0) - (m - c.mv_scan[g0]);
+    mv_copy(src, dst, i, o);
+  }
+}
+__global__ void k_mv_movers(DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ mk,
+                            const uint32_t* __restrict__ mvp) {
+  const uint32_t n = c.counters[0];
+  const uint32_t nm = c.mv_scan[n];
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nm; j += gridDim.x * blockDim.x) {
+    const uint32_t k = mk[j];
+    const uint32_t r = j - c.mv_mstart[k];  // rank among the sorted movers of key k
+    const uint32_t o = k < c.ngbxs
+                           ? c.gstart_new[k] + (r < c.mv_below[k] ? r : c.mv_stay[k] + r)
+                           : c.gstart_new[c.ngbxs] + r;
+    mv_copy(src, dst, mvp[j], o);
+  }
+}
+__global__ void k_mv_commit(DevCtx c) {  // the new gridbox starts become the refs
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < c.ngbxs + 2; k += gridDim.x * blockDim.x)
+    c.gstart[k] = c.gstart_new[k];
 }
 
 // sort keys of freshly uploaded droplets
@@ -935,6 +1026,62 @@ int sort_current(cleo_b200_ctx* x) {
   return CLEO_OK;
 }
 
+int radix_pairs_on(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1,
+                   const uint32_t* n_ptr, uint32_t bits, uint32_t* hist, uint32_t* tile_sums,
+                   uint32_t nt);
+
+// the re-sort after motion, incremental (k_motion flagged the movers and counted them per
+// gridbox): scan of the flags, list of the movers in position order, stable radix sort of the
+// movers by key, the new gridbox starts, then every superdroplet copied once to its place
+int sort_incremental(cleo_b200_ctx* x) {
+  DevCtx& d = x->d;
+  cudaStream_t s = x->stream;
+  const uint32_t ng = d.ngbxs;
+  const uint64_t n1 = (uint64_t)d.capacity + 1;
+  const uint32_t nscan = (uint32_t)((n1 + SCAN_TILE - 1) / SCAN_TILE);
+  // exclusive scan of capacity + 1 flags (entries past nrange are stale but only move the
+  // values after index nrange, which nothing reads)
+  k_scan_tiles<<<nscan, SCAN_THREADS, 0, s>>>(d.mv_scan, d.mv_scan, n1, x->mv_tsums);
+  k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(x->mv_tsums, nscan, nullptr);
+  k_scan_add<<<(unsigned)((n1 + 255) / 256), 256, 0, s>>>(d.mv_scan, n1, x->mv_tsums);
+  x->launches += 3;
+  const int gc = grid_for(d.capacity, 256), gg = grid_for((size_t)ng + 2, 256);
+  k_mv_list<<<gc, 256, 0, s>>>(d, x->keys[0], x->keys[1], x->vals[1]);
+  k_mv_count<<<1, 1, 0, s>>>(d, x->mv_count);
+  x->launches += 2;
+  // mover count = mv_scan[nrange]: read by the radix kernels through a device pointer
+  const int where = radix_pairs_on(x, x->keys[1], x->vals[1], d.scr_p, d.scr_j, x->mv_count,
+                                   x->key_bits, x->hist, x->tile_sums, x->ntiles_max);
+  uint32_t* mk = where == 0 ? x->keys[1] : d.scr_p;
+  uint32_t* mvp = where == 0 ? x->vals[1] : d.scr_j;
+  // new gridbox starts (exclusive scan of stayers + arrivals; the total is the in-domain count)
+  // and the first sorted mover of every key (exclusive scan of the arrivals)
+  k_mv_counts<<<gg, 256, 0, s>>>(d);
+  k_mv_arrivals<<<gg, 256, 0, s>>>(d);
+  const uint32_t ns2 = (uint32_t)(((uint64_t)ng + SCAN_TILE - 1) / SCAN_TILE);
+  for (uint32_t* arr : {d.gstart_new, d.mv_mstart}) {
+    k_scan_tiles<<<ns2 ? ns2 : 1, SCAN_THREADS, 0, s>>>(arr, arr, ng, x->mv_tsums);
+    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(x->mv_tsums, ns2 ? ns2 : 1, arr + ng);
+    k_scan_add<<<(unsigned)((ng + 255) / 256 + 1), 256, 0, s>>>(arr, ng, x->mv_tsums);
+  }
+  k_mv_ends<<<1, 1, 0, s>>>(d);
+  x->launches += 9;
+  Fields& src = x->buf[x->cur];
+  Fields& dst = x->buf[1 - x->cur];
+  k_mv_stayers<<<gc, 256, 0, s>>>(d, src, dst, x->keys[0]);
+  k_mv_movers<<<gc, 256, 0, s>>>(d, src, dst, mk, mvp);
+  k_mv_commit<<<gg, 256, 0, s>>>(d);
+  x->launches += 3;
+  x->cur = 1 - x->cur;
+  d.sd = x->buf[x->cur];
+  k_counts<<<grid_for(ng, 256), 256, 0, s>>>(d);
+  k_to_grave<<<gc, 256, 0, s>>>(d);
+  k_grave_commit<<<1, 1, 0, s>>>(d);
+  x->launches += 3;
+  CUDA_TRY(cudaGetLastError());
+  return CLEO_OK;
+}
+
 // stable radix sort of (key, value) pairs whose count is *n_ptr (device), over `bits` key bits,
 // from (k0, v0) using (k1, v1) as the other buffer; returns 0 if the result is in (k0, v0)
 // with explicit digit-table scratch for nt tiles (hist: 256 nt words, tile_sums: enough for the
@@ -1041,7 +1188,11 @@ int run_sdm_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
   if (did_motion) {
     {
       StageMark m(x, 0);
-      k_motion<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, x->keys[0], x->vals[0]);
+      const size_t ngb = (size_t)(d.ngbxs ? d.ngbxs : 1) * 4;
+      CUDA_TRY(cudaMemsetAsync(d.mv_leave, 0, ngb, s));
+      CUDA_TRY(cudaMemsetAsync(d.mv_arrive, 0, ngb, s));
+      CUDA_TRY(cudaMemsetAsync(d.mv_below, 0, ngb, s));
+      k_motion<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, x->keys[0]);
       x->launches += 1;
       if (d.p.monitors & CLEO_MONITOR_PRECIPITATION) {  // before the sort moves the droplets
         k_mon_precip<<<gg, 256, 0, s>>>(d);
@@ -1049,7 +1200,7 @@ int run_sdm_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
       }
     }
     StageMark m(x, 1);
-    const int rc = sort_current(x);
+    const int rc = sort_incremental(x);
     if (rc) return rc;
     if (mon_mm) {  // monitor_motion (movesupersindomain.hpp:297)
       k_mon_mm<<<gg, 256, 0, s>>>(d, 1, 0);
@@ -1276,6 +1427,18 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &x->bs.ctr, 8);
   rc |= dalloc(x, &x->bs.tsdm, 1);
   rc |= dalloc(x, &x->tile_sums, ((size_t)256 * x->ntiles_max + SCAN_TILE - 1) / SCAN_TILE + 1);
+  rc |= dalloc(x, &d.mv_scan, (size_t)cap + 1);
+  rc |= dalloc(x, &d.mv_leave, ng);
+  rc |= dalloc(x, &d.mv_arrive, ng);
+  rc |= dalloc(x, &d.mv_below, ng);
+  rc |= dalloc(x, &d.mv_stay, ng);
+  rc |= dalloc(x, &d.mv_mstart, (size_t)ng + 1);
+  rc |= dalloc(x, &d.gstart_new, (size_t)ng + 2);
+  rc |= dalloc(x, &x->mv_count, 1);
+  {
+    const size_t a = ((size_t)cap + 1 + SCAN_TILE - 1) / SCAN_TILE, b = ((size_t)ng + SCAN_TILE) / SCAN_TILE;
+    rc |= dalloc(x, &x->mv_tsums, (a > b ? a : b) + 1);
+  }
   if (params->monitors) {
     for (int r = 0; r < 2; ++r) {
       for (int w = 0; w < 2; ++w) {
