@@ -37,6 +37,8 @@ STATUS = {
     13: "CLEO_ERR_CUDA",
     14: "CLEO_ERR_TIMEOUT",
     15: "CLEO_ERR_MLP",
+    16: "CLEO_ERR_XI_OUTPUT",
+    17: "CLEO_ERR_IO",
 }
 CODE = {v: k for k, v in STATUS.items()}
 
@@ -50,6 +52,14 @@ EXEC_PLAIN, EXEC_BATCHED = 0, 1
 MLP_TCGEN05, MLP_MMA_SYNC, MLP_FP32 = 0, 1, 2
 MONITOR_MASSMOMENTS, MONITOR_RAINMASSMOMENTS, MONITOR_PRECIPITATION = 1, 2, 4
 MLP_NFEATURES, MLP_NHIDDEN, MLP_NPARAMS, MLP_NNORM = 7, 64, 4737, 16
+# enum cleo_obs_var: superdroplet output variables, with their output types
+OBS_VARS = {"sdId": (1, np.uint32), "sdgbxindex": (2, np.uint32), "xi": (4, np.uint64),
+            "radius": (8, np.float32), "msol": (16, np.float32), "coord3": (32, np.float32),
+            "coord1": (64, np.float32), "coord2": (128, np.float32)}
+OBS_ALL = 255
+# cleo_b200_obs_supers member of each output variable
+OBS_MEMBER = {"sdId": "sdid", "sdgbxindex": "sdgbxindex", "xi": "xi", "radius": "radius",
+              "msol": "msol", "coord3": "coord3", "coord1": "coord1", "coord2": "coord2"}
 
 _d = C.POINTER(C.c_double)
 _u32 = C.POINTER(C.c_uint32)
@@ -212,6 +222,23 @@ def monitors_struct(arrs: dict) -> Monitors:
     return m
 
 
+class ObsSupers(C.Structure):
+    """cleo_b200_obs_supers (host arrays of the output types; NULL members are skipped)."""
+
+    _fields_ = [("sdid", _u32), ("sdgbxindex", _u32), ("xi", _u64), ("radius", _f32),
+                ("msol", _f32), ("coord3", _f32), ("coord1", _f32), ("coord2", _f32)]
+
+
+def obs_struct(arrs: dict) -> ObsSupers:
+    """ObsSupers over arrays keyed by output variable name (absent names stay NULL)."""
+    o = ObsSupers()
+    ct = {np.uint32: C.c_uint32, np.uint64: C.c_uint64, np.float32: C.c_float}
+    for name, (_, dt) in OBS_VARS.items():
+        if name in arrs and arrs[name] is not None:
+            setattr(o, OBS_MEMBER[name], ptr(arrs[name], ct[dt]))
+    return o
+
+
 def declare_api(lib: C.CDLL, prefix: str) -> C.CDLL:
     """Declare argtypes/restype of the context API ``<prefix>_create`` ... on ``lib``."""
     for name, args in (("monitors_begin", [C.c_void_p]),
@@ -262,7 +289,10 @@ EXPORTED = (
     "cleo_b200_mlp_get_params", "cleo_b200_mlp_features", "cleo_b200_mlp_fit_normalisation",
     "cleo_b200_mlp_loss_grad", "cleo_b200_mlp_train", "cleo_b200_mlp_infer",
     "cleo_b200_set_surrogate", "cleo_b200_set_graphs", "cleo_b200_autotune",
-    "cleo_b200_tuned_config", "cleo_b200_monitors_begin", "cleo_b200_download_monitors",
+    "cleo_b200_tuned_config", "cleo_b200_set_launch_config", "cleo_b200_monitors_begin",
+    "cleo_b200_download_monitors",
+    "cleo_b200_gather_supers", "cleo_b200_zarr_open", "cleo_b200_zarr_observe",
+    "cleo_b200_zarr_observe_host", "cleo_b200_zarr_close",
 )
 
 _LIB = None
@@ -312,7 +342,14 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
             ("set_surrogate", [vp, vp]),
             ("set_graphs", [vp, C.c_int]),
             ("autotune", [vp, C.c_int]),
-            ("tuned_config", [vp, C.POINTER(C.c_int32)])):
+            ("tuned_config", [vp, C.POINTER(C.c_int32)]),
+            ("set_launch_config", [vp, C.POINTER(C.c_int32)]),
+            ("gather_supers", [vp, C.c_uint32, C.POINTER(ObsSupers), C.c_size_t,
+                               C.POINTER(C.c_size_t)]),
+            ("zarr_open", [C.c_char_p, C.c_size_t, C.c_uint32, C.c_uint32, C.POINTER(vp)]),
+            ("zarr_observe", [vp, vp, C.c_uint32]),
+            ("zarr_observe_host", [vp, C.c_uint32, C.POINTER(ObsSupers), C.c_size_t]),
+            ("zarr_close", [vp])):
         f = getattr(lib, "cleo_b200_" + name)
         f.argtypes = args
         f.restype = C.c_int

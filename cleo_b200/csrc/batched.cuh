@@ -9,9 +9,9 @@
 //   (radix sort of that list by cost, 16-bit keys)
 //   k_cond_b       thread per listed solve, neighbouring lanes of similar cost
 //   k_b_classify   gridboxes into size buckets (warp-aggregated atomics)
-//   k_b_small      persistent, warp per gridbox (n <= small_max <= 64): reduction of the condensed
-//                  mass and Newton iterations, state update, collisions in registers + per-warp
-//                  shared memory
+//   k_b_small      persistent, warp per gridbox (n <= small_max <= 128; 64- and 128-slot
+//                  variants): reduction of the condensed mass and Newton iterations, state
+//                  update, collisions in registers + per-warp shared memory
 //   k_b_cta<false> persistent, CTA per gridbox (small_max < n <= medium_max <= 1024): the same
 //                  with shared-memory staging
 //   k_b_cta<true>  CTA per gridbox (n > medium_max) with global scratch
@@ -267,16 +267,19 @@ __device__ __forceinline__ uint32_t fy_origin(const JT* J, uint32_t n, uint32_t 
 }
 
 // ---- small gridboxes: persistent, one warp per gridbox ----
-template <int MINB>
+// CAP (64 or 128) is the number of per-warp slots; every lane holds CAP / 32 of them.
+template <int MINB, int CAP>
 __global__ void __launch_bounds__(B_THREADS, MINB)
 k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
+  constexpr int H = CAP / 32;
+  static_assert(CAP % 32 == 0 && CAP <= 255, "slot indices are stored as bytes");
   const uint32_t t_sdm = *b.tsdm;
-  __shared__ double s_r[B_WARPS][SMALL_MAX];
-  __shared__ double s_m[B_WARPS][SMALL_MAX];
-  __shared__ unsigned long long s_x[B_WARPS][SMALL_MAX];
-  __shared__ double s_tv[B_WARPS][SMALL_MAX];
-  __shared__ uint8_t s_p[B_WARPS][SMALL_MAX];
-  __shared__ uint8_t s_j[B_WARPS][SMALL_MAX];
+  __shared__ double s_r[B_WARPS][CAP];
+  __shared__ double s_m[B_WARPS][CAP];
+  __shared__ unsigned long long s_x[B_WARPS][CAP];
+  __shared__ double s_tv[B_WARPS][CAP];
+  __shared__ uint8_t s_p[B_WARPS][CAP];
+  __shared__ uint8_t s_j[B_WARPS][CAP];
   const cleo_b200_params& p = c.p;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const uint32_t count = b.ctr[1];
@@ -305,7 +308,7 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
     if (!coll) continue;
     const uint64_t key = cleo_rng_key(p.seed, t_sdm, g);
     const uint64_t slot = b.slot[g];
-    // stage this gridbox: lane holds k = lane and k = lane + 32
+    // stage this gridbox: lane holds k = lane + 32 h
     for (uint32_t k = lane; k < n; k += 32) {
       const double rk = c.sd.r[base + k];
       s_r[wib][k] = rk;
@@ -316,21 +319,32 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
         s_j[wib][k] = (uint8_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - k)), 0, (uint64_t)k + 1);
     }
     __syncwarp();
-    for (uint32_t k = lane; k < n; k += 32) s_p[wib][k] = (uint8_t)fy_origin(s_j[wib], n, k);
+    {  // origins of the lane's positions, traced together through the swaps (fy_origin)
+      uint32_t pos[H];
+#pragma unroll
+      for (int h = 0; h < H; ++h) pos[h] = lane + 32 * h;
+      for (uint32_t s = 1; s < n; ++s) {
+        const uint32_t j = s_j[wib][s];
+#pragma unroll
+        for (int h = 0; h < H; ++h) pos[h] = (pos[h] == s) ? j : ((pos[h] == j) ? s : pos[h]);
+      }
+#pragma unroll
+      for (int h = 0; h < H; ++h)
+        if (lane + 32 * h < n) s_p[wib][lane + 32 * h] = (uint8_t)pos[h];
+    }
     __syncwarp();
     const uint64_t slot_pairs = slot + (n >= 1 ? n - 1 : 0);
     const uint32_t npairs = n / 2;
     const double scale_p = (double)n * ((double)n - 1.0) / (2.0 * (double)npairs);
     const double VOLUME = c.volume[g] * VOL0;
     uint32_t nnull = 0;
-    if ((uint32_t)lane < npairs) {
-      const uint32_t jj = lane;
+    for (uint32_t jj = lane; jj < npairs; jj += 32) {
       const uint32_t a = s_p[wib][2 * jj], bb = s_p[wib][2 * jj + 1];
       const Where w{c.err, g, (uint64_t)base + 2 * jj};
       Drop dA{s_x[wib][a], s_r[wib][a], s_m[wib][a]};
       Drop dB{s_x[wib][bb], s_r[wib][bb], s_m[wib][bb]};
-      nnull = collide_pair(p, dA, dB, s_tv[wib][a], s_tv[wib][bb], scale_p, VOLUME, key,
-                           slot_pairs, jj, w);
+      nnull += collide_pair(p, dA, dB, s_tv[wib][a], s_tv[wib][bb], scale_p, VOLUME, key,
+                            slot_pairs, jj, w);
       s_x[wib][a] = dA.xi; s_r[wib][a] = dA.r; s_m[wib][a] = dA.msol;
       s_x[wib][bb] = dB.xi; s_r[wib][bb] = dB.r; s_m[wib][bb] = dB.msol;
     }
@@ -338,12 +352,13 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
     const uint32_t totnull = warp_sum_u(nnull);
     const uint32_t nvalid = n - totnull;
     // destinations: valid superdroplets in shuffled order, then the nulls (collisions.hpp:240-248)
-    uint32_t src[2], q[2];
-    double c3v[2], c1v[2], c2v[2];
-    unsigned long long idv[2];
+    uint32_t src[H], q[H];
+    double c3v[H], c1v[H], c2v[H];
+    unsigned long long idv[H];
     uint32_t cval = 0, cnull = 0;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < H; ++h) {
+      if (32u * h >= n) break;  // uniform across the warp
       const uint32_t k = lane + 32 * h;
       const bool act = k < n;
       src[h] = act ? s_p[wib][k] : 0;
@@ -364,7 +379,7 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
     }
     __syncwarp();
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < H; ++h) {
       const uint32_t k = lane + 32 * h;
       if (k < n) {
         const uint32_t o = base + q[h];

@@ -5,7 +5,8 @@
 
 namespace {
 
-constexpr uint32_t SMALL_MAX = 64;
+constexpr uint32_t SMALL_MAX = 64;   // default limit of the warp kernel
+constexpr uint32_t WARP_MAX = 128;   // largest gridbox the warp kernel's 128-slot variant holds
 constexpr uint32_t MEDIUM_MAX = 1024;
 constexpr uint32_t MEDIUM_SMEM = 40 * MEDIUM_MAX;  // r, msol, xi, P, J, Simmel velocity
 constexpr uint32_t FY_PARALLEL_MAX = 256;  // gridboxes up to this size shuffle in parallel
@@ -23,7 +24,7 @@ struct BatchScratch {
   uint32_t* slot;    // per gridbox RNG slot offset within the SDM step
   uint32_t* ctr;     // [0] deferred solves, [1..3] bucket counts, [4..6] bucket heads
   uint32_t* tsdm;    // the SDM step's start time (keys the injected random numbers)
-  uint32_t small_max;   // gridboxes with 1..small_max superdroplets: warp kernel (<= SMALL_MAX)
+  uint32_t small_max;   // gridboxes with 1..small_max superdroplets: warp kernel (<= WARP_MAX)
   uint32_t medium_max;  // small_max..medium_max: CTA kernel in shared memory (<= MEDIUM_MAX)
 };
 

@@ -74,7 +74,8 @@ struct DevCtx {
   // incremental re-sort after motion: mover flags then their exclusive scan (capacity + 1),
   // per gridbox the valid superdroplets that leave, the arrivals and the arrivals from lower
   // positions, the stayers, and the new gridbox starts (ngbxs + 2)
-  uint32_t *mv_scan, *mv_leave, *mv_arrive, *mv_below, *mv_stay, *gstart_new, *mv_mstart;
+  uint32_t *mv_scan, *mv_leave, *mv_arrive, *mv_below, *mv_stay, *gstart_new, *mv_mstart,
+      *mv_shift;
   // scratch
   double *scr_r, *scr_m, *scr_c3, *scr_c1, *scr_c2;
   unsigned long long *scr_x, *scr_id;
@@ -109,9 +110,13 @@ struct cleo_b200_ctx {
   // sort scratch
   uint32_t *keys[2], *vals[2], *hist, *tile_sums;
   uint32_t *mv_tsums = nullptr, *mv_count = nullptr;  // incremental re-sort scratch
+  // superdroplet output staging (allocated at the first gather): converted fields, offsets
+  uint8_t* obs_stage = nullptr;
+  uint32_t *obs_start = nullptr, *obs_tsums = nullptr;
   uint32_t ntiles_max, key_bits;
   BatchScratch bs{};              // batched-schedule scratch
-  int grid_small = 0, grid_small3 = 0, grid_medium = 0, grid_large = 0, grid_flat = 0;
+  int grid_small[2][2] = {{0, 0}, {0, 0}};  // warp kernel [64 / 128 slots][2 / 3 CTAs per SM]
+  int grid_medium = 0, grid_large = 0, grid_flat = 0;
   unsigned long long launches = 0;  // kernels launched by this context
   std::vector<void*> allocs;
   // stage timing: (stage, start, end) event triples recorded while profiling is on
@@ -431,15 +436,61 @@ __device__ __forceinline__ void mv_copy(const Fields& s, const Fields& d, uint32
   d.msol[o] = s.msol[i];
   d.id[o] = s.id[i];
 }
-__global__ void k_mv_stayers(DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ keys) {
+// a stayer of gridbox g at position i goes to i - (movers before i) + shift[g]:
+// shift[g] = gstart_new[g] + mv_below[g] - gstart[g] + (movers before gstart[g]); computed per
+// gridbox together with the commit of the new gridbox starts (which nothing after this reads
+// in their old form)
+__global__ void k_mv_shift_commit(DevCtx c) {
+  const uint32_t ng = c.ngbxs;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ng + 2; k += gridDim.x * blockDim.x) {
+    if (k < ng) {
+      const uint32_t g0 = c.gstart[k];
+      c.mv_shift[k] = c.gstart_new[k] + c.mv_below[k] - g0 + c.mv_scan[g0];
+    }
+    c.gstart[k] = c.gstart_new[k];
+  }
+}
+__global__ void __launch_bounds__(256)
+k_mv_stayers(DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ keys) {
+  constexpr int U = 2;  // superdroplets per thread and iteration, all loads issued first
   const uint32_t n = c.counters[0];
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t m = c.mv_scan[i];
-    if (c.mv_scan[i + 1] != m) continue;
-    const uint32_t g = keys[i];
-    const uint32_t g0 = c.gstart[g];
-    const uint32_t o = c.gstart_new[g] + c.mv_below[g] + (i - g0) - (m - c.mv_scan[g0]);
-    mv_copy(src, dst, i, o);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += U * stride) {
+    uint32_t m[U], m1[U], g[U], gb[U];
+    double c3[U], c1[U], c2[U], r[U], ms[U];
+    unsigned long long xi[U], id[U];
+    bool ok[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint32_t i = i0 + u * stride;
+      ok[u] = i < n;
+      if (ok[u]) {
+        m[u] = c.mv_scan[i];
+        m1[u] = c.mv_scan[i + 1];
+        g[u] = keys[i];
+        gb[u] = src.gbx[i];
+        c3[u] = src.c3[i];
+        c1[u] = src.c1[i];
+        c2[u] = src.c2[i];
+        xi[u] = src.xi[i];
+        r[u] = src.r[i];
+        ms[u] = src.msol[i];
+        id[u] = src.id[i];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!ok[u] || m1[u] != m[u]) continue;  // beyond the range, or a mover
+      const uint32_t o = i0 + u * stride - m[u] + c.mv_shift[g[u]];
+      dst.gbx[o] = gb[u];
+      dst.c3[o] = c3[u];
+      dst.c1[o] = c1[u];
+      dst.c2[o] = c2[u];
+      dst.xi[o] = xi[u];
+      dst.r[o] = r[u];
+      dst.msol[o] = ms[u];
+      dst.id[o] = id[u];
+    }
   }
 }
 __global__ void k_mv_movers(DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ mk,
@@ -455,9 +506,41 @@ __global__ void k_mv_movers(DevCtx c, Fields src, Fields dst, const uint32_t* __
     mv_copy(src, dst, mvp[j], o);
   }
 }
-__global__ void k_mv_commit(DevCtx c) {  // the new gridbox starts become the refs
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < c.ngbxs + 2; k += gridDim.x * blockDim.x)
-    c.gstart[k] = c.gstart_new[k];
+
+// ---- superdroplet output: the domain superdroplets, gathered in gridbox order and converted
+// the way the reference's Collect* functors convert them (superdrops_observer.hpp:139-464) ----
+struct ObsOut {
+  uint32_t* sdid;
+  uint32_t* gbx;
+  uint64_t* xi;
+  float *r, *msol, *c3, *c1, *c2;
+};
+__global__ void k_obs_counts(DevCtx c, uint32_t* __restrict__ start) {  // scanned to out offsets
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x)
+    start[g] = c.gcount[g];
+}
+__global__ void __launch_bounds__(256)
+k_obs_gather(DevCtx c, ObsOut o, const uint32_t* __restrict__ start) {
+  const uint32_t n = c.counters[0];
+  const uint32_t ng = c.ngbxs;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t g = c.sd.gbx[i];
+    if (g >= ng) continue;  // a null superdroplet: not in the domain
+    // valid superdroplets lead their gridbox's range [gstart[g], gstart[g] + gcount[g])
+    const uint32_t k = start[g] + (i - c.gstart[g]);
+    if (o.sdid) o.sdid[k] = (uint32_t)c.sd.id[i];
+    if (o.gbx) o.gbx[k] = g;
+    if (o.xi) {
+      const uint64_t xi = c.sd.xi[i];
+      if (xi == ~0ull) Where{c.err, g, i}.fail(CLEO_ERR_XI_OUTPUT);
+      o.xi[k] = xi;
+    }
+    if (o.r) o.r[k] = (float)c.sd.r[i];
+    if (o.msol) o.msol[k] = (float)c.sd.msol[i];
+    if (o.c3) o.c3[k] = (float)c.sd.c3[i];
+    if (o.c1) o.c1[k] = (float)c.sd.c1[i];
+    if (o.c2) o.c2[k] = (float)c.sd.c2[i];
+  }
 }
 
 // sort keys of freshly uploaded droplets
@@ -1068,9 +1151,9 @@ int sort_incremental(cleo_b200_ctx* x) {
   x->launches += 9;
   Fields& src = x->buf[x->cur];
   Fields& dst = x->buf[1 - x->cur];
+  k_mv_shift_commit<<<gg, 256, 0, s>>>(d);
   k_mv_stayers<<<gc, 256, 0, s>>>(d, src, dst, x->keys[0]);
   k_mv_movers<<<gc, 256, 0, s>>>(d, src, dst, mk, mvp);
-  k_mv_commit<<<gg, 256, 0, s>>>(d);
   x->launches += 3;
   x->cur = 1 - x->cur;
   d.sd = x->buf[x->cur];
@@ -1161,10 +1244,16 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       StageMark mk(x, 4);
       k_b_reset<<<1, 32, 0, s>>>(d, b, 0);
       k_b_classify<<<gg, 256, 0, s>>>(d, b);
-      if (x->cfg.small_minb == 3)
-        k_b_small<3><<<x->grid_small3, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
+      const int wide = x->cfg.small_max > SMALL_MAX ? 1 : 0, m3 = x->cfg.small_minb == 3 ? 1 : 0;
+      const int gs = x->grid_small[wide][m3], ci = cond ? 1 : 0, li = coll ? 1 : 0;
+      if (wide && m3)
+        k_b_small<3, WARP_MAX><<<gs, B_THREADS, 0, s>>>(d, b, ci, li);
+      else if (wide)
+        k_b_small<2, WARP_MAX><<<gs, B_THREADS, 0, s>>>(d, b, ci, li);
+      else if (m3)
+        k_b_small<3, SMALL_MAX><<<gs, B_THREADS, 0, s>>>(d, b, ci, li);
       else
-        k_b_small<2><<<x->grid_small, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
+        k_b_small<2, SMALL_MAX><<<gs, B_THREADS, 0, s>>>(d, b, ci, li);
       k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_SMEM, s>>>(d, b, cond ? 1 : 0,
                                                                            coll ? 1 : 0);
       k_b_cta<true><<<x->grid_large, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
@@ -1243,7 +1332,7 @@ std::map<std::string, cleo_b200_ctx::TuneCfg> g_tune_cache;
 const cleo_b200_ctx::TuneCfg COND_OPTS[4] = {
     {128, 3, 0, 0}, {256, 3, 0, 0}, {128, 4, 0, 0}, {256, 4, 0, 0}};
 const cleo_b200_ctx::TuneCfg COLL_OPTS[4] = {
-    {0, 0, 32, 2}, {0, 0, SMALL_MAX, 2}, {0, 0, 32, 3}, {0, 0, SMALL_MAX, 3}};
+    {0, 0, SMALL_MAX, 2}, {0, 0, WARP_MAX, 2}, {0, 0, SMALL_MAX, 3}, {0, 0, WARP_MAX, 3}};
 
 std::string tune_key(const cleo_b200_ctx* x) {
   cudaDeviceProp prop;
@@ -1433,6 +1522,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &d.mv_below, ng);
   rc |= dalloc(x, &d.mv_stay, ng);
   rc |= dalloc(x, &d.mv_mstart, (size_t)ng + 1);
+  rc |= dalloc(x, &d.mv_shift, ng);
   rc |= dalloc(x, &d.gstart_new, (size_t)ng + 2);
   rc |= dalloc(x, &x->mv_count, 1);
   {
@@ -1508,10 +1598,18 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
     int dev = 0, sms = 148, occ = 1;
     CUDA_TRY(cudaGetDevice(&dev));
     CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<2>, B_THREADS, 0));
-    x->grid_small = sms * (occ > 0 ? occ : 1);
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<3>, B_THREADS, 0));
-    x->grid_small3 = sms * (occ > 0 ? occ : 1);
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<2, SMALL_MAX>,
+                                                           B_THREADS, 0));
+    x->grid_small[0][0] = sms * (occ > 0 ? occ : 1);
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<3, SMALL_MAX>,
+                                                           B_THREADS, 0));
+    x->grid_small[0][1] = sms * (occ > 0 ? occ : 1);
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<2, WARP_MAX>,
+                                                           B_THREADS, 0));
+    x->grid_small[1][0] = sms * (occ > 0 ? occ : 1);
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<3, WARP_MAX>,
+                                                           B_THREADS, 0));
+    x->grid_small[1][1] = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<false>, B_THREADS,
                                                            (size_t)MEDIUM_SMEM));
     x->grid_medium = sms * (occ > 0 ? occ : 1);
@@ -1677,6 +1775,19 @@ int cleo_b200_tuned_config(cleo_b200_ctx* x, int32_t cfg[4]) {
   return x->tune_step < x->tune_total ? 1 : CLEO_OK;
 }
 
+int cleo_b200_set_launch_config(cleo_b200_ctx* x, const int32_t cfg[4]) {
+  if (!x || !cfg) return CLEO_ERR_ARGUMENT;
+  if ((cfg[0] != 128 && cfg[0] != 256) || (cfg[1] != 3 && cfg[1] != 4) || cfg[2] < 1 ||
+      cfg[2] > (int32_t)WARP_MAX || (cfg[3] != 2 && cfg[3] != 3))
+    return CLEO_ERR_ARGUMENT;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  x->cfg = {cfg[0], cfg[1], (uint32_t)cfg[2], cfg[3]};
+  x->tune_total = 0;  // ends a tuning run in progress
+  x->tune_step = 0;
+  x->drop_graphs();
+  return CLEO_OK;
+}
+
 int cleo_b200_set_graphs(cleo_b200_ctx* x, int on) {
   if (!x) return CLEO_ERR_ARGUMENT;
   CUDA_TRY(cudaStreamSynchronize(x->stream));
@@ -1707,6 +1818,65 @@ int cleo_b200_domain_nsupers(cleo_b200_ctx* x, size_t* n) {
   for (uint32_t g = 0; g < x->d.ngbxs; ++g) s += cnt[g];
   *n = s;
   return CLEO_OK;
+}
+
+int cleo_b200_gather_supers(cleo_b200_ctx* x, uint32_t vars, const cleo_b200_obs_supers* out,
+                            size_t cap, size_t* n) {
+  if (!x || !out || !n || (vars & ~(uint32_t)CLEO_OBS_ALL)) return CLEO_ERR_ARGUMENT;
+  DevCtx& d = x->d;
+  cudaStream_t s = x->stream;
+  const size_t C = d.capacity ? d.capacity : 1;
+  const uint32_t ng = d.ngbxs;
+  if (!x->obs_stage) {  // 36 bytes per superdroplet of the capacity + field alignment, once
+    if (dalloc(x, &x->obs_stage, C * 36 + 8 * 16) || dalloc(x, &x->obs_start, (size_t)ng + 1) ||
+        dalloc(x, &x->obs_tsums, ((size_t)ng + SCAN_TILE) / SCAN_TILE + 1))
+      return CLEO_ERR_CUDA;
+  }
+  // field offsets in the staging area: 8-byte fields first, all 16-byte aligned
+  uint8_t* st = x->obs_stage;
+  ObsOut o{};
+  const auto want = [&](uint32_t bit) { return (vars & bit) != 0; };
+  const size_t a4 = (C * 4 + 15) / 16 * 16, a8 = (C * 8 + 15) / 16 * 16;
+  size_t off = 0;
+  if (want(CLEO_OBS_XI)) o.xi = reinterpret_cast<uint64_t*>(st + off), off += a8;
+  if (want(CLEO_OBS_SDID)) o.sdid = reinterpret_cast<uint32_t*>(st + off), off += a4;
+  if (want(CLEO_OBS_SDGBXINDEX)) o.gbx = reinterpret_cast<uint32_t*>(st + off), off += a4;
+  if (want(CLEO_OBS_RADIUS)) o.r = reinterpret_cast<float*>(st + off), off += a4;
+  if (want(CLEO_OBS_MSOL)) o.msol = reinterpret_cast<float*>(st + off), off += a4;
+  if (want(CLEO_OBS_COORD3)) o.c3 = reinterpret_cast<float*>(st + off), off += a4;
+  if (want(CLEO_OBS_COORD1)) o.c1 = reinterpret_cast<float*>(st + off), off += a4;
+  if (want(CLEO_OBS_COORD2)) o.c2 = reinterpret_cast<float*>(st + off), off += a4;
+  // output offsets: exclusive scan of the valid counts, the total at start[ngbxs]
+  const uint32_t ns = (uint32_t)(((uint64_t)ng + SCAN_TILE - 1) / SCAN_TILE);
+  k_obs_counts<<<grid_for(ng, 256), 256, 0, s>>>(d, x->obs_start);
+  k_scan_tiles<<<ns ? ns : 1, SCAN_THREADS, 0, s>>>(x->obs_start, x->obs_start, ng, x->obs_tsums);
+  k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(x->obs_tsums, ns ? ns : 1, x->obs_start + ng);
+  k_scan_add<<<(unsigned)((ng + 255) / 256 + 1), 256, 0, s>>>(x->obs_start, ng, x->obs_tsums);
+  k_obs_gather<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, o, x->obs_start);
+  x->launches += 5;
+  CUDA_TRY(cudaGetLastError());
+  uint32_t total = 0;
+  CUDA_TRY(cudaMemcpyAsync(&total, x->obs_start + ng, 4, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  *n = total;
+  if (total > cap) return CLEO_ERR_CAPACITY;
+  const auto get = [&](void* dst, const void* src, size_t esize) -> int {
+    if (dst && src && total) {
+      CUDA_TRY(cudaMemcpyAsync(dst, src, total * esize, cudaMemcpyDeviceToHost, s));
+    }
+    return CLEO_OK;
+  };
+  int rc = 0;
+  rc |= get(out->xi, o.xi, 8);
+  rc |= get(out->sdid, o.sdid, 4);
+  rc |= get(out->sdgbxindex, o.gbx, 4);
+  rc |= get(out->radius, o.r, 4);
+  rc |= get(out->msol, o.msol, 4);
+  rc |= get(out->coord3, o.c3, 4);
+  rc |= get(out->coord1, o.c1, 4);
+  rc |= get(out->coord2, o.c2, 4);
+  if (rc) return CLEO_ERR_CUDA;
+  return cleo_b200_status(x, nullptr);
 }
 
 int cleo_b200_download_supers(cleo_b200_ctx* x, cleo_b200_supers* h, size_t* n_domain,

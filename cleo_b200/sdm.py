@@ -146,3 +146,44 @@ def make_sdm(workload: dict, lib=None, prefix="cleo_b200", params=None) -> SDM:
     sdm.upload_state(workload["state"])
     sdm.upload_supers(workload["supers"])
     return sdm
+
+
+def _main(argv=None):
+    """Run SDM steps of a synthetic workload on the GPU and print the per-stage CUDA-event times
+    of the last step:  python -m cleo_b200.sdm --workload uneven3d --ndims 32 64 64 --steps 4
+
+    Every step is complete (motion, re-sort, condensation, collisions); nothing is skipped.
+    """
+    import argparse
+    import json
+
+    from . import workloads as W
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="uneven3d", choices=["uneven3d", "bubble3d"])
+    ap.add_argument("--ndims", type=int, nargs=3, default=(32, 64, 64))
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--plain", action="store_true", help="the plain schedule (default batched)")
+    a = ap.parse_args(argv)
+    build = W.uneven3d if a.workload == "uneven3d" else W.bubble3d
+    w = build(ndims=tuple(a.ndims))
+    w["params"].exec_mode = abi.EXEC_PLAIN if a.plain else abi.EXEC_BATCHED
+    g = make_sdm(w)
+    ts = w["tstep"]
+    for s in range(a.steps - 1):
+        g.run_step(s * ts, (s + 1) * ts)
+    lib = g.lib
+    lib.cleo_b200_set_profiling(g.ctx, 1)
+    g.run_step((a.steps - 1) * ts, a.steps * ts)
+    g.check()
+    ms = (C.c_double * 8)()
+    cnt = (C.c_uint64 * 8)()
+    lib.cleo_b200_stage_times(g.ctx, ms, cnt)
+    names = ("motion", "sort", "microphysics", "condensation", "collisions")
+    print(json.dumps({"workload": a.workload, "ndims": list(a.ndims),
+                      "superdroplets": int(g.download_supers()["n_domain"]),
+                      "stages_ms": {n: ms[k] for k, n in enumerate(names)}}))
+    g.close()
+
+
+if __name__ == "__main__":
+    _main()

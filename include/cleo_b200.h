@@ -56,7 +56,9 @@ typedef enum cleo_status {
   CLEO_ERR_ARGUMENT = 12,        /* invalid argument (null pointer, bad enum, size mismatch) */
   CLEO_ERR_CUDA = 13,            /* a CUDA runtime call failed */
   CLEO_ERR_TIMEOUT = 14,         /* a bounded device-side wait gave up */
-  CLEO_ERR_MLP = 15              /* surrogate not loaded / bad shape */
+  CLEO_ERR_MLP = 15,             /* surrogate not loaded / bad shape */
+  CLEO_ERR_XI_OUTPUT = 16,       /* superdrops_observer.hpp:229-234  xi too large to write */
+  CLEO_ERR_IO = 17               /* a file of an output dataset could not be written */
 } cleo_status;
 
 /* ---- enumerations of the reference's plug-in choices ---- */
@@ -385,7 +387,7 @@ int cleo_b200_set_graphs(cleo_b200_ctx* ctx, int on);
  * SDM steps run as ordinary steps (same results) while each times one of four candidate launch
  * configurations per stage: for condensation pass A, the block size (128 or 256) and the
  * compiled variant's resident-CTA target (3 or 4 per SM, i.e. its register budget); for
- * collisions, the largest gridbox of the warp-per-gridbox kernel (32 or 64) and that kernel's
+ * collisions, the largest gridbox of the warp-per-gridbox kernel (64 or 128) and that kernel's
  * resident-CTA target (2 or 3). The fastest option of each stage is kept, and cached per process
  * by GPU name and domain size so that later contexts of that size start from it. Steps run
  * eagerly (with a stream synchronisation each) while tuning.
@@ -394,6 +396,70 @@ int cleo_b200_autotune(cleo_b200_ctx* ctx, int reps);
 /* Current configuration {pass-A block, pass-A CTA target, warp-kernel gridbox limit, warp-kernel
  * CTA target}; returns 1 while tuning is still in progress, else CLEO_OK. */
 int cleo_b200_tuned_config(cleo_b200_ctx* ctx, int32_t cfg[4]);
+/* Set that configuration directly (ending a tuning run in progress): pass-A block 128 or 256,
+ * pass-A CTA target 3 or 4, warp-kernel gridbox limit 1..128 (gridboxes above it go to the
+ * CTA-per-gridbox kernels), warp-kernel CTA target 2 or 3. Results do not depend on it. */
+int cleo_b200_set_launch_config(cleo_b200_ctx* ctx, const int32_t cfg[4]);
+
+/*
+ * Superdroplet output (SuperdropsObserver, observers/superdrops_observer.hpp:485-490, with the
+ * Collect* variables of superdrops_observer.hpp:139-470, and TimeObserver, time_observer.hpp:
+ * 46-144, writing into a SimpleDataset<FSStore>, zarr/simple_dataset.hpp:44-292). An
+ * observation writes the domain superdroplets (each gridbox's superdroplets in gridbox order,
+ * as SDMMethods::at_start_step passes them, sdmmethods.hpp:300-305) to ragged 1-D Zarr v2
+ * arrays, converted the way the Collect* functors convert them: sdgbxindex and sdId to uint32,
+ * xi to uint64, radius, msol and the coordinates to float (dimensionless values, with the
+ * reference's units and scale factors in each array's .zattrs), then appends their count to
+ * "raggedcount" and the observation time float(t_mdl / 1e5) (step2dimlesstime,
+ * initialise/timesteps.hpp:56-59) to "time". The files are the ones the reference writes for
+ * the same observations, byte for byte.
+ */
+enum cleo_obs_var {
+  CLEO_OBS_SDID = 1,
+  CLEO_OBS_SDGBXINDEX = 2,
+  CLEO_OBS_XI = 4,
+  CLEO_OBS_RADIUS = 8,
+  CLEO_OBS_MSOL = 16,
+  CLEO_OBS_COORD3 = 32,
+  CLEO_OBS_COORD1 = 64,
+  CLEO_OBS_COORD2 = 128,
+  CLEO_OBS_ALL = 255
+};
+/* Host arrays of the output types; a NULL member is skipped. */
+typedef struct cleo_b200_obs_supers {
+  uint32_t* sdid;
+  uint32_t* sdgbxindex;
+  uint64_t* xi;
+  float* radius;
+  float* msol;
+  float* coord3;
+  float* coord1;
+  float* coord2;
+} cleo_b200_obs_supers;
+/*
+ * The domain superdroplets of a context, gathered and converted on the GPU (the Collect*
+ * functors' copy loop, parallel_write_data.hpp:240-246) and copied into out's host arrays of at
+ * least `cap` elements (pinned memory copies fastest). *n receives their number; more than cap
+ * gives CLEO_ERR_CAPACITY with nothing copied.
+ */
+int cleo_b200_gather_supers(cleo_b200_ctx* ctx, uint32_t vars, const cleo_b200_obs_supers* out,
+                            size_t cap, size_t* n);
+
+typedef struct cleo_b200_zarr cleo_b200_zarr;
+/* New dataset in directory `dir` (created if needed): TimeObserver >> SuperdropsObserver of the
+ * variables in `vars`, observing at model steps that are multiples of `interval`, all arrays in
+ * chunks of `maxchunk` elements. */
+int cleo_b200_zarr_open(const char* dir, size_t maxchunk, uint32_t interval, uint32_t vars,
+                        cleo_b200_zarr** out);
+/* ConstTstepObserver::at_start_step at model step t_mdl with a context's domain superdroplets
+ * (nothing unless t_mdl is a multiple of the interval). */
+int cleo_b200_zarr_observe(cleo_b200_zarr* z, cleo_b200_ctx* ctx, uint32_t t_mdl);
+/* The same observation of n superdroplets given as host arrays of the output types (members of
+ * the dataset's variables must be non-NULL). */
+int cleo_b200_zarr_observe_host(cleo_b200_zarr* z, uint32_t t_mdl, const cleo_b200_obs_supers* s,
+                                size_t n);
+/* Write the last partly filled chunks and the final array shapes, then free the writer. */
+int cleo_b200_zarr_close(cleo_b200_zarr* z);
 
 /* Library version string. */
 const char* cleo_b200_version(void);

@@ -29,7 +29,14 @@
 #include "coupldyn_fromfile/fromfile_cartesian_dynamics.hpp"
 #include "initialise/gbx_bounds_from_binary.hpp"
 #include "initialise/init_all_supers_from_binary.hpp"
+#include "initialise/timesteps.hpp"
+#include "observers/collect_data_for_simple_dataset.hpp"
+#include "observers/observers.hpp"
 #include "observers/sdmmonitor/monitor_massmoments_change.hpp"
+#include "observers/superdrops_observer.hpp"
+#include "observers/time_observer.hpp"
+#include "zarr/fsstore.hpp"
+#include "zarr/simple_dataset.hpp"
 #include "observers/sdmmonitor/monitor_precipitation_observer.hpp"
 #include "runcleo/sdmmethods.hpp"
 #include "superdrops/collisions/breakup.hpp"
@@ -212,6 +219,61 @@ struct ref_ctx {
   cleo_b200_error err{CLEO_OK, 0xFFFFFFFFu, 0};
 };
 
+/* ---- superdroplet output: the reference's own SimpleDataset<FSStore> with TimeObserver >>
+ * SuperdropsObserver collecting all eight variables, composed as the examples compose them
+ * (main_rshaft1d.cpp:111-123, main_rshaft1d.cpp:134) ---- */
+using ZDataset = SimpleDataset<FSStore>;
+struct ZarrObsBase {
+  virtual ~ZarrObsBase() = default;
+  virtual void at_start_step(unsigned int t, const viewd_constgbx g,
+                             const subviewd_constsupers s) const = 0;
+};
+template <class O>
+struct ZarrObs final : ZarrObsBase {
+  O obs;
+  explicit ZarrObs(O o) : obs(std::move(o)) {}
+  void at_start_step(unsigned int t, const viewd_constgbx g,
+                     const subviewd_constsupers s) const override {
+    if (obs.on_step(t)) obs.at_start_step(t, g, s);
+  }
+};
+template <class O>
+static std::unique_ptr<ZarrObsBase> make_zarr_obs(O o) {
+  return std::make_unique<ZarrObs<O>>(std::move(o));
+}
+struct ref_zarr {
+  FSStore store;
+  ZDataset dataset;
+  std::unique_ptr<ZarrObsBase> obs;
+  viewd_gbx nogbxs;
+  ref_zarr(const char* dir, size_t maxchunk, unsigned int interval)
+      : store(std::filesystem::path(dir)), dataset(store), nogbxs("nogbxs", 0) {
+    const Observer auto t = TimeObserver(interval, dataset, store, maxchunk, &step2dimlesstime);
+    const auto sdid = CollectSdId(dataset, maxchunk);
+    const auto sdgbxindex = CollectSdgbxindex(dataset, maxchunk);
+    const auto xi = CollectXi(dataset, maxchunk);
+    const auto radius = CollectRadius(dataset, maxchunk);
+    const auto msol = CollectMsol(dataset, maxchunk);
+    const auto coord3 = CollectCoord3(dataset, maxchunk);
+    const auto coord1 = CollectCoord1(dataset, maxchunk);
+    const auto coord2 = CollectCoord2(dataset, maxchunk);
+    const auto all = coord3 >> coord1 >> coord2 >> msol >> radius >> xi >> sdgbxindex >> sdid;
+    const Observer auto sd = SuperdropsObserver(interval, dataset, store, maxchunk, all);
+    obs = make_zarr_obs(t >> sd);
+  }
+  ~ref_zarr() { obs.reset(); }  // the observers write their last chunks and shapes here
+};
+
+static viewd_supers supers_from_soa(const cleo_b200_supers* h, size_t n) {
+  viewd_supers totsupers("totsupers", n);
+  for (size_t k = 0; k < n; ++k) {
+    const SuperdropAttrs attrs(SoluteProperties{}, h->xi[k], h->radius[k], h->msol[k], true);
+    totsupers(k) = Superdrop(h->sdgbxindex[k], h->coord3[k], h->coord1[k], h->coord2[k], attrs,
+                             IntID{h->sdid ? (size_t)h->sdid[k] : k});
+  }
+  return totsupers;
+}
+
 static void fail(ref_ctx* c, int code) {
   if (c->err.code == CLEO_OK) c->err.code = code;
 }
@@ -304,12 +366,7 @@ void ref_destroy(ref_ctx* c) { delete c; }
 
 int ref_upload_supers(ref_ctx* c, const cleo_b200_supers* h, size_t n) {
   try {
-    viewd_supers totsupers("totsupers", n);
-    for (size_t k = 0; k < n; ++k) {
-      const SuperdropAttrs attrs(SoluteProperties{}, h->xi[k], h->radius[k], h->msol[k], true);
-      totsupers(k) = Superdrop(h->sdgbxindex[k], h->coord3[k], h->coord1[k], h->coord2[k], attrs,
-                               IntID{h->sdid ? (size_t)h->sdid[k] : k});
-    }
+    viewd_supers totsupers = supers_from_soa(h, n);
     c->allsupers = std::make_unique<SupersInDomain>(totsupers, c->ngbxs);
     /* gridboxes refer to the sorted superdroplets (Gridbox ctor, gridbox.hpp:44-46) */
     auto hg = c->gbxs.view_host();
@@ -566,6 +623,44 @@ double ref_pair_probability(const cleo_b200_params* p, double r1, uint64_t xi1, 
 
 /* Neighbour maps as the reference builds them (doubly_periodic_domain.hpp:41-101 via
  * createcartesianmaps.cpp:203-220) for a 3-D domain; used to pin the host-side grid builder. */
+/* Superdroplet output through the reference's writer into directory `dir`: observations every
+ * `interval` model steps, arrays chunked by `maxchunk` elements. */
+int ref_zarr_open(const char* dir, size_t maxchunk, uint32_t interval, ref_zarr** out) {
+  if (!dir || !out || maxchunk == 0 || interval == 0) return CLEO_ERR_ARGUMENT;
+  try {
+    *out = new ref_zarr(dir, maxchunk, interval);
+  } catch (const std::exception&) {
+    return CLEO_ERR_ARGUMENT;
+  }
+  return CLEO_OK;
+}
+
+/* SDMMethods::at_start_step (sdmmethods.hpp:300-305): observe the domain superdroplets */
+int ref_zarr_observe(ref_zarr* z, ref_ctx* c, uint32_t t_mdl) {
+  if (!z || !c || !c->allsupers) return CLEO_ERR_ARGUMENT;
+  try {
+    z->obs->at_start_step(t_mdl, c->gbxs.view_device(), c->allsupers->domain_supers_readonly());
+  } catch (const kokkos_shim::Abort& e) {
+    return CLEO_ERR_ARGUMENT;
+  }
+  return CLEO_OK;
+}
+
+/* the same observation of n given superdroplets (taken as the domain superdroplets) */
+int ref_zarr_observe_supers(ref_zarr* z, uint32_t t_mdl, const cleo_b200_supers* h, size_t n) {
+  if (!z || (!h && n)) return CLEO_ERR_ARGUMENT;
+  try {
+    const viewd_supers v = supers_from_soa(h, n);
+    const subviewd_constsupers s = Kokkos::subview(viewd_constsupers(v), kkpair_size_t({0, n}));
+    z->obs->at_start_step(t_mdl, z->nogbxs, s);
+  } catch (const kokkos_shim::Abort& e) {
+    return CLEO_ERR_ARGUMENT;
+  }
+  return CLEO_OK;
+}
+
+void ref_zarr_close(ref_zarr* z) { delete z; }
+
 void ref_cartesian_neighbours(const uint32_t ndims[3], uint32_t idx, uint32_t out[6]) {
   const std::vector<size_t> nd{ndims[0], ndims[1], ndims[2]};
   const auto z = DoublyPeriodicDomain::cartesian_coord3nghbrs(idx, nd);

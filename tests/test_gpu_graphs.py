@@ -88,3 +88,28 @@ def test_autotune_keeps_results_and_picks_a_candidate(lib):
     w["params"].exec_mode = abi.EXEC_PLAIN
     p = make_sdm(w, lib=lib)
     assert lib.cleo_b200_autotune(p.ctx, 1) == abi.CODE["CLEO_ERR_ARGUMENT"]
+
+
+@pytest.mark.parametrize("cfg", [(256, 3, 64, 2), (128, 4, 128, 2), (256, 4, 128, 3),
+                                 (128, 3, 20, 3)])
+def test_launch_configs_match_oracle(lib, cfg):
+    """Every launch configuration the autotuner can choose (and an arbitrary warp-kernel limit)
+    gives the oracle's results; the workload has gridboxes on both sides of 64 and 128."""
+    import ctypes as C
+    w = W.uneven3d(ndims=(6, 8, 8), seed=23, median=60.0, sigma=0.5)
+    w["params"].exec_mode = abi.EXEC_BATCHED
+    counts = np.bincount(w["supers"]["sdgbxindex"], minlength=w["grid"]["ngbxs"])
+    assert counts.max() > 128 and ((counts > 64) & (counts <= 128)).sum() > 20
+    g = make_sdm(w, lib=lib)
+    arr = (C.c_int32 * 4)(*cfg)
+    assert lib.cleo_b200_set_launch_config(g.ctx, arr) == 0
+    got = (C.c_int32 * 4)()
+    assert lib.cleo_b200_tuned_config(g.ctx, got) == 0 and tuple(got) == cfg
+    o = make_sdm(w, lib=K.oracle_lib(), prefix="oc")
+    for k in range(4):
+        g.run_step(k * w["tstep"], (k + 1) * w["tstep"])
+        o.run_step(k * w["tstep"], (k + 1) * w["tstep"])
+    g.check()
+    K.assert_same_domain(g.download_supers(), o.download_supers(), rtol=1e-12, what=str(cfg))
+    bad = (C.c_int32 * 4)(256, 3, 129, 2)
+    assert lib.cleo_b200_set_launch_config(g.ctx, bad) == abi.CODE["CLEO_ERR_ARGUMENT"]
