@@ -76,6 +76,7 @@ struct DevCtx {
   // positions, the stayers, and the new gridbox starts (ngbxs + 2)
   uint32_t *mv_scan, *mv_leave, *mv_arrive, *mv_below, *mv_stay, *gstart_new, *mv_mstart,
       *mv_shift;
+  uint32_t* mv_total;  // valid superdroplets that changed gridbox in the last motion step
   // scratch
   double *scr_r, *scr_m, *scr_c3, *scr_c1, *scr_c2;
   unsigned long long *scr_x, *scr_id;
@@ -110,6 +111,12 @@ struct cleo_b200_ctx {
   // sort scratch
   uint32_t *keys[2], *vals[2], *hist, *tile_sums;
   uint32_t *mv_tsums = nullptr, *mv_count = nullptr;  // incremental re-sort scratch
+  // re-sort choice: {movers, superdroplets} of the last motion step in mapped pinned memory,
+  // written by the device and read by the host without synchronisation (a value one step old
+  // only changes which of the two equal-result sorts runs)
+  uint32_t* h_motion = nullptr;
+  uint32_t* d_motion = nullptr;
+  bool sort_full = false;
   // superdroplet output staging (allocated at the first gather): converted fields, offsets
   uint8_t* obs_stage = nullptr;
   uint32_t *obs_start = nullptr, *obs_tsums = nullptr;
@@ -255,16 +262,17 @@ __device__ __forceinline__ bool beyond_domainboundary(uint32_t gbxindex, uint32_
 // (predcorrmotion.hpp:85-106) with get_no_decomposition_bounding_gridbox (cartesianmaps.cpp:278)
 // and CartesianCheckBounds. Writes the sort key min(gbx, ngbxs) and the position.
 __global__ void __launch_bounds__(256, 3)
-k_motion(DevCtx c, uint32_t* __restrict__ keys) {
+k_motion(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, int incremental) {
   const uint32_t n = c.counters[0];
   const uint32_t ng = c.ngbxs;
   const double delt = c.p.motion_delt;
-  if (blockIdx.x == 0 && threadIdx.x == 0) c.mv_scan[n] = 0;  // the scan's total lands here
+  if (incremental && blockIdx.x == 0 && threadIdx.x == 0) c.mv_scan[n] = 0;  // scan total
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t g = c.sd.gbx[i];
+    if (!incremental) vals[i] = i;
     if (g >= ng) {  // null superdroplet left by collisions: out of the domain
       keys[i] = ng;
-      c.mv_scan[i] = 1;  // a mover, but not one of its range's gcount valid superdroplets
+      if (incremental) c.mv_scan[i] = 1;  // a mover, not one of its range's valid superdroplets
       continue;
     }
     const Where w{c.err, g, i};
@@ -380,6 +388,12 @@ k_motion(DevCtx c, uint32_t* __restrict__ keys) {
     keys[i] = key;
     // a superdroplet that changes gridbox (or leaves the domain) moves in the re-sort
     const bool mover = key != g;
+    {  // count them (warp-aggregated) for the choice of the next re-sort
+      const unsigned am = __activemask();
+      const unsigned bm = __ballot_sync(am, mover);
+      if (bm && (int)(threadIdx.x & 31) == __ffs(am) - 1) atomicAdd(c.mv_total, __popc(bm));
+    }
+    if (!incremental) continue;
     c.mv_scan[i] = mover ? 1u : 0u;
     if (mover) {
       atomicAdd(&c.mv_leave[g], 1u);
@@ -389,6 +403,10 @@ k_motion(DevCtx c, uint32_t* __restrict__ keys) {
       }
     }
   }
+}
+__global__ void k_mv_report(DevCtx c, uint32_t* __restrict__ out) {  // mapped host memory
+  out[0] = *c.mv_total;
+  out[1] = c.counters[0];
 }
 
 // ---- incremental re-sort (stable by gridbox, equal to the full radix sort) ----
@@ -1277,19 +1295,24 @@ int run_sdm_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
   if (did_motion) {
     {
       StageMark m(x, 0);
+      const bool inc = !x->sort_full;
       const size_t ngb = (size_t)(d.ngbxs ? d.ngbxs : 1) * 4;
-      CUDA_TRY(cudaMemsetAsync(d.mv_leave, 0, ngb, s));
-      CUDA_TRY(cudaMemsetAsync(d.mv_arrive, 0, ngb, s));
-      CUDA_TRY(cudaMemsetAsync(d.mv_below, 0, ngb, s));
-      k_motion<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, x->keys[0]);
-      x->launches += 1;
+      if (inc) {
+        CUDA_TRY(cudaMemsetAsync(d.mv_leave, 0, ngb, s));
+        CUDA_TRY(cudaMemsetAsync(d.mv_arrive, 0, ngb, s));
+        CUDA_TRY(cudaMemsetAsync(d.mv_below, 0, ngb, s));
+      }
+      CUDA_TRY(cudaMemsetAsync(d.mv_total, 0, 4, s));
+      k_motion<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, x->keys[0], x->vals[0], inc ? 1 : 0);
+      k_mv_report<<<1, 1, 0, s>>>(d, x->d_motion);
+      x->launches += 2;
       if (d.p.monitors & CLEO_MONITOR_PRECIPITATION) {  // before the sort moves the droplets
         k_mon_precip<<<gg, 256, 0, s>>>(d);
         x->launches += 1;
       }
     }
     StageMark m(x, 1);
-    const int rc = sort_incremental(x);
+    const int rc = x->sort_full ? sort_current(x) : sort_incremental(x);
     if (rc) return rc;
     if (mon_mm) {  // monitor_motion (movesupersindomain.hpp:297)
       k_mon_mm<<<gg, 256, 0, s>>>(d, 1, 0);
@@ -1394,7 +1417,7 @@ int run_step_graphed(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
   const cleo_b200_params& p = x->d.p;
   std::vector<uint32_t> sig;
   sig.push_back((uint32_t)x->cur);
-  sig.push_back(on_step(p.motionstep, t_sdm) ? 1u : 0u);
+  sig.push_back((on_step(p.motionstep, t_sdm) ? 1u : 0u) | (x->sort_full ? 2u : 0u));
   sig.push_back(t_sdm_next - t_sdm);
   for (uint32_t subt = t_sdm; subt < t_sdm_next;
        subt = min(next_step(p.condstep, subt), next_step(p.collstep, subt))) {
@@ -1523,6 +1546,12 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &d.mv_stay, ng);
   rc |= dalloc(x, &d.mv_mstart, (size_t)ng + 1);
   rc |= dalloc(x, &d.mv_shift, ng);
+  rc |= dalloc(x, &d.mv_total, 1);
+  if (cudaHostAlloc(&x->h_motion, 2 * sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer(&x->d_motion, x->h_motion, 0) != cudaSuccess)
+    rc |= CLEO_ERR_CUDA;
+  else
+    x->h_motion[0] = x->h_motion[1] = 0;
   rc |= dalloc(x, &d.gstart_new, (size_t)ng + 2);
   rc |= dalloc(x, &x->mv_count, 1);
   {
@@ -1641,6 +1670,7 @@ void cleo_b200_destroy(cleo_b200_ctx* x) {
   cudaFree(x->seed_buf);
   x->free_cs();
   for (void* p : x->allocs) cudaFree(p);
+  if (x->h_motion) cudaFreeHost(x->h_motion);
   if (x->own_stream && x->stream) cudaStreamDestroy(x->stream);
   delete x;
 }
@@ -1734,6 +1764,11 @@ int cleo_b200_step(cleo_b200_ctx* x, uint32_t t_mdl, uint32_t t_next) {
   while (t_sdm < t_next) {
     const uint32_t next_move = next_step(x->d.p.motionstep, t_sdm);
     const uint32_t t_sdm_next = t_next < next_move ? t_next : next_move;
+    {  // full re-sort when more than a fifth of the superdroplets changed gridbox last time
+      const volatile uint32_t* hm = x->h_motion;
+      const uint32_t movers = hm[0], nsd = hm[1];
+      x->sort_full = (uint64_t)movers * 5 > (uint64_t)nsd;
+    }
     int rc;
     if (batched) {
       if (x->t_dev != t_sdm) {
