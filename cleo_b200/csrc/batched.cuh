@@ -268,32 +268,94 @@ __device__ __forceinline__ uint32_t fy_origin(const JT* J, uint32_t n, uint32_t 
 
 // ---- small gridboxes: persistent, one warp per gridbox ----
 // CAP (64 or 128) is the number of per-warp slots; every lane holds CAP / 32 of them.
+// Radius, solute mass and multiplicity of each gridbox are staged in shared memory by bulk
+// copies (TMA, cp.async.bulk) into one of two buffers per warp: the next gridbox's copies are
+// in flight while the current one is processed. A copy starts at the even element at or below
+// the gridbox's first superdroplet (16-byte alignment) and covers an even number of elements, so
+// it may read one element past the range (the SoA arrays carry two elements of padding).
+using mlp::fence_async_smem;
+using mlp::mbar_init;
+using mlp::mbar_wait_bounded;
+using mlp::MBAR_TRIES;
+using mlp::smem_u32;
+
+template <int CAP>
+struct SmallLayout {
+  static constexpr uint32_t BUF = CAP + 2;  // elements per staged field
+  static constexpr uint32_t FIELD = BUF * 8;
+  static constexpr uint32_t OFF_TV = 2 * 3 * FIELD;
+  static constexpr uint32_t OFF_P = OFF_TV + CAP * 8;
+  static constexpr uint32_t OFF_J = OFF_P + CAP;
+  static constexpr uint32_t OFF_BAR = (OFF_J + CAP + 15) / 16 * 16;
+  static constexpr uint32_t WARP_BYTES = OFF_BAR + 16;
+  static constexpr uint32_t BYTES = WARP_BYTES * B_WARPS;
+  static_assert(FIELD % 16 == 0 && WARP_BYTES % 16 == 0, "bulk-copy buffers must be aligned");
+};
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(__cvta_generic_to_global(src)), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
 template <int MINB, int CAP>
 __global__ void __launch_bounds__(B_THREADS, MINB)
 k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
+  using L = SmallLayout<CAP>;
   constexpr int H = CAP / 32;
   static_assert(CAP % 32 == 0 && CAP <= 255, "slot indices are stored as bytes");
   const uint32_t t_sdm = *b.tsdm;
-  __shared__ double s_r[B_WARPS][CAP];
-  __shared__ double s_m[B_WARPS][CAP];
-  __shared__ unsigned long long s_x[B_WARPS][CAP];
-  __shared__ double s_tv[B_WARPS][CAP];
-  __shared__ uint8_t s_p[B_WARPS][CAP];
-  __shared__ uint8_t s_j[B_WARPS][CAP];
+  extern __shared__ __align__(16) unsigned char smem_small[];
   const cleo_b200_params& p = c.p;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  unsigned char* wsm = smem_small + wib * L::WARP_BYTES;
+  double* s_tv = reinterpret_cast<double*>(wsm + L::OFF_TV);
+  uint8_t* s_p = wsm + L::OFF_P;
+  uint8_t* s_j = wsm + L::OFF_J;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(wsm + L::OFF_BAR);
+  const auto field = [&](int buf, int f) { return wsm + (buf * 3 + f) * L::FIELD; };
   const uint32_t count = b.ctr[1];
   const uint32_t* list = b.bucket;
+  // stage gridbox g's r, msol, xi into buffer buf (lane 0)
+  const auto stage = [&](int buf, uint32_t g) {
+    const uint32_t base = c.gstart[g], n = c.gcount[g];
+    const uint32_t a0 = base & ~1u;
+    const uint32_t bytes = ((n + (base & 1u) + 1u) & ~1u) * 8u;
+    fence_async_smem();  // earlier generic accesses of the buffer precede the async writes
+    mbar_expect_tx(&bar[buf], 3u * bytes);
+    bulk_g2s(field(buf, 0), c.sd.r + a0, bytes, &bar[buf]);
+    bulk_g2s(field(buf, 1), c.sd.msol + a0, bytes, &bar[buf]);
+    bulk_g2s(field(buf, 2), c.sd.xi + a0, bytes, &bar[buf]);
+  };
   // static assignment (item = warp + k * warps): no shared counter, and the next gridbox's list
   // entry is loaded a whole gridbox ahead
   const uint32_t nwarps = gridDim.x * B_WARPS;
   uint32_t item = blockIdx.x * B_WARPS + wib;
   uint32_t g_next = item < count ? list[item] : 0u;
+  uint32_t parity = 0;  // bit k: the phase of bar[k] to wait for
+  int cur = 0;
+  if (coll) {
+    if (lane == 0) {
+      mbar_init(&bar[0], 1);
+      mbar_init(&bar[1], 1);
+      if (item < count) stage(0, g_next);
+    }
+    __syncwarp();
+  }
   for (; item < count; item += nwarps) {
     const uint32_t g = g_next;
-    if (item + nwarps < count) g_next = list[item + nwarps];
+    const bool has_next = item + nwarps < count;
+    if (has_next) g_next = list[item + nwarps];
     const uint32_t base = c.gstart[g];
-    uint32_t n = c.gcount[g];
+    const uint32_t n = c.gcount[g];
     if (cond) {
       double m = 0.0;
       uint32_t it = 0;
@@ -306,17 +368,24 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
       if (lane == 0) cond_commit(c, g, m, it);
     }
     if (!coll) continue;
+    // the next gridbox's copies go out before this one's wait
+    if (has_next && lane == 0) stage(cur ^ 1, g_next);
+    if (!mbar_wait_bounded(&bar[cur], (parity >> cur) & 1u, MBAR_TRIES)) {
+      if (lane == 0) Where{c.err, g, base}.fail(CLEO_ERR_TIMEOUT);
+      if (has_next) mbar_wait_bounded(&bar[cur ^ 1], (parity >> (cur ^ 1)) & 1u, MBAR_TRIES);
+      return;
+    }
+    parity ^= 1u << cur;
+    const uint32_t off = base & 1u;
+    double* s_r = reinterpret_cast<double*>(field(cur, 0)) + off;
+    double* s_m = reinterpret_cast<double*>(field(cur, 1)) + off;
+    unsigned long long* s_x = reinterpret_cast<unsigned long long*>(field(cur, 2)) + off;
     const uint64_t key = cleo_rng_key(p.seed, t_sdm, g);
     const uint64_t slot = b.slot[g];
-    // stage this gridbox: lane holds k = lane + 32 h
     for (uint32_t k = lane; k < n; k += 32) {
-      const double rk = c.sd.r[base + k];
-      s_r[wib][k] = rk;
-      s_m[wib][k] = c.sd.msol[base + k];
-      s_x[wib][k] = c.sd.xi[base + k];
-      s_tv[wib][k] = pair_tv(p, rk);
+      s_tv[k] = pair_tv(p, s_r[k]);
       if (k >= 1)
-        s_j[wib][k] = (uint8_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - k)), 0, (uint64_t)k + 1);
+        s_j[k] = (uint8_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - k)), 0, (uint64_t)k + 1);
     }
     __syncwarp();
     {  // origins of the lane's positions, traced together through the swaps (fy_origin)
@@ -324,13 +393,13 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
 #pragma unroll
       for (int h = 0; h < H; ++h) pos[h] = lane + 32 * h;
       for (uint32_t s = 1; s < n; ++s) {
-        const uint32_t j = s_j[wib][s];
+        const uint32_t j = s_j[s];
 #pragma unroll
         for (int h = 0; h < H; ++h) pos[h] = (pos[h] == s) ? j : ((pos[h] == j) ? s : pos[h]);
       }
 #pragma unroll
       for (int h = 0; h < H; ++h)
-        if (lane + 32 * h < n) s_p[wib][lane + 32 * h] = (uint8_t)pos[h];
+        if (lane + 32 * h < n) s_p[lane + 32 * h] = (uint8_t)pos[h];
     }
     __syncwarp();
     const uint64_t slot_pairs = slot + (n >= 1 ? n - 1 : 0);
@@ -339,14 +408,14 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
     const double VOLUME = c.volume[g] * VOL0;
     uint32_t nnull = 0;
     for (uint32_t jj = lane; jj < npairs; jj += 32) {
-      const uint32_t a = s_p[wib][2 * jj], bb = s_p[wib][2 * jj + 1];
+      const uint32_t a = s_p[2 * jj], bb = s_p[2 * jj + 1];
       const Where w{c.err, g, (uint64_t)base + 2 * jj};
-      Drop dA{s_x[wib][a], s_r[wib][a], s_m[wib][a]};
-      Drop dB{s_x[wib][bb], s_r[wib][bb], s_m[wib][bb]};
-      nnull += collide_pair(p, dA, dB, s_tv[wib][a], s_tv[wib][bb], scale_p, VOLUME, key,
-                            slot_pairs, jj, w);
-      s_x[wib][a] = dA.xi; s_r[wib][a] = dA.r; s_m[wib][a] = dA.msol;
-      s_x[wib][bb] = dB.xi; s_r[wib][bb] = dB.r; s_m[wib][bb] = dB.msol;
+      Drop dA{s_x[a], s_r[a], s_m[a]};
+      Drop dB{s_x[bb], s_r[bb], s_m[bb]};
+      nnull += collide_pair(p, dA, dB, s_tv[a], s_tv[bb], scale_p, VOLUME, key, slot_pairs, jj,
+                            w);
+      s_x[a] = dA.xi; s_r[a] = dA.r; s_m[a] = dA.msol;
+      s_x[bb] = dB.xi; s_r[bb] = dB.r; s_m[bb] = dB.msol;
     }
     __syncwarp();
     const uint32_t totnull = warp_sum_u(nnull);
@@ -361,8 +430,8 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
       if (32u * h >= n) break;  // uniform across the warp
       const uint32_t k = lane + 32 * h;
       const bool act = k < n;
-      src[h] = act ? s_p[wib][k] : 0;
-      const bool valid = act && s_x[wib][src[h]] != 0;
+      src[h] = act ? s_p[k] : 0;
+      const bool valid = act && s_x[src[h]] != 0;
       const unsigned mv = __ballot_sync(0xFFFFFFFFu, valid);
       const unsigned mn = __ballot_sync(0xFFFFFFFFu, act && !valid);
       const unsigned lt = (1u << lane) - 1u;
@@ -383,9 +452,9 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
       const uint32_t k = lane + 32 * h;
       if (k < n) {
         const uint32_t o = base + q[h];
-        c.sd.r[o] = s_r[wib][src[h]];
-        c.sd.msol[o] = s_m[wib][src[h]];
-        c.sd.xi[o] = s_x[wib][src[h]];
+        c.sd.r[o] = s_r[src[h]];
+        c.sd.msol[o] = s_m[src[h]];
+        c.sd.xi[o] = s_x[src[h]];
         c.sd.gbx[o] = q[h] < nvalid ? g : OOB;
         c.sd.c3[o] = c3v[h];
         c.sd.c1[o] = c1v[h];
@@ -393,12 +462,12 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
         c.sd.id[o] = idv[h];
       }
     }
-    __syncwarp();
+    __syncwarp();  // every lane is done with buffer cur before it is staged into again
     if (lane == 0) {
       c.gcount[g] = nvalid;
       b.slot[g] = (uint32_t)(slot_pairs + 2ull * npairs);
     }
-    n = nvalid;
+    cur ^= 1;
   }
 }
 

@@ -1070,8 +1070,11 @@ int dalloc(cleo_b200_ctx* x, T** p, size_t n) {
   return CLEO_OK;
 }
 
+// two elements of padding: the warp collision kernel's bulk copies may read one element past
+// the last superdroplet
 int alloc_fields(cleo_b200_ctx* x, Fields& f, size_t n) {
   int rc = 0;
+  n += 2;
   rc |= dalloc(x, &f.gbx, n);
   rc |= dalloc(x, &f.c3, n);
   rc |= dalloc(x, &f.c1, n);
@@ -1264,14 +1267,15 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       k_b_classify<<<gg, 256, 0, s>>>(d, b);
       const int wide = x->cfg.small_max > SMALL_MAX ? 1 : 0, m3 = x->cfg.small_minb == 3 ? 1 : 0;
       const int gs = x->grid_small[wide][m3], ci = cond ? 1 : 0, li = coll ? 1 : 0;
+      constexpr uint32_t SW = SmallLayout<WARP_MAX>::BYTES, SS = SmallLayout<SMALL_MAX>::BYTES;
       if (wide && m3)
-        k_b_small<3, WARP_MAX><<<gs, B_THREADS, 0, s>>>(d, b, ci, li);
+        k_b_small<3, WARP_MAX><<<gs, B_THREADS, SW, s>>>(d, b, ci, li);
       else if (wide)
-        k_b_small<2, WARP_MAX><<<gs, B_THREADS, 0, s>>>(d, b, ci, li);
+        k_b_small<2, WARP_MAX><<<gs, B_THREADS, SW, s>>>(d, b, ci, li);
       else if (m3)
-        k_b_small<3, SMALL_MAX><<<gs, B_THREADS, 0, s>>>(d, b, ci, li);
+        k_b_small<3, SMALL_MAX><<<gs, B_THREADS, SS, s>>>(d, b, ci, li);
       else
-        k_b_small<2, SMALL_MAX><<<gs, B_THREADS, 0, s>>>(d, b, ci, li);
+        k_b_small<2, SMALL_MAX><<<gs, B_THREADS, SS, s>>>(d, b, ci, li);
       k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_SMEM, s>>>(d, b, cond ? 1 : 0,
                                                                            coll ? 1 : 0);
       k_b_cta<true><<<x->grid_large, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
@@ -1627,17 +1631,26 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
     int dev = 0, sms = 148, occ = 1;
     CUDA_TRY(cudaGetDevice(&dev));
     CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    constexpr int SW = (int)SmallLayout<WARP_MAX>::BYTES, SS = (int)SmallLayout<SMALL_MAX>::BYTES;
+    CUDA_TRY(cudaFuncSetAttribute(k_b_small<2, SMALL_MAX>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SS));
+    CUDA_TRY(cudaFuncSetAttribute(k_b_small<3, SMALL_MAX>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SS));
+    CUDA_TRY(cudaFuncSetAttribute(k_b_small<2, WARP_MAX>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SW));
+    CUDA_TRY(cudaFuncSetAttribute(k_b_small<3, WARP_MAX>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SW));
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<2, SMALL_MAX>,
-                                                           B_THREADS, 0));
+                                                           B_THREADS, SS));
     x->grid_small[0][0] = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<3, SMALL_MAX>,
-                                                           B_THREADS, 0));
+                                                           B_THREADS, SS));
     x->grid_small[0][1] = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<2, WARP_MAX>,
-                                                           B_THREADS, 0));
+                                                           B_THREADS, SW));
     x->grid_small[1][0] = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<3, WARP_MAX>,
-                                                           B_THREADS, 0));
+                                                           B_THREADS, SW));
     x->grid_small[1][1] = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<false>, B_THREADS,
                                                            (size_t)MEDIUM_SMEM));

@@ -163,11 +163,17 @@ def _main(argv=None):
     ap.add_argument("--ndims", type=int, nargs=3, default=(32, 64, 64))
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--plain", action="store_true", help="the plain schedule (default batched)")
+    ap.add_argument("--launch-config", type=int, nargs=4, default=None,
+                    help="pass-A block, pass-A CTAs per SM, warp-kernel gridbox limit, "
+                         "warp-kernel CTAs per SM (cleo_b200_set_launch_config)")
     a = ap.parse_args(argv)
     build = W.uneven3d if a.workload == "uneven3d" else W.bubble3d
     w = build(ndims=tuple(a.ndims))
     w["params"].exec_mode = abi.EXEC_PLAIN if a.plain else abi.EXEC_BATCHED
     g = make_sdm(w)
+    if a.launch_config is not None:
+        cfg = (C.c_int32 * 4)(*a.launch_config)
+        g._check(g.lib.cleo_b200_set_launch_config(g.ctx, cfg), "in set_launch_config")
     ts = w["tstep"]
     for s in range(a.steps - 1):
         g.run_step(s * ts, (s + 1) * ts)
