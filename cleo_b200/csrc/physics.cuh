@@ -249,8 +249,10 @@ __device__ __forceinline__ double nfrags_of(const cleo_b200_params& p, double r1
   const double gamma = dpow(cke_cap * 1e6, beta);
   return 1.0 / (alpha - gamma) + epsilon;
 }
-__device__ __forceinline__ unsigned coalbure_flag(const cleo_b200_params& p, double phi, double r1,
-                                                  double r2) {  // coalbure_flag.hpp:42-198
+// The outcomes of a collision (flag, coalescence, breakup) run only for the pairs that collide;
+// kept out of line, they stay out of the collision kernels' hot loops and instruction caches.
+static __device__ __noinline__ unsigned coalbure_flag(const cleo_b200_params& p, double phi,
+                                                      double r1, double r2) {  // coalbure_flag.hpp:42-198
   switch (p.flag_kind) {
     case CLEO_FLAG_STRAUB: {
       const double cke = collision_kinetic_energy(r1, r2, terminalv(p.flag_tv, r1),
@@ -326,7 +328,7 @@ __device__ __forceinline__ void different_coalescence(uint64_t gamma, Drop& d1, 
   d2.r = nr;
   d2.msol = d2.msol + (double)gamma * d1.msol;
 }
-__device__ __forceinline__ uint32_t coalesce_pair(uint64_t gamma, Drop& d1, Drop& d2,
+static __device__ __noinline__ uint32_t coalesce_pair(uint64_t gamma, Drop& d1, Drop& d2,
                                                   const Where& w) {  // :92-113
   const uint64_t xi1 = d1.xi, xi2 = d2.xi;
   if (xi1 - gamma * xi2 > 0) {
@@ -389,7 +391,7 @@ __device__ __forceinline__ void different_breakup(const cleo_b200_params& p, Dro
   d2.r = new_r;
   d2.msol = new_msol;
 }
-__device__ __forceinline__ uint32_t breakup_pair(const cleo_b200_params& p, Drop& d1, Drop& d2,
+static __device__ __noinline__ uint32_t breakup_pair(const cleo_b200_params& p, Drop& d1, Drop& d2,
                                                  const Where& w) {  // :176-186
   if (d1.xi == d2.xi) {
     twin_breakup(p, d1, d2, w);
