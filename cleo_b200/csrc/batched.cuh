@@ -7,7 +7,10 @@
 //                  implicit-Euler solve; solves needing more (sub-stepping, or a restart after two
 //                  unconverged iterations) are appended to a list keyed by their cost
 //   (radix sort of that list by cost, 16-bit keys)
-//   k_cond_b       thread per listed solve, neighbouring lanes of similar cost
+//   k_mlp_tc       with nr_seed = CLEO_NRSEED_MLP only: the surrogate's Newton seeds for the
+//                  listed solves (the ones the reference guess did not settle in two iterations)
+//   k_cond_b       thread per listed solve, neighbouring lanes of similar cost, from the seed
+//                  where its residual beats the reference guess's
 //   k_b_classify   gridboxes into size buckets (warp-aggregated atomics)
 //   k_b_small      persistent, warp per gridbox (n <= small_max <= 128; 64- and 128-slot
 //                  variants): reduction of the condensed mass and Newton iterations, state
@@ -81,24 +84,27 @@ __global__ void k_b_thermo(DevCtx c, BatchScratch b) {
   }
 }
 
-// domain superdroplets -> Newton seed r^2 in b.dm (the surrogate's IO in the batched schedule)
-struct SdmSeedIO {
+// the surrogate's IO for the batched schedule: row j is the j-th solve of pass A's list of
+// unconverged and sub-stepping solves (b.lvals, count b.ctr[0]); the seed r^2 goes to b.dm of that
+// droplet, which pass B reads (and then overwrites with the droplet's condensed mass)
+struct SdmListSeedIO {
   const uint32_t* gbx;
   const double *r, *msol, *temp, *press, *s_ratio;
   double delt;
-  uint32_t ngbxs;
-  const uint32_t* nrange;  // counters[0]
+  const uint32_t* list;
+  const uint32_t* count;
   double* seed;
-  __device__ __forceinline__ bool in_domain(uint32_t i) const {
-    return i < *nrange && gbx[i] < ngbxs;
+  __device__ __forceinline__ uint32_t rows(uint32_t n) const {
+    const uint32_t c = *count;
+    return c < n ? c : n;
   }
-  __device__ __forceinline__ void features(uint32_t i, float x[mlp::NIN]) const {
-    if (!in_domain(i)) return;
+  __device__ __forceinline__ void features(uint32_t j, float x[mlp::NIN]) const {
+    const uint32_t i = list[j];
     const uint32_t g = gbx[i];
     mlp::raw_features(r[i], msol[i], temp[g], press[g], s_ratio[g], delt, x);
   }
-  __device__ __forceinline__ void store(uint32_t i, float t) const {
-    if (!in_domain(i)) return;
+  __device__ __forceinline__ void store(uint32_t j, float t) const {
+    const uint32_t i = list[j];
     const double ri = r[i];
     seed[i] = ri * ri * exp((double)t);
   }
@@ -139,22 +145,8 @@ k_cond_a(DevCtx c, BatchScratch b) {
         if (ucrit1 || p.cond_delt <= crit) {
           bool conv = false;
           GEval e = eval_g(o, p.cond_delt, r, z0);
-          bool seeded = false;  // the surrogate's seed, when its residual is the smaller one
-          if (p.nr_seed == CLEO_NRSEED_MLP && seed_ok(b.dm[i])) {
-            const GEval es = eval_g(o, p.cond_delt, r, b.dm[i]);
-            if (fabs(es.g) < fabs(e.g)) {
-              double zs;
-              conv = integrate_seeded(cfg, o, p.cond_delt, r, es, ni, zs) &&
-                     seeded_root_ok(o, ucrit1, zs);
-              e.z = zs;
-              seeded = true;
-              if (!conv) b.dm[i] = -1.0;  // pass B starts from the reference guess
-            }
-          }
-          if (!seeded) {
-            e = nr_iterate(cfg, o, p.cond_delt, r, e, conv, ni);
-            e = nr_iterate(cfg, o, p.cond_delt, r, e, conv, ni);
-          }
+          e = nr_iterate(cfg, o, p.cond_delt, r, e, conv, ni);
+          e = nr_iterate(cfg, o, p.cond_delt, r, e, conv, ni);
           if (conv) {
             const double rnew = fmax(sqrt(e.z), dryradius(msol));  // change_radius
             b.dm[i] = (condensate_mass(rnew, msol, w) - condensate_mass(r, msol, w)) *

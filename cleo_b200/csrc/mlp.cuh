@@ -244,6 +244,7 @@ __global__ void __launch_bounds__(128) k_mlp_tc(Infer w, IO io, uint32_t n) {
   const uint32_t a_addr = smem_u32(sA), b_addr = smem_u32(sB);
   uint32_t phase = 0;
 
+  n = io.rows(n);  // an IO may hold its row count in device memory (the same for every thread)
   for (uint32_t tile = blockIdx.x; (size_t)tile * TILE_M < n; tile += gridDim.x) {
     const uint32_t i = tile * TILE_M + tid;
     const bool valid = i < n;
@@ -401,6 +402,7 @@ struct ArrayIO {
     for (int q = 0; q < NIN; ++q) x[q] = feats[(size_t)i * NIN + q];
   }
   __device__ __forceinline__ void store(uint32_t i, float t) const { out[i] = t; }
+  __device__ __forceinline__ uint32_t rows(uint32_t n) const { return n; }
 };
 
 }  // namespace mlp

@@ -95,6 +95,7 @@ struct CondSeedIO {
     const double r = radius[i];
     seed[i] = r * r * exp((double)t);
   }
+  __device__ __forceinline__ uint32_t rows(uint32_t n) const { return n; }
 };
 
 }  // namespace
@@ -1240,17 +1241,6 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       StageMark mc(x, 3);
       k_b_thermo<<<gg, 256, 0, s>>>(d, b);
       x->launches += 1;
-      if (d.p.nr_seed == CLEO_NRSEED_MLP) {  // surrogate seeds into b.dm (read by pass A / B)
-        mlp::Infer w;
-        if (cleo_mlp_infer_view(x->mlp, &w) != CLEO_OK) return CLEO_ERR_MLP;
-        w.err = reinterpret_cast<uint32_t*>(&d.err->code);
-        const SdmSeedIO io{d.sd.gbx, d.sd.r, d.sd.msol, d.temp, d.press, b.th_s, d.p.cond_delt,
-                           d.ngbxs, d.counters, b.dm};
-        const uint32_t tiles = (d.capacity + mlp::TILE_M - 1) / mlp::TILE_M;
-        mlp::k_mlp_tc<SdmSeedIO><<<tiles < 148u * 4u ? tiles : 148u * 4u, 128, mlp::TC_SMEM, s>>>(
-            w, io, d.capacity);
-        x->launches += 1;
-      }
       if (x->cfg.cond_minb == 4)
         k_cond_a<4><<<grid_for(d.capacity, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
       else
@@ -1258,6 +1248,18 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       x->launches += 1;
       const int where = radix_pairs(x, b.lkeys, b.lvals, x->keys[1], x->vals[1], b.ctr, 16);
       if (where != 0) return CLEO_ERR_CUDA;  // 16 key bits: two passes, result back in place
+      if (d.p.nr_seed == CLEO_NRSEED_MLP) {
+        // the surrogate seeds only the solves pass A left unconverged (its list), in b.dm
+        mlp::Infer w;
+        if (cleo_mlp_infer_view(x->mlp, &w) != CLEO_OK) return CLEO_ERR_MLP;
+        w.err = reinterpret_cast<uint32_t*>(&d.err->code);
+        const SdmListSeedIO io{d.sd.gbx, d.sd.r,  d.sd.msol, d.temp, d.press, b.th_s,
+                               d.p.cond_delt, b.lvals, b.ctr, b.dm};
+        const uint32_t tiles = (d.capacity + mlp::TILE_M - 1) / mlp::TILE_M;
+        mlp::k_mlp_tc<SdmListSeedIO><<<tiles < 148u * 4u ? tiles : 148u * 4u, 128, mlp::TC_SMEM,
+                                       s>>>(w, io, d.capacity);
+        x->launches += 1;
+      }
       k_cond_b<<<x->grid_flat * 2, 256, 0, s>>>(d, b);
       x->launches += 1;
     }
