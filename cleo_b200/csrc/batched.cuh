@@ -74,7 +74,7 @@ __global__ void k_b_qcond(DevCtx c) {
 // ---- per-gridbox thermodynamics of superdroplets_change (condensation.cpp:43-59) ----
 __global__ void k_b_thermo(DevCtx c, BatchScratch b) {
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x) {
-    if (g == 0) b.ctr[0] = 0;
+    if (g == 0) b.ctr[0] = b.ctr[7] = 0;  // deferred solves, of which restarts
     if (c.gcount[g] == 0) continue;
     const Where w{c.err, g, c.gstart[g]};
     const double temp = c.temp[g];
@@ -84,8 +84,9 @@ __global__ void k_b_thermo(DevCtx c, BatchScratch b) {
   }
 }
 
-// the surrogate's IO for the batched schedule: row j is the j-th solve of pass A's list of
-// unconverged and sub-stepping solves (b.lvals, count b.ctr[0]); the seed r^2 goes to b.dm of that
+// the surrogate's IO for the batched schedule: row j is the j-th solve of pass A's sorted list,
+// whose first b.ctr[7] entries are the direct solves that two iterations did not settle (key 0;
+// the sub-stepping solves after them cannot use a seed); the seed r^2 goes to b.dm of that
 // droplet, which pass B reads (and then overwrites with the droplet's condensed mass)
 struct SdmListSeedIO {
   const uint32_t* gbx;
@@ -146,7 +147,10 @@ k_cond_a(DevCtx c, BatchScratch b) {
           bool conv = false;
           GEval e = eval_g(o, p.cond_delt, r, z0);
           e = nr_iterate(cfg, o, p.cond_delt, r, e, conv, ni);
+          const bool conv1 = conv;
+          const double z1 = e.z;
           e = nr_iterate(cfg, o, p.cond_delt, r, e, conv, ni);
+          if (!conv) b.zres[i] = conv1 ? -z1 : e.z;  // where pass B's restart continues
           if (conv) {
             const double rnew = fmax(sqrt(e.z), dryradius(msol));  // change_radius
             b.dm[i] = (condensate_mass(rnew, msol, w) - condensate_mass(r, msol, w)) *
@@ -163,6 +167,10 @@ k_cond_a(DevCtx c, BatchScratch b) {
       }
     }
     const uint32_t pos = warp_append(&b.ctr[0], defer);
+    {  // restarts (key 0) lead the sorted list; their number bounds the surrogate's rows
+      const unsigned rm = __ballot_sync(0xFFFFFFFFu, defer && key == 0u);
+      if (rm && (threadIdx.x & 31) == (unsigned)(__ffs(rm) - 1)) atomicAdd(&b.ctr[7], __popc(rm));
+    }
     if (defer) {
       b.lkeys[pos] = key;
       b.lvals[pos] = i;
@@ -185,8 +193,32 @@ k_cond_b(DevCtx c, BatchScratch b) {
     kohler_factors(msol, c.temp[g], akoh, bkoh);
     uint32_t ni = 0;
     const double seed = p.nr_seed == CLEO_NRSEED_MLP ? b.dm[i] : 0.0;
-    const double newr = solve_condensation(cfg, p.cond_delt, p.cond_minsubdelt, b.th_s[g], akoh,
-                                           bkoh, b.th_ff[g], r, seed, ni, w);
+    double newr;
+    if (b.lkeys[j] == 0u && cfg.maxniters >= 2) {
+      // a direct solve whose two iterations in pass A did not converge: the restart continues
+      // from them (resume_restart), unless the surrogate's seed converges first
+      const double ffactor_fv = b.th_ff[g] / ventilation_factor(r);
+      const OdeConsts o{b.th_s[g], akoh, bkoh, ffactor_fv};
+      ni = 2;
+      double rsqrd = 0.0;
+      bool done = false;
+      if (seed_ok(seed)) {
+        const double z0 = initialguess(o, r);
+        const bool ucrit1 = first_unique_criteria(o, r, z0);
+        const GEval e0 = eval_g(o, p.cond_delt, r, z0);
+        const GEval es = eval_g(o, p.cond_delt, r, seed);
+        done = fabs(es.g) < fabs(e0.g) && integrate_seeded(cfg, o, p.cond_delt, r, es, ni, rsqrd) &&
+               seeded_root_ok(o, ucrit1, rsqrd);
+      }
+      if (!done) {
+        const int code = resume_restart(cfg, o, p.cond_delt, r, b.zres[i], ni, rsqrd);
+        if (code) w.fail(code);
+      }
+      newr = sqrt(rsqrd);
+    } else {
+      newr = solve_condensation(cfg, p.cond_delt, p.cond_minsubdelt, b.th_s[g], akoh, bkoh,
+                                b.th_ff[g], r, seed, ni, w);
+    }
     const double rnew = fmax(newr, dryradius(msol));
     b.dm[i] = (condensate_mass(rnew, msol, w) - condensate_mass(r, msol, w)) * (double)c.sd.xi[i];
     b.its[i] = ni;

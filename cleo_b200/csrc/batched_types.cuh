@@ -18,6 +18,7 @@ struct BatchScratch {
   double* th_ff;     // per gridbox diffusion factor
   double* dm;        // per superdroplet condensed mass x xi
   uint32_t* its;     // per superdroplet Newton iterations
+  double* zres;      // per deferred direct solve: pass A's iterate that pass B resumes from
   uint32_t* lkeys;   // cost keys of deferred solves
   uint32_t* lvals;   // positions of deferred solves
   uint32_t* bucket;  // [3][ngbxs] gridbox lists per size bucket

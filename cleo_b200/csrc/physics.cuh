@@ -567,6 +567,40 @@ __device__ __forceinline__ int integrate_ode_core(const NewtonCfg& c, const OdeC
   z = e.z;
   return code;
 }
+// The restart of integrate_ode_core (newtonraphson_untilconverged from the initial guess,
+// impliciteuler.cpp:131-132, 207-227) when the two iterations before it have already been done:
+// the restart's first two iterations repeat them exactly, so it can continue from them. zres is
+// -z1 when the first iteration passed the convergence test (the restart stops after it) and z2
+// otherwise (the second did not pass it, or there would be no restart). Adds the restart's
+// iterations, the repeated ones included, to niters; needs maxniters >= 2.
+__device__ __forceinline__ int resume_restart(const NewtonCfg& c, const OdeConsts& o,
+                                              double subdelt, double rprev, double zres,
+                                              uint32_t& niters, double& z) {
+  if (zres < 0.0) {
+    niters += 1;
+    z = -zres;
+    return 0;
+  }
+  niters += 2;
+  GEval e = eval_g(o, subdelt, rprev, zres);
+  bool conv = false;
+  uint32_t niter = 3;
+  int code = 0;
+  while (!conv) {
+    if (niter > c.maxniters) {
+      code = CLEO_ERR_NR_NOCONVERGE;
+      break;
+    }
+    if (niters >= NR_ITER_CAP) {
+      code = CLEO_ERR_TIMEOUT;
+      break;
+    }
+    e = nr_iterate(c, o, subdelt, rprev, e, conv, niters);
+    niter += 1;
+  }
+  z = e.z;
+  return code;
+}
 __device__ __forceinline__ double integrate_ode(const NewtonCfg& c, const OdeConsts& o,
                                                 double subdelt, double rprev, const GEval& e0,
                                                 uint32_t& niters, const Where& w) {

@@ -1249,12 +1249,12 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       const int where = radix_pairs(x, b.lkeys, b.lvals, x->keys[1], x->vals[1], b.ctr, 16);
       if (where != 0) return CLEO_ERR_CUDA;  // 16 key bits: two passes, result back in place
       if (d.p.nr_seed == CLEO_NRSEED_MLP) {
-        // the surrogate seeds only the solves pass A left unconverged (its list), in b.dm
+        // the surrogate seeds only the direct solves pass A left unconverged, in b.dm
         mlp::Infer w;
         if (cleo_mlp_infer_view(x->mlp, &w) != CLEO_OK) return CLEO_ERR_MLP;
         w.err = reinterpret_cast<uint32_t*>(&d.err->code);
         const SdmListSeedIO io{d.sd.gbx, d.sd.r,  d.sd.msol, d.temp, d.press, b.th_s,
-                               d.p.cond_delt, b.lvals, b.ctr, b.dm};
+                               d.p.cond_delt, b.lvals, b.ctr + 7, b.dm};
         const uint32_t tiles = (d.capacity + mlp::TILE_M - 1) / mlp::TILE_M;
         mlp::k_mlp_tc<SdmListSeedIO><<<tiles < 148u * 4u ? tiles : 148u * 4u, 128, mlp::TC_SMEM,
                                        s>>>(w, io, d.capacity);
@@ -1538,6 +1538,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &x->bs.th_ff, ng);
   rc |= dalloc(x, &x->bs.dm, cap);
   rc |= dalloc(x, &x->bs.its, cap);
+  rc |= dalloc(x, &x->bs.zres, cap);
   rc |= dalloc(x, &x->bs.lkeys, cap);
   rc |= dalloc(x, &x->bs.lvals, cap);
   rc |= dalloc(x, &x->bs.bucket, 3 * ng);
