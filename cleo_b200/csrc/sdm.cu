@@ -171,11 +171,13 @@ struct cleo_b200_ctx {
   struct CsScratch {
     size_t cap = 0;
     uint32_t *k0 = nullptr, *v0 = nullptr, *k1 = nullptr, *v1 = nullptr;
-    uint32_t *hist = nullptr, *tsums = nullptr, *ctr = nullptr;
+    uint32_t *hist = nullptr, *tsums = nullptr, *ctr = nullptr;  // ctr: deferred solves
+    double* zres = nullptr;  // pass A's iterates of the restarts
     uint32_t nt = 0;
   } cs;
   void free_cs() {
     for (uint32_t* q : {cs.k0, cs.v0, cs.k1, cs.v1, cs.hist, cs.tsums, cs.ctr}) cudaFree(q);
+    cudaFree(cs.zres);
     cs = CsScratch();
   }
   cudaEvent_t take_event() {
@@ -967,12 +969,13 @@ __device__ __forceinline__ uint32_t cs_warp_append(uint32_t* ctr, bool flag) {
   base = __shfl_sync(0xFFFFFFFFu, base, 0);
   return base + __popc(m & ((1u << lane) - 1u));
 }
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256)
 k_cs_a(DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __restrict__ msol,
        const double* __restrict__ temp, const double* __restrict__ press,
        const double* __restrict__ s_ratio, const double* __restrict__ delt,
        double* __restrict__ seeds, double* __restrict__ out, uint32_t* __restrict__ niters_out,
-       uint32_t* __restrict__ lkeys, uint32_t* __restrict__ lvals, uint32_t* __restrict__ ctr) {
+       double* __restrict__ zres, uint32_t* __restrict__ lkeys, uint32_t* __restrict__ lvals,
+       uint32_t* __restrict__ ctr) {
   const NewtonCfg cfg{c.p.maxniters, c.p.rtol, c.p.atol};
   for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
     const uint32_t i = i0 + threadIdx.x;
@@ -991,9 +994,10 @@ k_cs_a(DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __
       const double crit = ucrit1 ? 0.0 : critical_timestep(o);
       uint32_t ni = 0, carried = 0;
       if (ucrit1 || dt <= crit) {
-        bool conv = false, seeded = false;
+        bool conv = false, seeded = false, conv1 = false;
+        double z1 = 0.0;
         GEval e = eval_g(o, dt, r, z0);
-        if (seeds && seed_ok(seeds[i])) {
+        if (seeds && seed_ok(seeds[i])) {  // the surrogate's seed, when its residual is smaller
           const GEval es = eval_g(o, dt, r, seeds[i]);
           if (fabs(es.g) < fabs(e.g)) {
             double zs;
@@ -1008,13 +1012,17 @@ k_cs_a(DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __
         }
         if (!seeded) {
           e = nr_iterate(cfg, o, dt, r, e, conv, ni);
+          conv1 = conv;
+          z1 = e.z;
           e = nr_iterate(cfg, o, dt, r, e, conv, ni);
         }
         if (conv) {
           out[i] = fmax(sqrt(e.z), dryradius(msol[i]));
           if (niters_out) niters_out[i] = ni;
         } else {
-          defer = true;  // restart until converged (impliciteuler.cpp:136-140)
+          defer = true;  // restart until converged (impliciteuler.cpp:136-140), key 0
+          // where pass B's restart continues; NaN after an abandoned seed (a full solve)
+          zres[i] = seeded ? __longlong_as_double(0x7FF8000000000000ll) : (conv1 ? -z1 : e.z);
         }
       } else {
         defer = true;
@@ -1034,22 +1042,36 @@ k_cs_b(DevCtx c, const double* __restrict__ radius, const double* __restrict__ m
        const double* __restrict__ temp, const double* __restrict__ press,
        const double* __restrict__ s_ratio, const double* __restrict__ delt,
        const double* __restrict__ seeds, double* __restrict__ out,
-       uint32_t* __restrict__ niters_out, const uint32_t* __restrict__ lvals,
+       uint32_t* __restrict__ niters_out, const double* __restrict__ zres,
+       const uint32_t* __restrict__ lkeys, const uint32_t* __restrict__ lvals,
        const uint32_t* __restrict__ ctr) {
   const NewtonCfg cfg{c.p.maxniters, c.p.rtol, c.p.atol};
   const uint32_t nl = *ctr;
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nl; j += gridDim.x * blockDim.x) {
     const uint32_t i = lvals[j];
     const Where w{c.err, OOB, i};
-    const double T = temp[i];
+    const double T = temp[i], r = radius[i], dt = delt[i];
     const double psat = saturation_pressure(T, w);
     const double ffactor = diffusion_factor(press[i], T, psat);
     double akoh, bkoh;
     kohler_factors(msol[i], T, akoh, bkoh);
     uint32_t ni = 0;
-    const double newr = solve_condensation(cfg, delt[i], c.p.cond_minsubdelt, s_ratio[i], akoh,
-                                           bkoh, ffactor, radius[i], seeds ? seeds[i] : 0.0, ni,
-                                           w);
+    double newr;
+    const double zr = lkeys[j] == 0u ? zres[i] : 0.0;
+    if (lkeys[j] == 0u && cfg.maxniters >= 2 && zr == zr) {
+      // a direct solve whose two reference iterations in pass A did not converge: the restart
+      // continues from them (resume_restart)
+      const OdeConsts o{s_ratio[i], akoh, bkoh, ffactor / ventilation_factor(r)};
+      ni = 2;
+      double rsqrd = 0.0;
+      const int code = resume_restart(cfg, o, dt, r, zr, ni, rsqrd);
+      if (code) w.fail(code);
+      newr = sqrt(rsqrd);
+    } else {
+      const double seed = seeds ? seeds[i] : 0.0;
+      newr = solve_condensation(cfg, dt, c.p.cond_minsubdelt, s_ratio[i], akoh, bkoh, ffactor, r,
+                                seed, ni, w);
+    }
     out[i] = fmax(newr, dryradius(msol[i]));
     if (niters_out) niters_out[i] += ni;
   }
@@ -2073,9 +2095,10 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_rad
     return CLEO_ERR_ARGUMENT;
   if (n >= 0xFFFFFFFFull) return CLEO_ERR_CAPACITY;
   if (n == 0) return CLEO_OK;
-  const double* seeds = nullptr;
-  if (x->d.p.nr_seed == CLEO_NRSEED_MLP) {
-    mlp::Infer w;
+  const bool seeded = x->d.p.nr_seed == CLEO_NRSEED_MLP;
+  const bool batched = x->d.p.exec_mode == CLEO_EXEC_BATCHED;
+  mlp::Infer w;
+  if (seeded) {
     if (cleo_mlp_infer_view(x->mlp, &w) != CLEO_OK) return CLEO_ERR_MLP;
     if (n > x->seed_cap) {
       CUDA_TRY(cudaStreamSynchronize(x->stream));
@@ -2086,14 +2109,19 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_rad
       x->seed_cap = n;
     }
     w.err = reinterpret_cast<uint32_t*>(&x->d.err->code);
-    const CondSeedIO io{d_radius, d_msol, d_temp, d_press, d_s_ratio, d_delt, x->seed_buf};
-    const uint32_t tiles = (uint32_t)((n + mlp::TILE_M - 1) / mlp::TILE_M);
-    mlp::k_mlp_tc<CondSeedIO><<<tiles < 148u * 4u ? tiles : 148u * 4u, 128, mlp::TC_SMEM,
-                                x->stream>>>(w, io, (uint32_t)n);
-    x->launches += 1;
-    seeds = x->seed_buf;
   }
-  if (x->d.p.exec_mode != CLEO_EXEC_BATCHED) {
+  const uint32_t tiles = (uint32_t)((n + mlp::TILE_M - 1) / mlp::TILE_M);
+  const uint32_t tc_grid = tiles < 148u * 4u ? tiles : 148u * 4u;
+  const double* seeds = seeded ? x->seed_buf : nullptr;
+  // every solve seeded up front: most direct solves of independent droplets need more than the
+  // two iterations of pass A, so the seed saves them (the batched SDM step instead seeds only the
+  // solves that two iterations did not settle)
+  if (seeded) {
+    const CondSeedIO io{d_radius, d_msol, d_temp, d_press, d_s_ratio, d_delt, x->seed_buf};
+    mlp::k_mlp_tc<CondSeedIO><<<tc_grid, 128, mlp::TC_SMEM, x->stream>>>(w, io, (uint32_t)n);
+    x->launches += 1;
+  }
+  if (!batched) {
     k_condsolve<<<grid_for(n, 128), 128, 0, x->stream>>>(x->d, (uint32_t)n, d_radius, d_msol,
                                                          d_temp, d_press, d_s_ratio, d_delt,
                                                          seeds, d_radius_out, d_niters_out);
@@ -2115,6 +2143,7 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_rad
     ok = ok && cudaMalloc(&cs.hist, nh * sizeof(uint32_t)) == cudaSuccess;
     ok = ok && cudaMalloc(&cs.tsums, nsums * sizeof(uint32_t)) == cudaSuccess;
     ok = ok && cudaMalloc(&cs.ctr, sizeof(uint32_t)) == cudaSuccess;
+    ok = ok && cudaMalloc(&cs.zres, n * sizeof(double)) == cudaSuccess;
     if (!ok) {
       x->free_cs();
       cudaGetLastError();
@@ -2126,14 +2155,14 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_rad
   CUDA_TRY(cudaMemsetAsync(cs.ctr, 0, sizeof(uint32_t), x->stream));
   k_cs_a<<<grid_for(n, 256), 256, 0, x->stream>>>(
       x->d, (uint32_t)n, d_radius, d_msol, d_temp, d_press, d_s_ratio, d_delt,
-      seeds ? x->seed_buf : nullptr, d_radius_out, d_niters_out, cs.k0, cs.v0, cs.ctr);
+      seeded ? x->seed_buf : nullptr, d_radius_out, d_niters_out, cs.zres, cs.k0, cs.v0, cs.ctr);
   x->launches += 1;
   const int where = radix_pairs_on(x, cs.k0, cs.v0, cs.k1, cs.v1, cs.ctr, 16, cs.hist, cs.tsums,
                                    cs.nt);
   if (where != 0) return CLEO_ERR_CUDA;  // two 8-bit passes leave the result in (k0, v0)
   k_cs_b<<<x->grid_flat * 2, 256, 0, x->stream>>>(x->d, d_radius, d_msol, d_temp, d_press,
                                                   d_s_ratio, d_delt, seeds, d_radius_out,
-                                                  d_niters_out, cs.v0, cs.ctr);
+                                                  d_niters_out, cs.zres, cs.k0, cs.v0, cs.ctr);
   x->launches += 1;
   CUDA_TRY(cudaGetLastError());
   return CLEO_OK;
