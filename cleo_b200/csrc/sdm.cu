@@ -139,7 +139,8 @@ struct cleo_b200_ctx {
   // autotuner that chooses it by timing candidates on live steps
   struct TuneCfg {
     int cond_block;       // threads per block of pass A
-    int cond_minb;        // pass-A variant: resident 256-thread CTAs per SM it is compiled for
+    int cond_minb;        // pass-A variant (3, 4 or 5): resident 256-thread CTAs per SM it is
+                          // compiled for
     uint32_t small_max;   // gridboxes up to this size go to the warp kernel
     int small_minb;       // warp-kernel variant: resident CTAs per SM it is compiled for
   };
@@ -1263,7 +1264,9 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       StageMark mc(x, 3);
       k_b_thermo<<<gg, 256, 0, s>>>(d, b);
       x->launches += 1;
-      if (x->cfg.cond_minb == 4)
+      if (x->cfg.cond_minb == 5)
+        k_cond_a<5><<<grid_for(d.capacity, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
+      else if (x->cfg.cond_minb == 4)
         k_cond_a<4><<<grid_for(d.capacity, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
       else
         k_cond_a<3><<<grid_for(d.capacity, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
@@ -1381,7 +1384,7 @@ std::mutex g_tune_mutex;
 std::map<std::string, cleo_b200_ctx::TuneCfg> g_tune_cache;
 
 const cleo_b200_ctx::TuneCfg COND_OPTS[4] = {
-    {128, 3, 0, 0}, {256, 3, 0, 0}, {128, 4, 0, 0}, {256, 4, 0, 0}};
+    {128, 4, 0, 0}, {256, 4, 0, 0}, {128, 5, 0, 0}, {256, 5, 0, 0}};
 const cleo_b200_ctx::TuneCfg COLL_OPTS[4] = {
     {0, 0, SMALL_MAX, 2}, {0, 0, WARP_MAX, 2}, {0, 0, SMALL_MAX, 3}, {0, 0, WARP_MAX, 3}};
 
@@ -1850,7 +1853,7 @@ int cleo_b200_tuned_config(cleo_b200_ctx* x, int32_t cfg[4]) {
 
 int cleo_b200_set_launch_config(cleo_b200_ctx* x, const int32_t cfg[4]) {
   if (!x || !cfg) return CLEO_ERR_ARGUMENT;
-  if ((cfg[0] != 128 && cfg[0] != 256) || (cfg[1] != 3 && cfg[1] != 4) || cfg[2] < 1 ||
+  if ((cfg[0] != 128 && cfg[0] != 256) || cfg[1] < 3 || cfg[1] > 5 || cfg[2] < 1 ||
       cfg[2] > (int32_t)WARP_MAX || (cfg[3] != 2 && cfg[3] != 3))
     return CLEO_ERR_ARGUMENT;
   CUDA_TRY(cudaStreamSynchronize(x->stream));

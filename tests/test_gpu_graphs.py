@@ -82,8 +82,8 @@ def test_autotune_keeps_results_and_picks_a_candidate(lib):
         assert rc == (1 if k < 7 else 0)
     tuned.check()
     K.assert_same_domain(tuned.download_supers(), plain.download_supers(), rtol=0.0, what="tuned")
-    assert cfg[0] in (128, 256) and cfg[1] in (3, 4)
-    assert cfg[2] in (32, 64) and cfg[3] in (2, 3)
+    assert cfg[0] in (128, 256) and cfg[1] in (4, 5)
+    assert cfg[2] in (64, 128) and cfg[3] in (2, 3)
     # plain schedule: nothing to tune
     w["params"].exec_mode = abi.EXEC_PLAIN
     p = make_sdm(w, lib=lib)
@@ -91,7 +91,7 @@ def test_autotune_keeps_results_and_picks_a_candidate(lib):
 
 
 @pytest.mark.parametrize("cfg", [(256, 3, 64, 2), (128, 4, 128, 2), (256, 4, 128, 3),
-                                 (128, 3, 20, 3)])
+                                 (128, 5, 20, 3), (256, 5, 64, 2)])
 def test_launch_configs_match_oracle(lib, cfg):
     """Every launch configuration the autotuner can choose (and an arbitrary warp-kernel limit)
     gives the oracle's results; the workload has gridboxes on both sides of 64 and 128."""
