@@ -250,13 +250,15 @@ def measure(lib, wl, mode, steps, warmup, dist, local, e2e=False, surrogate=None
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
+        # the states of each step are uploaded on the context's copy stream while the previous
+        # step runs (cleo_b200_upload_state_async), the budgets copied back behind each step
         for _ in range(steps):
-            assert lib.cleo_b200_upload_state(ctx, C.byref(st_struct)) == 0
+            assert lib.cleo_b200_upload_state_async(ctx, C.byref(st_struct)) == 0
             sdm.run_step(t * 100, (t + 1) * 100)
             t += 1
-            assert lib.cleo_b200_download_budgets(
-                ctx, C.cast(cm_out.data_ptr(), C.POINTER(C.c_double)),
-                C.cast(it_out.data_ptr(), C.POINTER(C.c_uint64))) == 0
+            assert lib.cleo_b200_download_budgets_async(
+                ctx, C.c_void_p(cm_out.data_ptr()), C.c_void_p(it_out.data_ptr())) == 0
+        assert lib.cleo_b200_synchronize(ctx) == 0
         e1.record(stream)
         e1.synchronize()
         barrier()

@@ -118,6 +118,12 @@ struct cleo_b200_ctx {
   uint32_t* h_motion = nullptr;
   uint32_t* d_motion = nullptr;
   bool sort_full = false;
+  // asynchronous state upload (cleo_b200_upload_state_async): staging area for the 11 state
+  // fields, a copy stream, and events for "copied" and "taken by a step"
+  double* stage_state = nullptr;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_uploaded = nullptr, ev_consumed = nullptr;
+  bool upload_pending = false, consumed_recorded = false;
   // superdroplet output staging (allocated at the first gather): converted fields, offsets
   uint8_t* obs_stage = nullptr;
   uint32_t *obs_start = nullptr, *obs_tsums = nullptr;
@@ -1710,6 +1716,12 @@ void cleo_b200_destroy(cleo_b200_ctx* x) {
   x->drop_graphs();
   cudaFree(x->seed_buf);
   x->free_cs();
+  if (x->copy_stream) {
+    cudaStreamSynchronize(x->copy_stream);
+    cudaStreamDestroy(x->copy_stream);
+  }
+  if (x->ev_uploaded) cudaEventDestroy(x->ev_uploaded);
+  if (x->ev_consumed) cudaEventDestroy(x->ev_consumed);
   for (void* p : x->allocs) cudaFree(p);
   if (x->h_motion) cudaFreeHost(x->h_motion);
   if (x->own_stream && x->stream) cudaStreamDestroy(x->stream);
@@ -1783,6 +1795,10 @@ int cleo_b200_upload_supers(cleo_b200_ctx* x, const cleo_b200_supers* h, size_t 
 
 int cleo_b200_upload_state(cleo_b200_ctx* x, const cleo_b200_gbx_state* h) {
   if (!x || !h) return CLEO_ERR_ARGUMENT;
+  if (x->upload_pending) {  // these states replace the staged ones
+    CUDA_TRY(cudaStreamSynchronize(x->copy_stream));
+    x->upload_pending = false;
+  }
   const size_t ng = x->d.ngbxs;
   const double* src[11] = {h->volume, h->press, h->temp, h->qvap, h->qcond, h->wvel_lo,
                            h->wvel_hi, h->uvel_lo, h->uvel_hi, h->vvel_lo, h->vvel_hi};
@@ -1796,10 +1812,73 @@ int cleo_b200_upload_state(cleo_b200_ctx* x, const cleo_b200_gbx_state* h) {
   return CLEO_OK;
 }
 
+int cleo_b200_upload_state_async(cleo_b200_ctx* x, const cleo_b200_gbx_state* h) {
+  if (!x || !h) return CLEO_ERR_ARGUMENT;
+  const size_t ng = x->d.ngbxs;
+  const double* src[11] = {h->volume, h->press, h->temp, h->qvap, h->qcond, h->wvel_lo,
+                           h->wvel_hi, h->uvel_lo, h->uvel_hi, h->vvel_lo, h->vvel_hi};
+  for (int k = 0; k < 11; ++k)
+    if (!src[k]) return CLEO_ERR_ARGUMENT;
+  if (!x->stage_state) {  // first use: staging area, copy stream, events
+    if (dalloc(x, &x->stage_state, 11 * (ng ? ng : 1))) return CLEO_ERR_CUDA;
+    CUDA_TRY(cudaStreamCreateWithFlags(&x->copy_stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&x->ev_uploaded, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&x->ev_consumed, cudaEventDisableTiming));
+  }
+  // the staging area is free once the previous step has taken its states
+  if (x->consumed_recorded) CUDA_TRY(cudaStreamWaitEvent(x->copy_stream, x->ev_consumed, 0));
+  for (int k = 0; k < 11; ++k)
+    CUDA_TRY(cudaMemcpyAsync(x->stage_state + (size_t)k * ng, src[k], ng * 8,
+                             cudaMemcpyHostToDevice, x->copy_stream));
+  CUDA_TRY(cudaEventRecord(x->ev_uploaded, x->copy_stream));
+  x->upload_pending = true;
+  return CLEO_OK;
+}
+
+int cleo_b200_download_budgets_async(cleo_b200_ctx* x, double* cond_mass, uint64_t* nr_iters) {
+  if (!x) return CLEO_ERR_ARGUMENT;
+  const size_t ng = x->d.ngbxs;
+  if (cond_mass)
+    CUDA_TRY(cudaMemcpyAsync(cond_mass, x->d.cond_mass, ng * 8, cudaMemcpyDeviceToHost,
+                             x->stream));
+  if (nr_iters)
+    CUDA_TRY(cudaMemcpyAsync(nr_iters, x->d.nr_iters, ng * 8, cudaMemcpyDeviceToHost,
+                             x->stream));
+  return CLEO_OK;
+}
+
+int cleo_b200_synchronize(cleo_b200_ctx* x) {
+  if (!x) return CLEO_ERR_ARGUMENT;
+  if (x->copy_stream) CUDA_TRY(cudaStreamSynchronize(x->copy_stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  return CLEO_OK;
+}
+
+// the states staged by cleo_b200_upload_state_async become the live ones (on the context's
+// stream, after the copy); returns once the host arrays have been read
+static int take_staged_state(cleo_b200_ctx* x) {
+  const size_t ng = x->d.ngbxs;
+  double* dst[11] = {x->d.volume, x->d.press, x->d.temp, x->d.qvap, x->d.qcond, x->d.wlo,
+                     x->d.whi, x->d.ulo, x->d.uhi, x->d.vlo, x->d.vhi};
+  CUDA_TRY(cudaStreamWaitEvent(x->stream, x->ev_uploaded, 0));
+  for (int k = 0; k < 11; ++k)
+    CUDA_TRY(cudaMemcpyAsync(dst[k], x->stage_state + (size_t)k * ng, ng * 8,
+                             cudaMemcpyDeviceToDevice, x->stream));
+  CUDA_TRY(cudaEventRecord(x->ev_consumed, x->stream));
+  x->consumed_recorded = true;
+  x->upload_pending = false;
+  CUDA_TRY(cudaEventSynchronize(x->ev_uploaded));
+  return CLEO_OK;
+}
+
 int cleo_b200_step(cleo_b200_ctx* x, uint32_t t_mdl, uint32_t t_next) {
   if (!x) return CLEO_ERR_ARGUMENT;
   if (x->d.p.nr_seed == CLEO_NRSEED_MLP && x->d.p.condstep != CLEO_STEP_OFF && !x->mlp)
     return CLEO_ERR_MLP;
+  if (x->upload_pending) {
+    const int rc = take_staged_state(x);
+    if (rc) return rc;
+  }
   const bool batched = x->d.p.exec_mode == CLEO_EXEC_BATCHED;
   uint32_t t_sdm = t_mdl;
   while (t_sdm < t_next) {

@@ -88,6 +88,26 @@ class SDM:
         s = abi.state_struct(arrs)
         self._check(self._f("upload_state")(self._ctx, C.byref(s)), "in upload_state")
 
+    def upload_state_async(self, st: dict):
+        """cleo_b200_upload_state_async: the states are taken by the next run_step (the arrays
+        are kept alive until then)."""
+        arrs = {f: np.ascontiguousarray(st[f], dtype=np.float64) for f in abi.STATE_FIELDS}
+        s = abi.state_struct(arrs)
+        self._check(self._f("upload_state_async")(self._ctx, C.byref(s)),
+                    "in upload_state_async")
+        self._staged = arrs
+
+    def download_budgets_async(self, cond_mass: np.ndarray, nr_iters: np.ndarray):
+        """Enqueue the budgets' copy into the given arrays (float64 and uint64 of ngbxs); they
+        hold the values after synchronize()."""
+        assert cond_mass.dtype == np.float64 and nr_iters.dtype == np.uint64
+        self._check(self._f("download_budgets_async")(
+            self._ctx, C.c_void_p(cond_mass.ctypes.data), C.c_void_p(nr_iters.ctypes.data)),
+            "in download_budgets_async")
+
+    def synchronize(self):
+        self._check(self._f("synchronize")(self._ctx), "in synchronize")
+
     def run_step(self, t_mdl: int, t_next: int):
         """SDMMethods::run_step(t_mdl, t_next): enqueue one coupling step."""
         self._check(self._f("step")(self._ctx, int(t_mdl), int(t_next)), "in step")

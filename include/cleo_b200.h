@@ -202,6 +202,20 @@ void cleo_b200_destroy(cleo_b200_ctx* ctx);
 int cleo_b200_upload_supers(cleo_b200_ctx* ctx, const cleo_b200_supers* host, size_t n);
 /* Copy ngbxs gridbox states (host SoA) into the context. */
 int cleo_b200_upload_state(cleo_b200_ctx* ctx, const cleo_b200_gbx_state* host);
+/*
+ * Asynchronous state exchange, for a host whose coupling-step states are known ahead of the
+ * step (prescribed or file-driven dynamics): cleo_b200_upload_state_async copies the states
+ * (host arrays; pinned memory lets the copy overlap) into a device staging area on a copy stream
+ * of the context, behind the previous step's use of that area, and returns at once; the next
+ * cleo_b200_step waits for the copy, makes the staged states the live ones at its start, and
+ * returns once the host arrays have been read (they may be refilled after it returns). An
+ * upload_state (synchronous) in between replaces the staged states. The budgets' copy to the host
+ * (cleo_b200_download_budgets_async) is enqueued after the work so far; its arrays hold the
+ * values once cleo_b200_synchronize has returned. Results are those of the synchronous calls.
+ */
+int cleo_b200_upload_state_async(cleo_b200_ctx* ctx, const cleo_b200_gbx_state* h);
+int cleo_b200_download_budgets_async(cleo_b200_ctx* ctx, double* cond_mass, uint64_t* nr_iters);
+int cleo_b200_synchronize(cleo_b200_ctx* ctx);
 
 /*
  * Advance the domain from model step t_mdl to t_next: motion + sort, then microphysics

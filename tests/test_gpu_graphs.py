@@ -113,3 +113,47 @@ def test_launch_configs_match_oracle(lib, cfg):
     K.assert_same_domain(g.download_supers(), o.download_supers(), rtol=1e-12, what=str(cfg))
     bad = (C.c_int32 * 4)(256, 3, 129, 2)
     assert lib.cleo_b200_set_launch_config(g.ctx, bad) == abi.CODE["CLEO_ERR_ARGUMENT"]
+
+
+def test_async_state_upload_matches_sync(lib):
+    """States uploaded asynchronously (copy stream, taken at the next step's start) and budgets
+    copied back asynchronously give the synchronous calls' results, with states that change
+    every step."""
+    w = _workload("uniform")
+    ts = w["tstep"]
+    rng = np.random.default_rng(3)
+    states = []
+    for _ in range(5):
+        st = {f: w["state"][f].copy() for f in abi.STATE_FIELDS}
+        st["temp"] = st["temp"] * (1.0 + 2e-3 * rng.standard_normal(st["temp"].size))
+        st["qvap"] = st["qvap"] * (1.0 + 5e-3 * rng.standard_normal(st["qvap"].size))
+        states.append(st)
+    a, b = make_sdm(w, lib=lib), make_sdm(w, lib=lib)
+    ng = w["grid"]["ngbxs"]
+    bud_a, bud_b = [], []
+    for k in range(5):
+        a.upload_state(states[k])
+        a.run_step(k * ts, (k + 1) * ts)
+        bud_a.append(a.download_budgets())
+    for k in range(5):
+        b.upload_state_async(states[k])
+        b.run_step(k * ts, (k + 1) * ts)
+        cm, it = np.zeros(ng), np.zeros(ng, dtype=np.uint64)
+        b.download_budgets_async(cm, it)
+        bud_b.append((cm, it))
+    b.synchronize()
+    for (ca, ia), (cb, ib) in zip(bud_a, bud_b):
+        assert np.array_equal(ca, cb) and np.array_equal(ia, ib)
+    K.assert_same_domain(a.download_supers(), b.download_supers(), rtol=0.0, what="async")
+    sa, sb = a.download_state(), b.download_state()
+    for f in abi.STATE_FIELDS:
+        assert np.array_equal(sa[f], sb[f]), f
+    # a synchronous upload replaces states staged but not yet taken
+    b.upload_state_async(states[0])
+    b.upload_state(states[4])
+    a.upload_state(states[4])
+    a.run_step(5 * ts, 6 * ts)
+    b.run_step(5 * ts, 6 * ts)
+    K.assert_same_domain(a.download_supers(), b.download_supers(), rtol=0.0, what="replaced")
+    a.check()
+    b.check()
