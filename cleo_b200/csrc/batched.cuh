@@ -144,12 +144,17 @@ k_cond_a(DevCtx c, BatchScratch b) {
         const double crit = ucrit1 ? 0.0 : critical_timestep(o);
         uint32_t ni = 0;
         if (ucrit1 || p.cond_delt <= crit) {
-          bool conv = false;
+          bool conv = false, conv1 = false;
+          double z1 = 0.0;
           GEval e = eval_g(o, p.cond_delt, r, z0);
-          e = nr_iterate(cfg, o, p.cond_delt, r, e, conv, ni);
-          const bool conv1 = conv;
-          const double z1 = e.z;
-          e = nr_iterate(cfg, o, p.cond_delt, r, e, conv, ni);
+#pragma unroll 1
+          for (int it = 0; it < 2; ++it) {  // one copy of the iteration: a smaller hot loop
+            e = nr_iterate(cfg, o, p.cond_delt, r, e, conv, ni);
+            if (it == 0) {
+              conv1 = conv;
+              z1 = e.z;
+            }
+          }
           if (!conv) b.zres[i] = conv1 ? -z1 : e.z;  // where pass B's restart continues
           if (conv) {
             const double rnew = fmax(sqrt(e.z), dryradius(msol));  // change_radius
@@ -184,7 +189,11 @@ k_cond_b(DevCtx c, BatchScratch b) {
   const cleo_b200_params& p = c.p;
   const uint32_t nl = b.ctr[0];
   const NewtonCfg cfg{p.maxniters, p.rtol, p.atol};
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nl; j += gridDim.x * blockDim.x) {
+  for (uint32_t jr = blockIdx.x * blockDim.x + threadIdx.x; jr < nl;
+       jr += gridDim.x * blockDim.x) {
+    // the list is sorted by ascending cost: the most expensive solves start first, so that the
+    // longest sub-stepping ones do not run alone at the end
+    const uint32_t j = nl - 1 - jr;
     const uint32_t i = b.lvals[j];
     const uint32_t g = c.sd.gbx[i];
     const Where w{c.err, g, i};

@@ -1054,7 +1054,9 @@ k_cs_b(DevCtx c, const double* __restrict__ radius, const double* __restrict__ m
        const uint32_t* __restrict__ ctr) {
   const NewtonCfg cfg{c.p.maxniters, c.p.rtol, c.p.atol};
   const uint32_t nl = *ctr;
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nl; j += gridDim.x * blockDim.x) {
+  for (uint32_t jr = blockIdx.x * blockDim.x + threadIdx.x; jr < nl;
+       jr += gridDim.x * blockDim.x) {
+    const uint32_t j = nl - 1 - jr;  // most expensive solves first (the list is sorted by cost)
     const uint32_t i = lvals[j];
     const Where w{c.err, OOB, i};
     const double T = temp[i], r = radius[i], dt = delt[i];
