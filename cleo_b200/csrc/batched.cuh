@@ -184,7 +184,8 @@ k_cond_a(DevCtx c, BatchScratch b) {
 }
 
 // ---- pass B: the deferred solves, in order of cost ----
-__global__ void __launch_bounds__(256)
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB)
 k_cond_b(DevCtx c, BatchScratch b) {
   const cleo_b200_params& p = c.p;
   const uint32_t nl = b.ctr[0];

@@ -131,6 +131,7 @@ struct cleo_b200_ctx {
   BatchScratch bs{};              // batched-schedule scratch
   int grid_small[2][2] = {{0, 0}, {0, 0}};  // warp kernel [64 / 128 slots][2 / 3 CTAs per SM]
   int grid_medium = 0, grid_large = 0, grid_flat = 0;
+  int grid_condb[3] = {0, 0, 0};  // pass B at 3, 4, 5 resident CTAs per SM
   unsigned long long launches = 0;  // kernels launched by this context
   std::vector<void*> allocs;
   // stage timing: (stage, start, end) event triples recorded while profiling is on
@@ -1293,7 +1294,13 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
                                        s>>>(w, io, d.capacity);
         x->launches += 1;
       }
-      k_cond_b<<<x->grid_flat * 2, 256, 0, s>>>(d, b);
+      // pass B with the register budget of pass A's variant (grid: twice its resident CTAs)
+      if (x->cfg.cond_minb >= 5)
+        k_cond_b<5><<<x->grid_condb[2], 256, 0, s>>>(d, b);
+      else if (x->cfg.cond_minb == 4)
+        k_cond_b<4><<<x->grid_condb[1], 256, 0, s>>>(d, b);
+      else
+        k_cond_b<3><<<x->grid_condb[0], 256, 0, s>>>(d, b);
       x->launches += 1;
     }
     if (cond || coll) {
@@ -1693,7 +1700,13 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
     x->grid_medium = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<true>, B_THREADS, 0));
     x->grid_large = sms * (occ > 0 ? occ : 1);
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cond_b, 256, 0));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cond_b<3>, 256, 0));
+    x->grid_condb[0] = 2 * sms * (occ > 0 ? occ : 1);
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cond_b<4>, 256, 0));
+    x->grid_condb[1] = 2 * sms * (occ > 0 ? occ : 1);
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cond_b<5>, 256, 0));
+    x->grid_condb[2] = 2 * sms * (occ > 0 ? occ : 1);
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cs_b, 256, 0));
     x->grid_flat = sms * (occ > 0 ? occ : 1);
   }
   x->tune_key = tune_key(x);
