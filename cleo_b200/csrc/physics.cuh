@@ -542,15 +542,40 @@ __device__ __forceinline__ int integrate_ode_core(const NewtonCfg& c, const OdeC
                                                   double subdelt, double rprev, const GEval& e0,
                                                   uint32_t& niters, double& z) {
   bool conv = false;
-  GEval e = e0;
-  for (int it = 0; it < 2; ++it) e = nr_iterate(c, o, subdelt, rprev, e, conv, niters);
+  GEval e = nr_iterate(c, o, subdelt, rprev, e0, conv, niters);
+  const bool conv1 = conv;
+  const double z1 = e.z;
+  e = nr_iterate(c, o, subdelt, rprev, e, conv, niters);
   if (conv) {
     z = e.z;
     return 0;
   }
-  e = e0;
-  conv = false;
-  uint32_t niter = 1;
+  // the restart from e0 (newtonraphson_untilconverged): its first two iterations repeat the two
+  // above exactly, so they are taken from them, each behind the checks the restart makes before it
+  if (1 > c.maxniters) {
+    z = e0.z;
+    return CLEO_ERR_NR_NOCONVERGE;
+  }
+  if (niters >= NR_ITER_CAP) {
+    z = e0.z;
+    return CLEO_ERR_TIMEOUT;
+  }
+  niters += 1;
+  if (conv1) {
+    z = z1;
+    return 0;
+  }
+  if (2 > c.maxniters) {
+    z = z1;
+    return CLEO_ERR_NR_NOCONVERGE;
+  }
+  if (niters >= NR_ITER_CAP) {
+    z = z1;
+    return CLEO_ERR_TIMEOUT;
+  }
+  niters += 1;
+  conv = false;  // as after the second iteration above
+  uint32_t niter = 3;
   int code = 0;
   while (!conv) {
     if (niter > c.maxniters) {
