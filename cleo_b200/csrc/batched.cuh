@@ -517,12 +517,19 @@ k_b_cta(DevCtx c, BatchScratch b, int cond, int coll) {
   __shared__ unsigned long long shu[32];
   __shared__ uint32_t shw[40];
   __shared__ uint32_t s_item;
+  __shared__ uint64_t s_bar;  // completion of the medium path's bulk copies
   constexpr uint32_t PT = MEDIUM_MAX / B_THREADS;  // superdroplets per thread (medium)
+  constexpr uint32_t MBUF = MEDIUM_MAX + 2;        // staged elements per field (medium)
   const cleo_b200_params& p = c.p;
   const int tid = threadIdx.x;
   const uint32_t q_idx = LARGE ? 2 : 1;
   const uint32_t count = b.ctr[1 + q_idx];
   const uint32_t* list = b.bucket + (size_t)q_idx * c.ngbxs;
+  uint32_t bar_parity = 0;
+  if (!LARGE) {
+    if (tid == 0) mbar_init(&s_bar, 1);
+    __syncthreads();
+  }
   while (true) {
     if (tid == 0) s_item = atomicAdd(&b.ctr[4 + q_idx], 1u);
     __syncthreads();
@@ -546,21 +553,47 @@ k_b_cta(DevCtx c, BatchScratch b, int cond, int coll) {
     if (!coll) continue;
     const uint64_t key = cleo_rng_key(p.seed, t_sdm, g);
     const uint64_t slot = b.slot[g];
-    double* Sr = LARGE ? c.scr_r + base : reinterpret_cast<double*>(smem);
-    double* Sm = LARGE ? c.scr_m + base : reinterpret_cast<double*>(smem) + MEDIUM_MAX;
+    // medium: r, msol, xi staged in shared memory by bulk copies (TMA) from the even element at
+    // or below the gridbox's first superdroplet (16-byte alignment; the SoA arrays' padding
+    // covers the element a copy may read past the range); large: global scratch
+    const uint32_t off = base & 1u;
+    double* Sr = LARGE ? c.scr_r + base : reinterpret_cast<double*>(smem) + off;
+    double* Sm = LARGE ? c.scr_m + base : reinterpret_cast<double*>(smem) + MBUF + off;
     unsigned long long* Sx = LARGE ? c.scr_x + base
-                                   : reinterpret_cast<unsigned long long*>(smem) + 2 * MEDIUM_MAX;
-    uint32_t* P = LARGE ? c.scr_p + base : reinterpret_cast<uint32_t*>(smem + 24 * MEDIUM_MAX);
-    uint32_t* J = LARGE ? c.scr_j + base : reinterpret_cast<uint32_t*>(smem + 28 * MEDIUM_MAX);
+                                   : reinterpret_cast<unsigned long long*>(smem) + 2 * MBUF + off;
+    uint32_t* P = LARGE ? c.scr_p + base : reinterpret_cast<uint32_t*>(smem + 24 * MBUF);
+    uint32_t* J = LARGE ? c.scr_j + base
+                        : reinterpret_cast<uint32_t*>(smem + 24 * MBUF + 4 * MEDIUM_MAX);
     // Simmel terminal velocities once per droplet (medium: shared memory after the five staged
     // arrays; large: computed per pair)
-    double* Stv = LARGE ? nullptr : reinterpret_cast<double*>(smem + 32 * MEDIUM_MAX);
+    double* Stv = LARGE ? nullptr : reinterpret_cast<double*>(smem + 24 * MBUF + 8 * MEDIUM_MAX);
+    if (!LARGE) {
+      if (tid == 0) {  // the previous gridbox's accesses ended at the barriers above
+        const uint32_t bytes = ((n + off + 1u) & ~1u) * 8u;
+        const uint32_t a0 = base & ~1u;
+        fence_async_smem();
+        mbar_expect_tx(&s_bar, 3u * bytes);
+        bulk_g2s(smem, c.sd.r + a0, bytes, &s_bar);
+        bulk_g2s(smem + 8 * MBUF, c.sd.msol + a0, bytes, &s_bar);
+        bulk_g2s(smem + 16 * MBUF, c.sd.xi + a0, bytes, &s_bar);
+      }
+      // every thread waits with a bound; the outcome is agreed by the whole block
+      const bool ok = __syncthreads_and(mbar_wait_bounded(&s_bar, bar_parity, MBAR_TRIES) ? 1 : 0);
+      if (!ok) {
+        if (tid == 0) Where{c.err, g, base}.fail(CLEO_ERR_TIMEOUT);
+        mbar_wait_bounded(&s_bar, bar_parity, MBAR_TRIES);  // let the copies in flight land
+        return;
+      }
+      bar_parity ^= 1u;
+    }
     for (uint32_t k = tid; k < n; k += B_THREADS) {
-      const double rk = c.sd.r[base + k];
-      Sr[k] = rk;
-      Sm[k] = c.sd.msol[base + k];
-      Sx[k] = c.sd.xi[base + k];
-      if (!LARGE) Stv[k] = pair_tv(p, rk);
+      if (LARGE) {
+        Sr[k] = c.sd.r[base + k];
+        Sm[k] = c.sd.msol[base + k];
+        Sx[k] = c.sd.xi[base + k];
+      } else {
+        Stv[k] = pair_tv(p, Sr[k]);
+      }
       if (k >= 1) J[k] = (uint32_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - k)), 0, (uint64_t)k + 1);
     }
     __syncthreads();

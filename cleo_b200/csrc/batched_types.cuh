@@ -8,7 +8,9 @@ namespace {
 constexpr uint32_t SMALL_MAX = 64;   // default limit of the warp kernel
 constexpr uint32_t WARP_MAX = 128;   // largest gridbox the warp kernel's 128-slot variant holds
 constexpr uint32_t MEDIUM_MAX = 1024;
-constexpr uint32_t MEDIUM_SMEM = 40 * MEDIUM_MAX;  // r, msol, xi, P, J, Simmel velocity
+// r, msol, xi (each with two elements of slack for the bulk copies' alignment), P, J, Simmel
+// velocity
+constexpr uint32_t MEDIUM_SMEM = 24 * (MEDIUM_MAX + 2) + 16 * MEDIUM_MAX;
 constexpr uint32_t FY_PARALLEL_MAX = 256;  // gridboxes up to this size shuffle in parallel
 constexpr int B_THREADS = 256;
 constexpr int B_WARPS = B_THREADS / 32;
