@@ -247,11 +247,17 @@ def measure(lib, wl, mode, steps, warmup, dist, local, e2e=False, surrogate=None
         cm_out = torch.empty(ngbxs, dtype=torch.float64).pin_memory()
         it_out = torch.empty(ngbxs, dtype=torch.int64).pin_memory()
         lib.cleo_b200_download_state(ctx, C.byref(st_struct))
+        # one untimed exchange sets the copy stream and staging areas up (steady state)
+        assert lib.cleo_b200_upload_state_async(ctx, C.byref(st_struct)) == 0
+        assert lib.cleo_b200_download_budgets_async(
+            ctx, C.c_void_p(cm_out.data_ptr()), C.c_void_p(it_out.data_ptr())) == 0
+        assert lib.cleo_b200_synchronize(ctx) == 0
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         # the states of each step are uploaded on the context's copy stream while the previous
-        # step runs (cleo_b200_upload_state_async), the budgets copied back behind each step
+        # step runs (cleo_b200_upload_state_async), the budgets copied back behind each step on
+        # the same stream
         for _ in range(steps):
             assert lib.cleo_b200_upload_state_async(ctx, C.byref(st_struct)) == 0
             sdm.run_step(t * 100, (t + 1) * 100)

@@ -124,6 +124,19 @@ struct cleo_b200_ctx {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_uploaded = nullptr, ev_consumed = nullptr;
   bool upload_pending = false, consumed_recorded = false;
+  // asynchronous budget download: a device snapshot copied to the host on the copy stream
+  double* snap_budgets = nullptr;  // [2][ngbxs]: condensed mass, Newton iterations
+  cudaStream_t d2h_stream = nullptr;  // its own stream: the next upload must not queue behind it
+  cudaEvent_t ev_snap = nullptr, ev_snap_free = nullptr;
+  bool snap_in_flight = false;
+  int ensure_copy_stream() {
+    if (copy_stream) return CLEO_OK;
+    bool ok = cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&d2h_stream, cudaStreamNonBlocking) == cudaSuccess;
+    for (cudaEvent_t* e : {&ev_uploaded, &ev_consumed, &ev_snap, &ev_snap_free})
+      ok = ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
+    return ok ? CLEO_OK : CLEO_ERR_CUDA;
+  }
   // superdroplet output staging (allocated at the first gather): converted fields, offsets
   uint8_t* obs_stage = nullptr;
   uint32_t *obs_start = nullptr, *obs_tsums = nullptr;
@@ -1731,12 +1744,13 @@ void cleo_b200_destroy(cleo_b200_ctx* x) {
   x->drop_graphs();
   cudaFree(x->seed_buf);
   x->free_cs();
-  if (x->copy_stream) {
-    cudaStreamSynchronize(x->copy_stream);
-    cudaStreamDestroy(x->copy_stream);
+  for (cudaStream_t cs : {x->copy_stream, x->d2h_stream}) {
+    if (!cs) continue;
+    cudaStreamSynchronize(cs);
+    cudaStreamDestroy(cs);
   }
-  if (x->ev_uploaded) cudaEventDestroy(x->ev_uploaded);
-  if (x->ev_consumed) cudaEventDestroy(x->ev_consumed);
+  for (cudaEvent_t e : {x->ev_uploaded, x->ev_consumed, x->ev_snap, x->ev_snap_free})
+    if (e) cudaEventDestroy(e);
   for (void* p : x->allocs) cudaFree(p);
   if (x->h_motion) cudaFreeHost(x->h_motion);
   if (x->own_stream && x->stream) cudaStreamDestroy(x->stream);
@@ -1836,9 +1850,8 @@ int cleo_b200_upload_state_async(cleo_b200_ctx* x, const cleo_b200_gbx_state* h)
     if (!src[k]) return CLEO_ERR_ARGUMENT;
   if (!x->stage_state) {  // first use: staging area, copy stream, events
     if (dalloc(x, &x->stage_state, 11 * (ng ? ng : 1))) return CLEO_ERR_CUDA;
-    CUDA_TRY(cudaStreamCreateWithFlags(&x->copy_stream, cudaStreamNonBlocking));
-    CUDA_TRY(cudaEventCreateWithFlags(&x->ev_uploaded, cudaEventDisableTiming));
-    CUDA_TRY(cudaEventCreateWithFlags(&x->ev_consumed, cudaEventDisableTiming));
+    const int rc = x->ensure_copy_stream();
+    if (rc) return rc;
   }
   // the staging area is free once the previous step has taken its states
   if (x->consumed_recorded) CUDA_TRY(cudaStreamWaitEvent(x->copy_stream, x->ev_consumed, 0));
@@ -1853,12 +1866,26 @@ int cleo_b200_upload_state_async(cleo_b200_ctx* x, const cleo_b200_gbx_state* h)
 int cleo_b200_download_budgets_async(cleo_b200_ctx* x, double* cond_mass, uint64_t* nr_iters) {
   if (!x) return CLEO_ERR_ARGUMENT;
   const size_t ng = x->d.ngbxs;
+  if (!x->snap_budgets) {
+    if (dalloc(x, &x->snap_budgets, 2 * (ng ? ng : 1))) return CLEO_ERR_CUDA;
+    const int rc = x->ensure_copy_stream();
+    if (rc) return rc;
+  }
+  // snapshot behind the work so far (device to device), once the previous snapshot has left
+  if (x->snap_in_flight) CUDA_TRY(cudaStreamWaitEvent(x->stream, x->ev_snap_free, 0));
+  double* sc = x->snap_budgets;
+  uint64_t* si = reinterpret_cast<uint64_t*>(x->snap_budgets + ng);
+  CUDA_TRY(cudaMemcpyAsync(sc, x->d.cond_mass, ng * 8, cudaMemcpyDeviceToDevice, x->stream));
+  CUDA_TRY(cudaMemcpyAsync(si, x->d.nr_iters, ng * 8, cudaMemcpyDeviceToDevice, x->stream));
+  CUDA_TRY(cudaEventRecord(x->ev_snap, x->stream));
+  // to the host on a stream of its own, overlapping the next step
+  CUDA_TRY(cudaStreamWaitEvent(x->d2h_stream, x->ev_snap, 0));
   if (cond_mass)
-    CUDA_TRY(cudaMemcpyAsync(cond_mass, x->d.cond_mass, ng * 8, cudaMemcpyDeviceToHost,
-                             x->stream));
+    CUDA_TRY(cudaMemcpyAsync(cond_mass, sc, ng * 8, cudaMemcpyDeviceToHost, x->d2h_stream));
   if (nr_iters)
-    CUDA_TRY(cudaMemcpyAsync(nr_iters, x->d.nr_iters, ng * 8, cudaMemcpyDeviceToHost,
-                             x->stream));
+    CUDA_TRY(cudaMemcpyAsync(nr_iters, si, ng * 8, cudaMemcpyDeviceToHost, x->d2h_stream));
+  CUDA_TRY(cudaEventRecord(x->ev_snap_free, x->d2h_stream));
+  x->snap_in_flight = true;
   return CLEO_OK;
 }
 
@@ -1866,6 +1893,7 @@ int cleo_b200_synchronize(cleo_b200_ctx* x) {
   if (!x) return CLEO_ERR_ARGUMENT;
   if (x->copy_stream) CUDA_TRY(cudaStreamSynchronize(x->copy_stream));
   CUDA_TRY(cudaStreamSynchronize(x->stream));
+  if (x->d2h_stream) CUDA_TRY(cudaStreamSynchronize(x->d2h_stream));
   return CLEO_OK;
 }
 

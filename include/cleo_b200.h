@@ -209,9 +209,11 @@ int cleo_b200_upload_state(cleo_b200_ctx* ctx, const cleo_b200_gbx_state* host);
  * of the context, behind the previous step's use of that area, and returns at once; the next
  * cleo_b200_step waits for the copy, makes the staged states the live ones at its start, and
  * returns once the host arrays have been read (they may be refilled after it returns). An
- * upload_state (synchronous) in between replaces the staged states. The budgets' copy to the host
- * (cleo_b200_download_budgets_async) is enqueued after the work so far; its arrays hold the
- * values once cleo_b200_synchronize has returned. Results are those of the synchronous calls.
+ * upload_state (synchronous) in between replaces the staged states.
+ * cleo_b200_download_budgets_async takes a device snapshot of the budgets behind the work so far
+ * and copies it to the host arrays on a stream of its own while the following steps run; the arrays
+ * hold the values once cleo_b200_synchronize has returned. Results are those of the synchronous
+ * calls.
  */
 int cleo_b200_upload_state_async(cleo_b200_ctx* ctx, const cleo_b200_gbx_state* h);
 int cleo_b200_download_budgets_async(cleo_b200_ctx* ctx, double* cond_mass, uint64_t* nr_iters);
