@@ -55,8 +55,25 @@ __global__ void k_b_qcond(DevCtx c) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
-  for (uint32_t g = warp; g < c.ngbxs; g += nwarps) {
-    const uint32_t base = c.gstart[g], n = c.gcount[g];
+  // each gridbox's range and state are loaded a gridbox ahead (one dependent round trip less)
+  uint32_t g = warp;
+  uint32_t base = 0, n = 0;
+  double vol = 0.0, press = 0.0, temp = 0.0, qvap = 0.0;
+  if (g < c.ngbxs) {
+    base = c.gstart[g];
+    n = c.gcount[g];
+    if (lane == 0) vol = c.volume[g], press = c.press[g], temp = c.temp[g], qvap = c.qvap[g];
+  }
+  for (; g < c.ngbxs; g += nwarps) {
+    const uint32_t gn = g + nwarps;
+    uint32_t base_n = 0, n_n = 0;
+    double vol_n = 0.0, press_n = 0.0, temp_n = 0.0, qvap_n = 0.0;
+    if (gn < c.ngbxs) {
+      base_n = c.gstart[gn];
+      n_n = c.gcount[gn];
+      if (lane == 0)
+        vol_n = c.volume[gn], press_n = c.press[gn], temp_n = c.temp[gn], qvap_n = c.qvap[gn];
+    }
     double m = 0.0;
     for (uint32_t k = lane; k < n; k += 32) {
       const Where w{c.err, g, base + k};
@@ -65,9 +82,10 @@ __global__ void k_b_qcond(DevCtx c) {
     m = warp_sum_d(m);
     if (lane == 0) {
       const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
-      const double rho_cond = m / c.volume[g] * R0cubed_VOL0;
-      c.qcond[g] = rho_cond / dry_air_density(c.press[g], c.temp[g], c.qvap[g]);
+      const double rho_cond = m / vol * R0cubed_VOL0;
+      c.qcond[g] = rho_cond / dry_air_density(press, temp, qvap);
     }
+    base = base_n, n = n_n, vol = vol_n, press = press_n, temp = temp_n, qvap = qvap_n;
   }
 }
 
