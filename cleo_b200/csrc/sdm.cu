@@ -10,12 +10,20 @@
 // once, sdmmethods.hpp:221-229; both give the same in-domain superdroplets in the same order).
 //
 // One SDM step (SDMMethods::run_step, sdmmethods.hpp:319-332):
-//   motion  -> k_motion: predictor-corrector coords + new gridbox index + sort key per droplet
-//   sort    -> radix passes over (key, position), gather of all fields, gridbox refs by binary
-//              search, append of out-of-domain droplets to the store
-//   microphysics -> k_micro: one CTA per gridbox: qcond from the moved droplets, condensation
-//              (FP64 Newton) and collisions (shared-memory shuffle, parallel pairs, null removal)
-//              for every sub-step of the SDM step.
+//   motion  -> k_motion: predictor-corrector coords + new gridbox index + sort key per droplet,
+//              and (for the incremental re-sort) the flags and per-gridbox counts of the movers
+//   sort    -> chosen per step from the previous motion step's mover count: incremental (scan of
+//              the mover flags, radix sort of the movers only, one copy of every droplet to its
+//              place: k_mv_*) while at most a fifth of the droplets moved, else the full sort
+//              (radix passes over (key, position), gather of all fields, gridbox refs by binary
+//              search); then the append of out-of-domain droplets to the store
+//   microphysics -> plain schedule: k_micro, one CTA per gridbox: qcond from the moved droplets,
+//              condensation (FP64 Newton) and collisions (shared-memory shuffle, parallel pairs,
+//              null removal) for every sub-step of the SDM step; batched schedule: the kernels of
+//              batched.cuh, captured as one CUDA graph per step pattern.
+// Around the step: superdroplet output (gather into CLEO's output types), SDMMonitor members,
+// the asynchronous state and budget exchange, the autotuner and the condensation surrogate's
+// seeding.
 #include <cuda_runtime.h>
 
 #include <cstdio>
