@@ -338,7 +338,8 @@ struct SmallLayout {
   static constexpr uint32_t OFF_TV = 2 * 3 * FIELD;
   static constexpr uint32_t OFF_P = OFF_TV + CAP * 8;
   static constexpr uint32_t OFF_J = OFF_P + CAP;
-  static constexpr uint32_t OFF_BAR = (OFF_J + CAP + 15) / 16 * 16;
+  static constexpr uint32_t OFF_F = OFF_J + CAP;  // first index of each swap target (chains)
+  static constexpr uint32_t OFF_BAR = (OFF_F + CAP + 15) / 16 * 16;
   static constexpr uint32_t WARP_BYTES = OFF_BAR + 16;
   static constexpr uint32_t BYTES = WARP_BYTES * B_WARPS;
   static_assert(FIELD % 16 == 0 && WARP_BYTES % 16 == 0, "bulk-copy buffers must be aligned");
@@ -372,6 +373,7 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
   double* s_tv = reinterpret_cast<double*>(wsm + L::OFF_TV);
   uint8_t* s_p = wsm + L::OFF_P;
   uint8_t* s_j = wsm + L::OFF_J;
+  uint8_t* s_f = wsm + L::OFF_F;
   uint64_t* bar = reinterpret_cast<uint64_t*>(wsm + L::OFF_BAR);
   const auto field = [&](int buf, int f) { return wsm + (buf * 3 + f) * L::FIELD; };
   const uint32_t count = b.ctr[1];
@@ -440,18 +442,46 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
         s_j[k] = (uint8_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - k)), 0, (uint64_t)k + 1);
     }
     __syncwarp();
-    {  // origins of the lane's positions, traced together through the swaps (fy_origin)
-      uint32_t pos[H];
+    {
+      // origins of the shuffled positions (what fy_origin computes), by chains: tracing position
+      // k through the swaps, nothing happens before swap k, swap k takes it to J[k], and after
+      // that it moves only to a later index s whose J[s] equals its current position. With
+      // FIRST[v] (the first index s >= 1 with J[s] == v) and NEXTSAME[s] (the next index after s
+      // with the same J value), the origin of k is the end of the chain J[k] -> NEXTSAME[k] ->
+      // FIRST[.] -> ... (0 -> FIRST[0] -> ... for k = 0), about ln n lookups instead of n - 1
+      // swaps. Both tables are built from the index groups of 32, last group first, with
+      // __match_any_sync.
+      constexpr uint32_t NONE = 0xFFu;
+      for (uint32_t v = lane; v < n; v += 32) s_f[v] = (uint8_t)NONE;
+      __syncwarp();
+      uint32_t nsame[H];
 #pragma unroll
-      for (int h = 0; h < H; ++h) pos[h] = lane + 32 * h;
-      for (uint32_t s = 1; s < n; ++s) {
-        const uint32_t j = s_j[s];
-#pragma unroll
-        for (int h = 0; h < H; ++h) pos[h] = (pos[h] == s) ? j : ((pos[h] == j) ? s : pos[h]);
+      for (int h = H - 1; h >= 0; --h) {
+        nsame[h] = NONE;
+        if (32u * h >= n) continue;  // uniform across the warp
+        const uint32_t sidx = lane + 32u * h;
+        const bool act = sidx >= 1 && sidx < n;
+        const uint32_t v = act ? (uint32_t)s_j[sidx] : 0x100u + lane;  // inactive: unique
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, v);
+        const unsigned higher = peers & ~((2u << lane) - 1u);
+        if (act) nsame[h] = higher ? 32u * h + __ffs(higher) - 1 : (uint32_t)s_f[v];
+        __syncwarp();
+        if (act && lane == __ffs(peers) - 1) s_f[v] = (uint8_t)sidx;
+        __syncwarp();
       }
 #pragma unroll
-      for (int h = 0; h < H; ++h)
-        if (lane + 32 * h < n) s_p[lane + 32 * h] = (uint8_t)pos[h];
+      for (int h = 0; h < H; ++h) {
+        const uint32_t k = lane + 32u * h;
+        if (k < n) {
+          uint32_t cur = k == 0 ? 0u : (uint32_t)s_j[k];
+          uint32_t nx = k == 0 ? (uint32_t)s_f[0] : nsame[h];
+          while (nx != NONE) {  // strictly increasing, so at most n hops
+            cur = nx;
+            nx = s_f[cur];
+          }
+          s_p[k] = (uint8_t)cur;
+        }
+      }
     }
     __syncwarp();
     const uint64_t slot_pairs = slot + (n >= 1 ? n - 1 : 0);
