@@ -292,6 +292,7 @@ EXPORTED = (
     "cleo_b200_tuned_config", "cleo_b200_set_launch_config", "cleo_b200_monitors_begin",
     "cleo_b200_download_monitors",
     "cleo_b200_upload_state_async", "cleo_b200_download_budgets_async", "cleo_b200_synchronize",
+    "cleo_b200_check_bounded_wait",
     "cleo_b200_gather_supers", "cleo_b200_zarr_open", "cleo_b200_zarr_observe",
     "cleo_b200_zarr_observe_host", "cleo_b200_zarr_close",
 )
@@ -348,6 +349,7 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
             ("upload_state_async", [vp, C.POINTER(GbxState)]),
             ("download_budgets_async", [vp, vp, vp]),
             ("synchronize", [vp]),
+            ("check_bounded_wait", [C.c_uint32]),
             ("gather_supers", [vp, C.c_uint32, C.POINTER(ObsSupers), C.c_size_t,
                                C.POINTER(C.c_size_t)]),
             ("zarr_open", [C.c_char_p, C.c_size_t, C.c_uint32, C.c_uint32, C.POINTER(vp)]),

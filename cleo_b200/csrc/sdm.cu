@@ -593,6 +593,17 @@ k_obs_gather(DevCtx c, ObsOut o, const uint32_t* __restrict__ start) {
   }
 }
 
+// self-check of the bounded waits: an mbarrier that nothing arrives on, waited for with the
+// same bounded wait as the bulk-copy and tensor-core waits; the bound must run out
+__global__ void k_wait_check(uint32_t max_tries, int* __restrict__ out) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) mlp::mbar_init(&bar, 1);
+  __syncthreads();
+  const bool completed = mlp::mbar_wait_bounded(&bar, 0, max_tries);
+  const int all = __syncthreads_or(completed ? 1 : 0);
+  if (threadIdx.x == 0) *out = all ? CLEO_OK : CLEO_ERR_TIMEOUT;
+}
+
 // sort keys of freshly uploaded droplets
 __global__ void k_keys_from_gbx(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
   const uint32_t n = c.counters[0];
@@ -1992,6 +2003,19 @@ int cleo_b200_set_launch_config(cleo_b200_ctx* x, const int32_t cfg[4]) {
   x->tune_step = 0;
   x->drop_graphs();
   return CLEO_OK;
+}
+
+int cleo_b200_check_bounded_wait(uint32_t max_tries) {
+  if (max_tries == 0 || max_tries > (1u << 24)) return CLEO_ERR_ARGUMENT;
+  int* d_out = nullptr;
+  CUDA_TRY(cudaMalloc(&d_out, sizeof(int)));
+  int h = -1;
+  k_wait_check<<<1, 128>>>(max_tries, d_out);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(&h, d_out, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return CLEO_ERR_CUDA;
+  return h;
 }
 
 int cleo_b200_set_graphs(cleo_b200_ctx* x, int on) {

@@ -477,6 +477,16 @@ int cleo_b200_zarr_observe_host(cleo_b200_zarr* z, uint32_t t_mdl, const cleo_b2
 /* Write the last partly filled chunks and the final array shapes, then free the writer. */
 int cleo_b200_zarr_close(cleo_b200_zarr* z);
 
+/*
+ * Self-check of the bounded device waits (no counterpart in the reference). Every wait of the
+ * library's kernels on an mbarrier (bulk-copy staging, tensor-core completion) gives up after a
+ * bounded number of tries, records CLEO_ERR_TIMEOUT and lets the kernel return, so that a stuck
+ * wait surfaces as a status instead of a hung device. This runs that wait on the current device
+ * on a barrier that nothing completes, with max_tries (1 .. 2^24) tries per thread, and returns
+ * the status the wait produced: CLEO_ERR_TIMEOUT when the bound works.
+ */
+int cleo_b200_check_bounded_wait(uint32_t max_tries);
+
 /* Library version string. */
 const char* cleo_b200_version(void);
 
