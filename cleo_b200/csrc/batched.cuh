@@ -92,7 +92,7 @@ __global__ void k_b_qcond(DevCtx c) {
 // ---- per-gridbox thermodynamics of superdroplets_change (condensation.cpp:43-59) ----
 __global__ void k_b_thermo(DevCtx c, BatchScratch b) {
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x) {
-    if (g == 0) b.ctr[0] = b.ctr[7] = 0;  // deferred solves, of which restarts
+    if (g == 0) b.ctr[0] = b.ctr[9] = 0;  // deferred solves, of which restarts
     if (c.gcount[g] == 0) continue;
     const Where w{c.err, g, c.gstart[g]};
     const double temp = c.temp[g];
@@ -103,7 +103,7 @@ __global__ void k_b_thermo(DevCtx c, BatchScratch b) {
 }
 
 // the surrogate's IO for the batched schedule: row j is the j-th solve of pass A's sorted list,
-// whose first b.ctr[7] entries are the direct solves that two iterations did not settle (key 0;
+// whose first b.ctr[9] entries are the direct solves that two iterations did not settle (key 0;
 // the sub-stepping solves after them cannot use a seed); the seed r^2 goes to b.dm of that
 // droplet, which pass B reads (and then overwrites with the droplet's condensed mass)
 struct SdmListSeedIO {
@@ -192,7 +192,7 @@ k_cond_a(DevCtx c, BatchScratch b) {
     const uint32_t pos = warp_append(&b.ctr[0], defer);
     {  // restarts (key 0) lead the sorted list; their number bounds the surrogate's rows
       const unsigned rm = __ballot_sync(0xFFFFFFFFu, defer && key == 0u);
-      if (rm && (threadIdx.x & 31) == (unsigned)(__ffs(rm) - 1)) atomicAdd(&b.ctr[7], __popc(rm));
+      if (rm && (threadIdx.x & 31) == (unsigned)(__ffs(rm) - 1)) atomicAdd(&b.ctr[9], __popc(rm));
     }
     if (defer) {
       b.lkeys[pos] = key;
@@ -260,9 +260,13 @@ __global__ void k_b_classify(DevCtx c, BatchScratch b) {
   for (uint32_t g0 = blockIdx.x * blockDim.x; g0 < ng; g0 += gridDim.x * blockDim.x) {
     const uint32_t g = g0 + threadIdx.x;
     const uint32_t n = g < ng ? c.gcount[g] : 0u;
-    const int bk = (n == 0) ? -1 : (n <= b.small_max ? 0 : (n <= b.medium_max ? 1 : 2));
+    // buckets: warp kernel's 64-slot variant, its 128-slot variant (65 .. small_max), CTA per
+    // gridbox in shared memory, CTA per gridbox with global scratch
+    const uint32_t lo = b.small_max < SMALL_MAX ? b.small_max : SMALL_MAX;
+    const int bk = (n == 0) ? -1
+                 : (n <= lo ? 0 : (n <= b.small_max ? 1 : (n <= b.medium_max ? 2 : 3)));
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
+    for (int q = 0; q < 4; ++q) {
       const uint32_t pos = warp_append(&b.ctr[1 + q], bk == q);
       if (bk == q) b.bucket[(size_t)q * ng + pos] = g;
     }
@@ -361,7 +365,7 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 
 template <int MINB, int CAP>
 __global__ void __launch_bounds__(B_THREADS, MINB)
-k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
+k_b_small(DevCtx c, BatchScratch b, int cond, int coll, int q) {
   using L = SmallLayout<CAP>;
   constexpr int H = CAP / 32;
   static_assert(CAP % 32 == 0 && CAP <= 255, "slot indices are stored as bytes");
@@ -376,8 +380,8 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll) {
   uint8_t* s_f = wsm + L::OFF_F;
   uint64_t* bar = reinterpret_cast<uint64_t*>(wsm + L::OFF_BAR);
   const auto field = [&](int buf, int f) { return wsm + (buf * 3 + f) * L::FIELD; };
-  const uint32_t count = b.ctr[1];
-  const uint32_t* list = b.bucket;
+  const uint32_t count = b.ctr[1 + q];
+  const uint32_t* list = b.bucket + (size_t)q * c.ngbxs;
   // stage gridbox g's r, msol, xi into buffer buf (lane 0)
   const auto stage = [&](int buf, uint32_t g) {
     const uint32_t base = c.gstart[g], n = c.gcount[g];
@@ -570,7 +574,7 @@ k_b_cta(DevCtx c, BatchScratch b, int cond, int coll) {
   constexpr uint32_t MBUF = MEDIUM_MAX + 2;        // staged elements per field (medium)
   const cleo_b200_params& p = c.p;
   const int tid = threadIdx.x;
-  const uint32_t q_idx = LARGE ? 2 : 1;
+  const uint32_t q_idx = LARGE ? 3 : 2;
   const uint32_t count = b.ctr[1 + q_idx];
   const uint32_t* list = b.bucket + (size_t)q_idx * c.ngbxs;
   uint32_t bar_parity = 0;
@@ -579,7 +583,7 @@ k_b_cta(DevCtx c, BatchScratch b, int cond, int coll) {
     __syncthreads();
   }
   while (true) {
-    if (tid == 0) s_item = atomicAdd(&b.ctr[4 + q_idx], 1u);
+    if (tid == 0) s_item = atomicAdd(&b.ctr[5 + q_idx], 1u);
     __syncthreads();
     const uint32_t item = s_item;
     __syncthreads();
@@ -764,7 +768,7 @@ __global__ void k_b_reset(DevCtx c, BatchScratch b, int slots) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (slots)
     for (uint32_t g = i; g < c.ngbxs; g += gridDim.x * blockDim.x) b.slot[g] = 0;
-  if (i < 6) b.ctr[1 + i] = 0;
+  if (i < 8) b.ctr[1 + i] = 0;  // bucket counts and heads
 }
 
 }  // namespace

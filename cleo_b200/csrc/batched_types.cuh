@@ -23,9 +23,10 @@ struct BatchScratch {
   double* zres;      // per deferred direct solve: pass A's iterate that pass B resumes from
   uint32_t* lkeys;   // cost keys of deferred solves
   uint32_t* lvals;   // positions of deferred solves
-  uint32_t* bucket;  // [3][ngbxs] gridbox lists per size bucket
+  uint32_t* bucket;  // [4][ngbxs] gridbox lists per size bucket
   uint32_t* slot;    // per gridbox RNG slot offset within the SDM step
-  uint32_t* ctr;     // [0] deferred solves, [1..3] bucket counts, [4..6] bucket heads
+  uint32_t* ctr;     // [0] deferred solves, [1..4] bucket counts, [5..8] bucket heads,
+                     // [9] restarts among the deferred solves
   uint32_t* tsdm;    // the SDM step's start time (keys the injected random numbers)
   uint32_t small_max;   // gridboxes with 1..small_max superdroplets: warp kernel (<= WARP_MAX)
   uint32_t medium_max;  // small_max..medium_max: CTA kernel in shared memory (<= MEDIUM_MAX)

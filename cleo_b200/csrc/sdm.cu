@@ -1320,7 +1320,7 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
         if (cleo_mlp_infer_view(x->mlp, &w) != CLEO_OK) return CLEO_ERR_MLP;
         w.err = reinterpret_cast<uint32_t*>(&d.err->code);
         const SdmListSeedIO io{d.sd.gbx, d.sd.r,  d.sd.msol, d.temp, d.press, b.th_s,
-                               d.p.cond_delt, b.lvals, b.ctr + 7, b.dm};
+                               d.p.cond_delt, b.lvals, b.ctr + 9, b.dm};
         const uint32_t tiles = (d.capacity + mlp::TILE_M - 1) / mlp::TILE_M;
         mlp::k_mlp_tc<SdmListSeedIO><<<tiles < 148u * 4u ? tiles : 148u * 4u, 128, mlp::TC_SMEM,
                                        s>>>(w, io, d.capacity);
@@ -1339,17 +1339,20 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       StageMark mk(x, 4);
       k_b_reset<<<1, 32, 0, s>>>(d, b, 0);
       k_b_classify<<<gg, 256, 0, s>>>(d, b);
+      // the warp kernel's 64-slot variant takes gridboxes up to 64 superdroplets, its 128-slot
+      // variant those of 65 .. small_max (when small_max > 64)
       const int wide = x->cfg.small_max > SMALL_MAX ? 1 : 0, m3 = x->cfg.small_minb == 3 ? 1 : 0;
-      const int gs = x->grid_small[wide][m3], ci = cond ? 1 : 0, li = coll ? 1 : 0;
+      const int ci = cond ? 1 : 0, li = coll ? 1 : 0;
       constexpr uint32_t SW = SmallLayout<WARP_MAX>::BYTES, SS = SmallLayout<SMALL_MAX>::BYTES;
-      if (wide && m3)
-        k_b_small<3, WARP_MAX><<<gs, B_THREADS, SW, s>>>(d, b, ci, li);
-      else if (wide)
-        k_b_small<2, WARP_MAX><<<gs, B_THREADS, SW, s>>>(d, b, ci, li);
-      else if (m3)
-        k_b_small<3, SMALL_MAX><<<gs, B_THREADS, SS, s>>>(d, b, ci, li);
+      if (m3)
+        k_b_small<3, SMALL_MAX><<<x->grid_small[0][1], B_THREADS, SS, s>>>(d, b, ci, li, 0);
       else
-        k_b_small<2, SMALL_MAX><<<gs, B_THREADS, SS, s>>>(d, b, ci, li);
+        k_b_small<2, SMALL_MAX><<<x->grid_small[0][0], B_THREADS, SS, s>>>(d, b, ci, li, 0);
+      if (wide && m3)
+        k_b_small<3, WARP_MAX><<<x->grid_small[1][1], B_THREADS, SW, s>>>(d, b, ci, li, 1);
+      else if (wide)
+        k_b_small<2, WARP_MAX><<<x->grid_small[1][0], B_THREADS, SW, s>>>(d, b, ci, li, 1);
+      x->launches += wide;
       k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_SMEM, s>>>(d, b, cond ? 1 : 0,
                                                                            coll ? 1 : 0);
       k_b_cta<true><<<x->grid_large, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
@@ -1613,9 +1616,9 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &x->bs.zres, cap);
   rc |= dalloc(x, &x->bs.lkeys, cap);
   rc |= dalloc(x, &x->bs.lvals, cap);
-  rc |= dalloc(x, &x->bs.bucket, 3 * ng);
+  rc |= dalloc(x, &x->bs.bucket, 4 * ng);
   rc |= dalloc(x, &x->bs.slot, ng);
-  rc |= dalloc(x, &x->bs.ctr, 8);
+  rc |= dalloc(x, &x->bs.ctr, 12);
   rc |= dalloc(x, &x->bs.tsdm, 1);
   rc |= dalloc(x, &x->tile_sums, ((size_t)256 * x->ntiles_max + SCAN_TILE - 1) / SCAN_TILE + 1);
   rc |= dalloc(x, &d.mv_scan, (size_t)cap + 1);
@@ -1685,7 +1688,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   CUDA_TRY(cudaMemsetAsync(d.gcount, 0, (ng ? ng : 1) * 4, x->stream));
   CUDA_TRY(cudaMemsetAsync(d.err, 0, sizeof(DevError), x->stream));
   CUDA_TRY(cudaFuncSetAttribute(k_micro, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MICRO_SMEM));
-  CUDA_TRY(cudaMemsetAsync(x->bs.ctr, 0, 32, x->stream));
+  CUDA_TRY(cudaMemsetAsync(x->bs.ctr, 0, 48, x->stream));
   CUDA_TRY(cudaMemsetAsync(x->bs.tsdm, 0, 4, x->stream));
   CUDA_TRY(cudaMemsetAsync(x->bs.slot, 0, (ng ? ng : 1) * 4, x->stream));
   if (params->monitors) {  // gridbox areas (GbxBoundsFromBinary::gbxarea) and zeroed monitors
