@@ -293,7 +293,7 @@ __device__ __forceinline__ bool beyond_domainboundary(uint32_t gbxindex, uint32_
 // PredCorr::operator() (predcorr.hpp:156-171), cfl_criteria, PredCorrMotion::superdrop_gbx
 // (predcorrmotion.hpp:85-106) with get_no_decomposition_bounding_gridbox (cartesianmaps.cpp:278)
 // and CartesianCheckBounds. Writes the sort key min(gbx, ngbxs) and the position.
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 4)  // 64 registers: measured 15% faster than 80
 k_motion(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, int incremental) {
   const uint32_t n = c.counters[0];
   const uint32_t ng = c.ngbxs;
