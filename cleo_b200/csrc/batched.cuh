@@ -99,6 +99,10 @@ __global__ void k_b_thermo(DevCtx c, BatchScratch b) {
     const double psat = saturation_pressure(temp, w);
     b.th_s[g] = supersaturation_ratio(c.press[g], c.qvap[g], psat);
     b.th_ff[g] = diffusion_factor(c.press[g], temp, psat);
+    const double akoh = kohler_a(temp);  // the droplets' factors that depend on akoh alone
+    b.th_ak[g] = akoh;
+    b.th_a3[g] = activation_a3(akoh);
+    b.th_u3[g] = unique_a3(akoh);
   }
 }
 
@@ -152,16 +156,14 @@ k_cond_a(DevCtx c, BatchScratch b) {
       if (g < c.ngbxs) {
         const Where w{c.err, g, i};
         const double r = c.sd.r[i], msol = c.sd.msol[i];
-        double akoh, bkoh;
-        kohler_factors(msol, c.temp[g], akoh, bkoh);
         const double ffactor_fv = b.th_ff[g] / ventilation_factor(r);
-        const OdeConsts o{b.th_s[g], akoh, bkoh, ffactor_fv};
-        const double z0 = initialguess(o, r);
+        const OdeConsts o{b.th_s[g], b.th_ak[g], kohler_b(msol), ffactor_fv};
+        const double z0 = initialguess_a3(o, r, b.th_a3[g]);
         // ucrit1 || ucrit2, the critical timestep only evaluated when ucrit1 fails
-        const bool ucrit1 = first_unique_criteria(o, r, z0);
-        const double crit = ucrit1 ? 0.0 : critical_timestep(o);
+        const bool ucrit1 = first_unique_a3(o, r, z0, b.th_u3[g]);
+        double crit = 0.0;
         uint32_t ni = 0;
-        if (ucrit1 || p.cond_delt <= crit) {
+        if (ucrit1 || below_critical_timestep(o, p.cond_delt, crit)) {
           bool conv = false, conv1 = false;
           double z1 = 0.0;
           GEval e = eval_g(o, p.cond_delt, r, z0);
@@ -175,7 +177,7 @@ k_cond_a(DevCtx c, BatchScratch b) {
           }
           if (!conv) b.zres[i] = conv1 ? -z1 : e.z;  // where pass B's restart continues
           if (conv) {
-            const double rnew = fmax(sqrt(e.z), dryradius(msol));  // change_radius
+            const double rnew = max_dryradius(sqrt(e.z), msol);  // change_radius
             b.dm[i] = (condensate_mass(rnew, msol, w) - condensate_mass(r, msol, w)) *
                       (double)c.sd.xi[i];
             b.its[i] = ni;
@@ -217,8 +219,7 @@ k_cond_b(DevCtx c, BatchScratch b) {
     const uint32_t g = c.sd.gbx[i];
     const Where w{c.err, g, i};
     const double r = c.sd.r[i], msol = c.sd.msol[i];
-    double akoh, bkoh;
-    kohler_factors(msol, c.temp[g], akoh, bkoh);
+    const double akoh = b.th_ak[g], bkoh = kohler_b(msol);
     uint32_t ni = 0;
     const double seed = p.nr_seed == CLEO_NRSEED_MLP ? b.dm[i] : 0.0;
     double newr;
@@ -231,8 +232,8 @@ k_cond_b(DevCtx c, BatchScratch b) {
       double rsqrd = 0.0;
       bool done = false;
       if (seed_ok(seed)) {
-        const double z0 = initialguess(o, r);
-        const bool ucrit1 = first_unique_criteria(o, r, z0);
+        const double z0 = initialguess_a3(o, r, b.th_a3[g]);
+        const bool ucrit1 = first_unique_a3(o, r, z0, b.th_u3[g]);
         const GEval e0 = eval_g(o, p.cond_delt, r, z0);
         const GEval es = eval_g(o, p.cond_delt, r, seed);
         done = fabs(es.g) < fabs(e0.g) && integrate_seeded(cfg, o, p.cond_delt, r, es, ni, rsqrd) &&
@@ -247,7 +248,7 @@ k_cond_b(DevCtx c, BatchScratch b) {
       newr = solve_condensation(cfg, p.cond_delt, p.cond_minsubdelt, b.th_s[g], akoh, bkoh,
                                 b.th_ff[g], r, seed, ni, w);
     }
-    const double rnew = fmax(newr, dryradius(msol));
+    const double rnew = max_dryradius(newr, msol);
     b.dm[i] = (condensate_mass(rnew, msol, w) - condensate_mass(r, msol, w)) * (double)c.sd.xi[i];
     b.its[i] = ni;
     c.sd.r[i] = rnew;

@@ -18,6 +18,9 @@ constexpr int B_WARPS = B_THREADS / 32;
 struct BatchScratch {
   double* th_s;      // per gridbox supersaturation ratio
   double* th_ff;     // per gridbox diffusion factor
+  double* th_ak;     // per gridbox Kohler factor akoh (kohler_a)
+  double* th_a3;     // per gridbox activation_a3(akoh)
+  double* th_u3;     // per gridbox unique_a3(akoh)
   double* dm;        // per superdroplet condensed mass x xi
   uint32_t* its;     // per superdroplet Newton iterations
   double* zres;      // per deferred direct solve: pass A's iterate that pass B resumes from

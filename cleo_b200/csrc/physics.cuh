@@ -471,12 +471,18 @@ __device__ __forceinline__ double ventilation_factor(double radius) {
   const double vent_factor = 1.0 + 1.0 / (a + b);
   return fmin(vent_factor, vent_factor_max);
 }
+__device__ __forceinline__ double kohler_a(double temp) {
+  const double akoh_constant = 3.3e-7 / (TEMP0 * R0);
+  return akoh_constant / temp;
+}
+__device__ __forceinline__ double kohler_b(double msol) {
+  const double bkoh_constant = 4.3e-6 * RHO0 / MR0;
+  return bkoh_constant * msol * IONIC / Mr_sol;
+}
 __device__ __forceinline__ void kohler_factors(double msol, double temp, double& akoh,
                                                double& bkoh) {
-  const double akoh_constant = 3.3e-7 / (TEMP0 * R0);
-  akoh = akoh_constant / temp;
-  const double bkoh_constant = 4.3e-6 * RHO0 / MR0;
-  bkoh = bkoh_constant * msol * IONIC / Mr_sol;
+  akoh = kohler_a(temp);
+  bkoh = kohler_b(msol);
 }
 
 // ---- ImplicitEuler: impliciteuler.{hpp:41-345, cpp:35-301} ----
@@ -662,8 +668,14 @@ __device__ __forceinline__ bool integrate_seeded(const NewtonCfg& c, const OdeCo
 __device__ __forceinline__ bool seeded_root_ok(const OdeConsts& o, bool ucrit1, double z) {
   return !ucrit1 || z <= 3.0 * o.bkoh / o.akoh;
 }
-__device__ __forceinline__ double initialguess(const OdeConsts& o, double rprev) {  // :156-170
-  const double s_act = 1 + sqrt(4.0 * dpow(o.akoh, 3.0) / 27 / o.bkoh);
+// The factors of initialguess and first_unique_criteria that depend on akoh alone, i.e. on the
+// gridbox's temperature: the batched schedule evaluates them once per gridbox (same expressions,
+// so the same doubles). The two differ in rounding (a correctly rounded cube against a product).
+__device__ __forceinline__ double activation_a3(double akoh) { return 4.0 * dpow(akoh, 3.0) / 27; }
+__device__ __forceinline__ double unique_a3(double akoh) { return 4.0 * akoh * akoh * akoh / 27.0; }
+// initialguess (:156-170) given a3 = activation_a3(o.akoh)
+__device__ __forceinline__ double initialguess_a3(const OdeConsts& o, double rprev, double a3) {
+  const double s_act = 1 + sqrt(a3 / o.bkoh);
   if (o.s_ratio > s_act) {
     const double bigr = 1e-3 / R0;
     const double maxradius = fmax(bigr, rprev);
@@ -671,20 +683,51 @@ __device__ __forceinline__ double initialguess(const OdeConsts& o, double rprev)
   }
   return rprev * rprev;
 }
-__device__ __forceinline__ bool first_unique_criteria(const OdeConsts& o, double rprev,
-                                                      double ziter) {  // :69-83
+__device__ __forceinline__ double initialguess(const OdeConsts& o, double rprev) {  // :156-170
+  return initialguess_a3(o, rprev, activation_a3(o.akoh));
+}
+// first_unique_criteria (:69-83) given a3 = unique_a3(o.akoh)
+__device__ __forceinline__ bool first_unique_a3(const OdeConsts& o, double rprev, double ziter,
+                                                double a3) {
   const double akoh = o.akoh;
   const double bkoh = o.bkoh;
   const double rcritsqrd = 3.0 * bkoh / akoh;
   const bool is_ziter_unactivated = ziter < rcritsqrd;
   const bool is_unactivated = (rprev * rprev < rcritsqrd && is_ziter_unactivated);
-  const double sqrdval = 4.0 * akoh * akoh * akoh / 27.0 / bkoh;
+  const double sqrdval = a3 / bkoh;
   const bool is_subactivated_saturation = (o.s_ratio <= 1.0 + dpow(sqrdval, 0.5));
   return (is_unactivated && is_subactivated_saturation);
+}
+__device__ __forceinline__ bool first_unique_criteria(const OdeConsts& o, double rprev,
+                                                      double ziter) {  // :69-83
+  return first_unique_a3(o, rprev, ziter, unique_a3(o.akoh));
 }
 __device__ __forceinline__ double critical_timestep(const OdeConsts& o) {  // hpp:266-269
   const double cuberoot = dpow(5.0 * o.bkoh / o.akoh, 1.5);
   return 2.5 * o.ffactor_fv / o.akoh * cuberoot;
+}
+// delt <= critical_timestep(o), decided from x sqrt(x) in place of the correctly rounded
+// pow(x, 1.5): the two estimates of the timestep differ by a few units in the last place, so
+// outside a band of 1e-12 relative around the estimate the answer is the same, and inside it
+// the exact timestep decides. `crit` receives the timestep used (the estimate outside the band).
+__device__ __forceinline__ bool below_critical_timestep(const OdeConsts& o, double delt,
+                                                        double& crit) {
+  const double x = 5.0 * o.bkoh / o.akoh;
+  crit = 2.5 * o.ffactor_fv / o.akoh * (x * sqrt(x));
+  const double band = 1e-12 * fabs(crit);
+  if (delt <= crit - band) return true;
+  if (delt > crit + band) return false;
+  crit = critical_timestep(o);  // also where the estimate is not finite
+  return delt <= crit;
+}
+// fmax(r, dryradius(msol)) (change_radius, superdrop.hpp) without the cube root where r is
+// plainly the larger: r^3 Rho_sol > vconst msol (1 + 1e-13) gives r > dryradius(msol), the
+// margin being about 100 times the rounding of both sides and of the cube root; fmax then
+// returns r, as it does after the cube root. Otherwise (and for NaN) the cube root decides.
+__device__ __forceinline__ double max_dryradius(double r, double msol) {
+  const double vconst = 3.0 / (4.0 * PI);
+  if (r * r * r * Rho_sol > vconst * msol * (1.0 + 1e-13)) return r;
+  return fmax(r, dryradius(msol));
 }
 // solve_condensation: impliciteuler.cpp:35-54 (+ substepping :98-113). A usable seed_rsqrd
 // replaces the Newton start of the direct branch (not the branch decision) by a predicted r^2.
@@ -698,7 +741,8 @@ __device__ __forceinline__ double solve_condensation(const NewtonCfg& c, double 
   double ziter = initialguess(o, rprev);
   // ucrit1 || ucrit2: the critical timestep (a general pow) is only needed when ucrit1 fails
   const bool ucrit1 = first_unique_criteria(o, rprev, ziter);
-  const bool direct = ucrit1 || (delt <= critical_timestep(o));
+  double crit;  // the sub-stepping branch below takes the exact timestep
+  const bool direct = ucrit1 || below_critical_timestep(o, delt, crit);
   double rsqrd;
   if (direct) {
     const GEval e0 = eval_g(o, delt, rprev, ziter);

@@ -785,7 +785,7 @@ k_micro(DevCtx c, uint32_t t_sdm, uint32_t t_sdm_next, int did_motion) {
           uint32_t ni = 0;
           const double newr = solve_condensation(cfg, p.cond_delt, p.cond_minsubdelt, s_ratio,
                                                  akoh, bkoh, ffactor, r, 0.0, ni, w);
-          const double rnew = fmax(newr, dryradius(msol));  // change_radius
+          const double rnew = max_dryradius(newr, msol);  // change_radius
           c.sd.r[i] = rnew;
           dm += (condensate_mass(rnew, msol, w) - old_m_cond) * (double)c.sd.xi[i];
           its += ni;
@@ -925,7 +925,7 @@ __global__ void k_condsolve(DevCtx c, uint32_t n, const double* __restrict__ rad
     const double newr = solve_condensation(cfg, delt[i], c.p.cond_minsubdelt, s_ratio[i], akoh,
                                            bkoh, ffactor, radius[i], seeds ? seeds[i] : 0.0, ni,
                                            w);
-    out[i] = fmax(newr, dryradius(msol[i]));
+    out[i] = max_dryradius(newr, msol[i]);
     if (niters_out) niters_out[i] = ni;
   }
 }
@@ -1031,9 +1031,9 @@ k_cs_a(DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __
       const OdeConsts o{s_ratio[i], akoh, bkoh, ffactor / ventilation_factor(r)};
       const double z0 = initialguess(o, r);
       const bool ucrit1 = first_unique_criteria(o, r, z0);
-      const double crit = ucrit1 ? 0.0 : critical_timestep(o);
+      double crit = 0.0;
       uint32_t ni = 0, carried = 0;
-      if (ucrit1 || dt <= crit) {
+      if (ucrit1 || below_critical_timestep(o, dt, crit)) {
         bool conv = false, seeded = false, conv1 = false;
         double z1 = 0.0;
         GEval e = eval_g(o, dt, r, z0);
@@ -1057,7 +1057,7 @@ k_cs_a(DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __
           e = nr_iterate(cfg, o, dt, r, e, conv, ni);
         }
         if (conv) {
-          out[i] = fmax(sqrt(e.z), dryradius(msol[i]));
+          out[i] = max_dryradius(sqrt(e.z), msol[i]);
           if (niters_out) niters_out[i] = ni;
         } else {
           defer = true;  // restart until converged (impliciteuler.cpp:136-140), key 0
@@ -1114,7 +1114,7 @@ k_cs_b(DevCtx c, const double* __restrict__ radius, const double* __restrict__ m
       newr = solve_condensation(cfg, dt, c.p.cond_minsubdelt, s_ratio[i], akoh, bkoh, ffactor, r,
                                 seed, ni, w);
     }
-    out[i] = fmax(newr, dryradius(msol[i]));
+    out[i] = max_dryradius(newr, msol[i]);
     if (niters_out) niters_out[i] += ni;
   }
 }
@@ -1611,6 +1611,9 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &x->hist, (size_t)256 * x->ntiles_max);
   rc |= dalloc(x, &x->bs.th_s, ng);
   rc |= dalloc(x, &x->bs.th_ff, ng);
+  rc |= dalloc(x, &x->bs.th_ak, ng);
+  rc |= dalloc(x, &x->bs.th_a3, ng);
+  rc |= dalloc(x, &x->bs.th_u3, ng);
   rc |= dalloc(x, &x->bs.dm, cap);
   rc |= dalloc(x, &x->bs.its, cap);
   rc |= dalloc(x, &x->bs.zres, cap);
