@@ -50,42 +50,51 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
   return base + __popc(m & ((1u << lane) - 1u));
 }
 
-// ---- effect_on_hydrometeor_states (movesupersindomain.hpp:95-136), warp per gridbox ----
+// ---- effect_on_hydrometeor_states (movesupersindomain.hpp:95-136) ----
+// A warp takes 32 consecutive gridboxes: it sums their condensate one gridbox at a time over its
+// lanes (each lane in the order of its superdroplets, then the warp's fixed reduction tree; the
+// next gridbox's first 32 superdroplets are loaded while the current one is reduced), lane j
+// keeps gridbox j's sum, and the 32 gridboxes' qcond are then computed side by side, one per lane.
 __global__ void k_b_qcond(DevCtx c) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
-  // each gridbox's range and state are loaded a gridbox ahead (one dependent round trip less)
-  uint32_t g = warp;
-  uint32_t base = 0, n = 0;
-  double vol = 0.0, press = 0.0, temp = 0.0, qvap = 0.0;
-  if (g < c.ngbxs) {
-    base = c.gstart[g];
-    n = c.gcount[g];
-    if (lane == 0) vol = c.volume[g], press = c.press[g], temp = c.temp[g], qvap = c.qvap[g];
-  }
-  for (; g < c.ngbxs; g += nwarps) {
-    const uint32_t gn = g + nwarps;
-    uint32_t base_n = 0, n_n = 0;
-    double vol_n = 0.0, press_n = 0.0, temp_n = 0.0, qvap_n = 0.0;
-    if (gn < c.ngbxs) {
-      base_n = c.gstart[gn];
-      n_n = c.gcount[gn];
-      if (lane == 0)
-        vol_n = c.volume[gn], press_n = c.press[gn], temp_n = c.temp[gn], qvap_n = c.qvap[gn];
+  for (uint32_t g0 = warp * 32u; g0 < c.ngbxs; g0 += nwarps * 32u) {
+    const uint32_t gl = g0 + lane;
+    const bool own = gl < c.ngbxs;
+    const uint32_t my_base = own ? c.gstart[gl] : 0u, my_n = own ? c.gcount[gl] : 0u;
+    const uint32_t nb = c.ngbxs - g0 < 32u ? c.ngbxs - g0 : 32u;
+    uint32_t base = __shfl_sync(0xFFFFFFFFu, my_base, 0), n = __shfl_sync(0xFFFFFFFFu, my_n, 0);
+    double r = 0.0, ms = 0.0;
+    unsigned long long xi = 0;
+    if ((uint32_t)lane < n) r = c.sd.r[base + lane], ms = c.sd.msol[base + lane], xi = c.sd.xi[base + lane];
+    double mine = 0.0;
+    for (uint32_t j = 0; j < nb; ++j) {
+      uint32_t base_n = 0, n_n = 0;
+      double r_n = 0.0, ms_n = 0.0;
+      unsigned long long xi_n = 0;
+      if (j + 1 < nb) {  // uniform across the warp
+        base_n = __shfl_sync(0xFFFFFFFFu, my_base, j + 1);
+        n_n = __shfl_sync(0xFFFFFFFFu, my_n, j + 1);
+        if ((uint32_t)lane < n_n)
+          r_n = c.sd.r[base_n + lane], ms_n = c.sd.msol[base_n + lane], xi_n = c.sd.xi[base_n + lane];
+      }
+      const uint32_t g = g0 + j;
+      double m = 0.0;
+      if ((uint32_t)lane < n) m += condensate_mass(r, ms, Where{c.err, g, base + lane}) * (double)xi;
+      for (uint32_t k = lane + 32u; k < n; k += 32u) {
+        const Where w{c.err, g, base + k};
+        m += condensate_mass(c.sd.r[base + k], c.sd.msol[base + k], w) * (double)c.sd.xi[base + k];
+      }
+      m = warp_sum_d(m);
+      if ((uint32_t)lane == j) mine = m;
+      base = base_n, n = n_n, r = r_n, ms = ms_n, xi = xi_n;
     }
-    double m = 0.0;
-    for (uint32_t k = lane; k < n; k += 32) {
-      const Where w{c.err, g, base + k};
-      m += condensate_mass(c.sd.r[base + k], c.sd.msol[base + k], w) * (double)c.sd.xi[base + k];
-    }
-    m = warp_sum_d(m);
-    if (lane == 0) {
+    if (own) {
       const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
-      const double rho_cond = m / vol * R0cubed_VOL0;
-      c.qcond[g] = rho_cond / dry_air_density(press, temp, qvap);
+      const double rho_cond = mine / c.volume[gl] * R0cubed_VOL0;
+      c.qcond[gl] = rho_cond / dry_air_density(c.press[gl], c.temp[gl], c.qvap[gl]);
     }
-    base = base_n, n = n_n, vol = vol_n, press = press_n, temp = temp_n, qvap = qvap_n;
   }
 }
 
@@ -336,11 +345,17 @@ using mlp::mbar_wait_bounded;
 using mlp::MBAR_TRIES;
 using mlp::smem_u32;
 
+// The 64-slot variant stages all seven 8-byte fields (r, msol, xi, coordinates, id), so its
+// write-back reads shared memory instead of gathering the coordinates and ids from global memory
+// in shuffled order; the 128-slot variant stages r, msol and xi (seven fields of 128 slots would
+// leave room for fewer CTAs per SM than its registers allow).
 template <int CAP>
 struct SmallLayout {
+  static constexpr bool ALL = CAP <= 64;
+  static constexpr uint32_t NF = ALL ? 7 : 3;  // staged fields per buffer
   static constexpr uint32_t BUF = CAP + 2;  // elements per staged field
   static constexpr uint32_t FIELD = BUF * 8;
-  static constexpr uint32_t OFF_TV = 2 * 3 * FIELD;
+  static constexpr uint32_t OFF_TV = 2 * NF * FIELD;
   static constexpr uint32_t OFF_P = OFF_TV + CAP * 8;
   static constexpr uint32_t OFF_J = OFF_P + CAP;
   static constexpr uint32_t OFF_F = OFF_J + CAP;  // first index of each swap target (chains)
@@ -380,7 +395,7 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll, int q) {
   uint8_t* s_j = wsm + L::OFF_J;
   uint8_t* s_f = wsm + L::OFF_F;
   uint64_t* bar = reinterpret_cast<uint64_t*>(wsm + L::OFF_BAR);
-  const auto field = [&](int buf, int f) { return wsm + (buf * 3 + f) * L::FIELD; };
+  const auto field = [&](int buf, int f) { return wsm + (buf * L::NF + f) * L::FIELD; };
   const uint32_t count = b.ctr[1 + q];
   const uint32_t* list = b.bucket + (size_t)q * c.ngbxs;
   // stage gridbox g's r, msol, xi into buffer buf (lane 0)
@@ -389,10 +404,16 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll, int q) {
     const uint32_t a0 = base & ~1u;
     const uint32_t bytes = ((n + (base & 1u) + 1u) & ~1u) * 8u;
     fence_async_smem();  // earlier generic accesses of the buffer precede the async writes
-    mbar_expect_tx(&bar[buf], 3u * bytes);
+    mbar_expect_tx(&bar[buf], L::NF * bytes);
     bulk_g2s(field(buf, 0), c.sd.r + a0, bytes, &bar[buf]);
     bulk_g2s(field(buf, 1), c.sd.msol + a0, bytes, &bar[buf]);
     bulk_g2s(field(buf, 2), c.sd.xi + a0, bytes, &bar[buf]);
+    if constexpr (L::ALL) {
+      bulk_g2s(field(buf, 3), c.sd.c3 + a0, bytes, &bar[buf]);
+      bulk_g2s(field(buf, 4), c.sd.c1 + a0, bytes, &bar[buf]);
+      bulk_g2s(field(buf, 5), c.sd.c2 + a0, bytes, &bar[buf]);
+      bulk_g2s(field(buf, 6), c.sd.id + a0, bytes, &bar[buf]);
+    }
   };
   // static assignment (item = warp + k * warps): no shared counter, and the next gridbox's list
   // entry is loaded a whole gridbox ahead
@@ -401,6 +422,14 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll, int q) {
   uint32_t g_next = item < count ? list[item] : 0u;
   uint32_t parity = 0;  // bit k: the phase of bar[k] to wait for
   int cur = 0;
+  // condensation commits of up to 32 gridboxes, lane j holding the j-th, made side by side
+  // (after the 32nd and after the warp's last gridbox)
+  uint32_t pend_g = 0, pend_it = 0, npend = 0;
+  double pend_m = 0.0;
+  const auto commit_pending = [&]() {
+    if ((uint32_t)lane < npend) cond_commit(c, pend_g, pend_m, pend_it);
+    npend = 0;
+  };
   if (coll) {
     if (lane == 0) {
       mbar_init(&bar[0], 1);
@@ -424,7 +453,8 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll, int q) {
       }
       m = warp_sum_d(m);
       it = warp_sum_u(it);
-      if (lane == 0) cond_commit(c, g, m, it);
+      if ((uint32_t)lane == npend) pend_g = g, pend_m = m, pend_it = it;
+      if (++npend == 32u || !has_next) commit_pending();  // one call site: a smaller loop body
     }
     if (!coll) continue;
     // the next gridbox's copies go out before this one's wait
@@ -432,7 +462,7 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll, int q) {
     if (!mbar_wait_bounded(&bar[cur], (parity >> cur) & 1u, MBAR_TRIES)) {
       if (lane == 0) Where{c.err, g, base}.fail(CLEO_ERR_TIMEOUT);
       if (has_next) mbar_wait_bounded(&bar[cur ^ 1], (parity >> (cur ^ 1)) & 1u, MBAR_TRIES);
-      return;
+      return;  // the step fails with CLEO_ERR_TIMEOUT; pending commits are dropped
     }
     parity ^= 1u << cur;
     const uint32_t off = base & 1u;
@@ -509,8 +539,8 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll, int q) {
     const uint32_t nvalid = n - totnull;
     // destinations: valid superdroplets in shuffled order, then the nulls (collisions.hpp:240-248)
     uint32_t src[H], q[H];
-    double c3v[H], c1v[H], c2v[H];
-    unsigned long long idv[H];
+    double c3v[L::ALL ? 1 : H], c1v[L::ALL ? 1 : H], c2v[L::ALL ? 1 : H];
+    unsigned long long idv[L::ALL ? 1 : H];
     uint32_t cval = 0, cnull = 0;
 #pragma unroll
     for (int h = 0; h < H; ++h) {
@@ -525,12 +555,14 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll, int q) {
       q[h] = valid ? cval + __popc(mv & lt) : nvalid + cnull + __popc(mn & lt);
       cval += __popc(mv);
       cnull += __popc(mn);
-      if (act) {
-        const uint32_t s = base + src[h];
-        c3v[h] = c.sd.c3[s];
-        c1v[h] = c.sd.c1[s];
-        c2v[h] = c.sd.c2[s];
-        idv[h] = c.sd.id[s];
+      if constexpr (!L::ALL) {
+        if (act) {
+          const uint32_t s = base + src[h];
+          c3v[h] = c.sd.c3[s];
+          c1v[h] = c.sd.c1[s];
+          c2v[h] = c.sd.c2[s];
+          idv[h] = c.sd.id[s];
+        }
       }
     }
     __syncwarp();
@@ -543,10 +575,17 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll, int q) {
         c.sd.msol[o] = s_m[src[h]];
         c.sd.xi[o] = s_x[src[h]];
         c.sd.gbx[o] = q[h] < nvalid ? g : OOB;
-        c.sd.c3[o] = c3v[h];
-        c.sd.c1[o] = c1v[h];
-        c.sd.c2[o] = c2v[h];
-        c.sd.id[o] = idv[h];
+        if constexpr (L::ALL) {
+          c.sd.c3[o] = reinterpret_cast<const double*>(field(cur, 3))[off + src[h]];
+          c.sd.c1[o] = reinterpret_cast<const double*>(field(cur, 4))[off + src[h]];
+          c.sd.c2[o] = reinterpret_cast<const double*>(field(cur, 5))[off + src[h]];
+          c.sd.id[o] = reinterpret_cast<const unsigned long long*>(field(cur, 6))[off + src[h]];
+        } else {
+          c.sd.c3[o] = c3v[h];
+          c.sd.c1[o] = c1v[h];
+          c.sd.c2[o] = c2v[h];
+          c.sd.id[o] = idv[h];
+        }
       }
     }
     __syncwarp();  // every lane is done with buffer cur before it is staged into again

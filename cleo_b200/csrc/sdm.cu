@@ -1291,8 +1291,9 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
   StageMark m(x, 2);
   const int gg = grid_for(d.ngbxs, 256);
   if (did_motion) {
-    const size_t warps = d.ngbxs < (size_t)148 * 64 ? d.ngbxs : (size_t)148 * 64;
-    k_b_qcond<<<(unsigned)((warps * 32 + 255) / 256 + 1), 256, 0, s>>>(d);
+    const size_t batches = ((size_t)d.ngbxs + 31) / 32;  // a warp per 32 gridboxes
+    const size_t warps = batches < 1 ? 1 : (batches < (size_t)148 * 64 ? batches : (size_t)148 * 64);
+    k_b_qcond<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(d);
     x->launches += 1;
   }
   k_b_reset<<<gg, 256, 0, s>>>(d, b, 1);
