@@ -309,13 +309,15 @@ __device__ __forceinline__ uint32_t collide_pair(const cleo_b200_params& p, Drop
   const bool swap = dA.xi < dB.xi;
   Drop& d1 = swap ? dB : dA;
   Drop& d2 = swap ? dA : dB;
-  const double prob_jk =
-      pair_prob_tv(p, d1.r, d2.r, swap ? tvB : tvA, swap ? tvA : tvB, VOLUME);
+  const double tv1 = swap ? tvB : tvA, tv2 = swap ? tvA : tvB;
+  const double prob_jk = pair_prob_tv(p, d1.r, d2.r, tv1, tv2, VOLUME);
   const double large_xi = (double)d1.xi;
   const double prob = scale_p * large_xi * prob_jk;
   const double phi_coll = cleo_rng_to_unit(cleo_rng_u64(key, slot_pairs + 2ull * jj));
   const double phi_out = cleo_rng_to_unit(cleo_rng_u64(key, slot_pairs + 2ull * jj + 1));
-  return enact_collision(p, d1, d2, prob, phi_coll, phi_out, w);
+  // the pair's terminal velocities are the flag's too when both are Simmel's (pair_tv)
+  const bool tv_known = p.coll_prob == CLEO_PROB_LONG && p.flag_tv == CLEO_TV_SIMMEL;
+  return enact_collision(p, d1, d2, prob, phi_coll, phi_out, w, tv_known, tv1, tv2);
 }
 
 // Fisher-Yates (shuffle.hpp:80-87) applies swap(p[i], p[J[i]]) for i = n-1 down to 1 to the

@@ -251,24 +251,28 @@ __device__ __forceinline__ double nfrags_of(const cleo_b200_params& p, double r1
 }
 // The outcomes of a collision (flag, coalescence, breakup) run only for the pairs that collide;
 // kept out of line, they stay out of the collision kernels' hot loops and instruction caches.
+// tv1, tv2: terminalv(p.flag_tv, r1) and terminalv(p.flag_tv, r2) when tv_known (a caller that
+// already holds them), else evaluated here
 static __device__ __noinline__ unsigned coalbure_flag(const cleo_b200_params& p, double phi,
-                                                      double r1, double r2) {  // coalbure_flag.hpp:42-198
+                                                      double r1, double r2, bool tv_known,
+                                                      double tv1, double tv2) {  // coalbure_flag.hpp:42-198
+  if (!tv_known && p.flag_kind != CLEO_FLAG_CONST) {
+    tv1 = terminalv(p.flag_tv, r1);
+    tv2 = terminalv(p.flag_tv, r2);
+  }
   switch (p.flag_kind) {
     case CLEO_FLAG_STRAUB: {
-      const double cke = collision_kinetic_energy(r1, r2, terminalv(p.flag_tv, r1),
-                                                  terminalv(p.flag_tv, r2));
+      const double cke = collision_kinetic_energy(r1, r2, tv1, tv2);
       return (phi < ecoal_straub2010(r1, r2, cke)) ? 1u : 2u;
     }
     case CLEO_FLAG_TESTIKSTRAUB: {
-      const double cke = collision_kinetic_energy(r1, r2, terminalv(p.flag_tv, r1),
-                                                  terminalv(p.flag_tv, r2));
+      const double cke = collision_kinetic_energy(r1, r2, tv1, tv2);
       if (cke < surfenergy(fmin(r1, r2))) return (phi < ecoal_straub2010(r1, r2, cke)) ? 1u : 0u;
       if (cke < surfenergy(fmax(r1, r2))) return (phi < ecoal_straub2010(r1, r2, cke)) ? 1u : 2u;
       return 2u;
     }
     case CLEO_FLAG_SZAKALLURBICH: {
-      const double cke = collision_kinetic_energy(r1, r2, terminalv(p.flag_tv, r1),
-                                                  terminalv(p.flag_tv, r2));
+      const double cke = collision_kinetic_energy(r1, r2, tv1, tv2);
       if (cke < surfenergy(fmin(r1, r2))) return 0u;
       if (cke < coal_surfenergy(r1, r2)) return 1u;
       return 2u;
@@ -288,6 +292,7 @@ __device__ __forceinline__ uint64_t coalescence_gamma(uint64_t xi1, uint64_t xi2
                                                       double phi) {  // :68-79
   uint64_t gamma = (uint64_t)floor(prob);
   if (phi < (prob - (double)gamma)) ++gamma;
+  if (gamma == 0) return 0;  // fmin(0, maxgamma) is 0: the 64-bit division only when it matters
   const uint64_t maxgamma = xi1 / xi2;
   return (uint64_t)fmin((double)gamma, (double)maxgamma);
 }
@@ -403,9 +408,11 @@ static __device__ __noinline__ uint32_t breakup_pair(const cleo_b200_params& p, 
 
 // Enact the collision of a pair (already ordered so that d1.xi >= d2.xi): returns the number of
 // superdroplets made null. coalescence.cpp:39-54, breakup.hpp:140-166, coalbure.hpp:207-256.
+// tv_known, tv1, tv2: the flag's terminal velocities of d1 and d2 when the caller holds them
 __device__ __forceinline__ uint32_t enact_collision(const cleo_b200_params& p, Drop& d1, Drop& d2,
                                                    double prob, double phi_coll, double phi_out,
-                                                   const Where& w) {
+                                                   const Where& w, bool tv_known = false,
+                                                   double tv1 = 0.0, double tv2 = 0.0) {
   if (p.coll_enact == CLEO_ENACT_COALESCENCE) {
     const uint64_t gamma = coalescence_gamma(d1.xi, d2.xi, prob, phi_coll);
     if (gamma != 0) return coalesce_pair(gamma, d1, d2, w);
@@ -417,7 +424,7 @@ __device__ __forceinline__ uint32_t enact_collision(const cleo_b200_params& p, D
   }
   const uint64_t gamma = coalescence_gamma(d1.xi, d2.xi, prob, phi_coll);
   if (gamma != 0) {
-    const unsigned flag = coalbure_flag(p, phi_out, d1.r, d2.r);
+    const unsigned flag = coalbure_flag(p, phi_out, d1.r, d2.r, tv_known, tv1, tv2);
     if (flag == 1u) return coalesce_pair(gamma, d1, d2, w);
     if (flag == 2u) return breakup_pair(p, d1, d2, w);
   }

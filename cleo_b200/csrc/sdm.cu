@@ -84,6 +84,7 @@ struct DevCtx {
   // positions, the stayers, and the new gridbox starts (ngbxs + 2)
   uint32_t *mv_scan, *mv_leave, *mv_arrive, *mv_below, *mv_stay, *gstart_new, *mv_mstart,
       *mv_shift;
+  uint32_t* mv_tsums;  // the flag scan's tile offsets (the scan's readers add them: mv_before)
   uint32_t* mv_total;  // valid superdroplets that changed gridbox in the last motion step
   // scratch
   double *scr_r, *scr_m, *scr_c3, *scr_c1, *scr_c2;
@@ -119,7 +120,7 @@ struct cleo_b200_ctx {
   int device = 0;
   // sort scratch
   uint32_t *keys[2], *vals[2], *hist, *tile_sums;
-  uint32_t *mv_tsums = nullptr, *mv_count = nullptr;  // incremental re-sort scratch
+  uint32_t *gs_tsums = nullptr, *mv_count = nullptr;  // incremental re-sort scratch
   // re-sort choice: {movers, superdroplets} of the last motion step in mapped pinned memory,
   // written by the device and read by the host without synchronisation (a value one step old
   // only changes which of the two equal-result sorts runs)
@@ -448,12 +449,17 @@ __global__ void k_mv_report(DevCtx c, uint32_t* __restrict__ out) {  // mapped h
 // key unchanged: gcount[k] less the valid ones that left), the movers into k from positions
 // after it; out-of-domain ones and nulls follow all gridboxes in position order. Only the
 // movers are sorted.
+// the exclusive scan of the mover flags at position i: the scan within its tile plus the tile's
+// offset (the scan's own pass adding the offsets in place is left out; its readers add them)
+__device__ __forceinline__ uint32_t mv_before(const DevCtx& c, uint32_t i) {
+  return c.mv_scan[i] + c.mv_tsums[i / SCAN_TILE];
+}
 __global__ void k_mv_list(DevCtx c, const uint32_t* __restrict__ keys, uint32_t* __restrict__ mk,
                           uint32_t* __restrict__ mvp) {
   const uint32_t n = c.counters[0];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t p = c.mv_scan[i];
-    if (c.mv_scan[i + 1] != p) {  // a mover: the exclusive scan steps over it
+    const uint32_t p = mv_before(c, i);
+    if (mv_before(c, i + 1) != p) {  // a mover: the exclusive scan steps over it
       mk[p] = keys[i];
       mvp[p] = i;
     }
@@ -470,7 +476,7 @@ __global__ void k_mv_ends(DevCtx c) {  // after the scan: gstart_new[ngbxs] = in
   c.gstart_new[c.ngbxs + 1] = c.counters[0];
 }
 __global__ void k_mv_count(DevCtx c, uint32_t* __restrict__ count) {  // number of movers
-  *count = c.mv_scan[c.counters[0]];
+  *count = mv_before(c, c.counters[0]);
 }
 __global__ void k_mv_arrivals(DevCtx c) {  // to be scanned: first sorted mover of each key
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x)
@@ -495,7 +501,7 @@ __global__ void k_mv_shift_commit(DevCtx c) {
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ng + 2; k += gridDim.x * blockDim.x) {
     if (k < ng) {
       const uint32_t g0 = c.gstart[k];
-      c.mv_shift[k] = c.gstart_new[k] + c.mv_below[k] - g0 + c.mv_scan[g0];
+      c.mv_shift[k] = c.gstart_new[k] + c.mv_below[k] - g0 + mv_before(c, g0);
     }
     c.gstart[k] = c.gstart_new[k];
   }
@@ -515,8 +521,8 @@ k_mv_stayers(DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ keys
       const uint32_t i = i0 + u * stride;
       ok[u] = i < n;
       if (ok[u]) {
-        m[u] = c.mv_scan[i];
-        m1[u] = c.mv_scan[i + 1];
+        m[u] = mv_before(c, i);
+        m1[u] = mv_before(c, i + 1);
         g[u] = keys[i];
         gb[u] = src.gbx[i];
         c3[u] = src.c3[i];
@@ -546,7 +552,7 @@ k_mv_stayers(DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ keys
 __global__ void k_mv_movers(DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ mk,
                             const uint32_t* __restrict__ mvp) {
   const uint32_t n = c.counters[0];
-  const uint32_t nm = c.mv_scan[n];
+  const uint32_t nm = mv_before(c, n);
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nm; j += gridDim.x * blockDim.x) {
     const uint32_t k = mk[j];
     const uint32_t r = j - c.mv_mstart[k];  // rank among the sorted movers of key k
@@ -1210,10 +1216,10 @@ int sort_incremental(cleo_b200_ctx* x) {
   const uint32_t nscan = (uint32_t)((n1 + SCAN_TILE - 1) / SCAN_TILE);
   // exclusive scan of capacity + 1 flags (entries past nrange are stale but only move the
   // values after index nrange, which nothing reads)
-  k_scan_tiles<<<nscan, SCAN_THREADS, 0, s>>>(d.mv_scan, d.mv_scan, n1, x->mv_tsums);
-  k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(x->mv_tsums, nscan, nullptr);
-  k_scan_add<<<(unsigned)((n1 + 255) / 256), 256, 0, s>>>(d.mv_scan, n1, x->mv_tsums);
-  x->launches += 3;
+  // (readers add the tile offsets: mv_before)
+  k_scan_tiles<<<nscan, SCAN_THREADS, 0, s>>>(d.mv_scan, d.mv_scan, n1, d.mv_tsums);
+  k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(d.mv_tsums, nscan, nullptr);
+  x->launches += 2;
   const int gc = grid_for(d.capacity, 256), gg = grid_for((size_t)ng + 2, 256);
   k_mv_list<<<gc, 256, 0, s>>>(d, x->keys[0], x->keys[1], x->vals[1]);
   k_mv_count<<<1, 1, 0, s>>>(d, x->mv_count);
@@ -1229,9 +1235,9 @@ int sort_incremental(cleo_b200_ctx* x) {
   k_mv_arrivals<<<gg, 256, 0, s>>>(d);
   const uint32_t ns2 = (uint32_t)(((uint64_t)ng + SCAN_TILE - 1) / SCAN_TILE);
   for (uint32_t* arr : {d.gstart_new, d.mv_mstart}) {
-    k_scan_tiles<<<ns2 ? ns2 : 1, SCAN_THREADS, 0, s>>>(arr, arr, ng, x->mv_tsums);
-    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(x->mv_tsums, ns2 ? ns2 : 1, arr + ng);
-    k_scan_add<<<(unsigned)((ng + 255) / 256 + 1), 256, 0, s>>>(arr, ng, x->mv_tsums);
+    k_scan_tiles<<<ns2 ? ns2 : 1, SCAN_THREADS, 0, s>>>(arr, arr, ng, x->gs_tsums);
+    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(x->gs_tsums, ns2 ? ns2 : 1, arr + ng);
+    k_scan_add<<<(unsigned)((ng + 255) / 256 + 1), 256, 0, s>>>(arr, ng, x->gs_tsums);
   }
   k_mv_ends<<<1, 1, 0, s>>>(d);
   x->launches += 9;
@@ -1642,7 +1648,8 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &x->mv_count, 1);
   {
     const size_t a = ((size_t)cap + 1 + SCAN_TILE - 1) / SCAN_TILE, b = ((size_t)ng + SCAN_TILE) / SCAN_TILE;
-    rc |= dalloc(x, &x->mv_tsums, (a > b ? a : b) + 1);
+    rc |= dalloc(x, &d.mv_tsums, a + 1);
+    rc |= dalloc(x, &x->gs_tsums, b + 1);
   }
   if (params->monitors) {
     for (int r = 0; r < 2; ++r) {
