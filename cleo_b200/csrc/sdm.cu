@@ -151,7 +151,8 @@ struct cleo_b200_ctx {
   uint32_t *obs_start = nullptr, *obs_tsums = nullptr;
   uint32_t ntiles_max, key_bits;
   BatchScratch bs{};              // batched-schedule scratch
-  int grid_small[2][2] = {{0, 0}, {0, 0}};  // warp kernel [64 / 128 slots][2 / 3 CTAs per SM]
+  int grid_small[2] = {0, 0};  // the 64-slot warp kernel at [2 / 3 CTAs per SM]
+  int grid_wide = 0;            // the 128-slot warp kernel (2 CTAs per SM)
   int grid_medium = 0, grid_large = 0, grid_flat = 0;
   int grid_condb[3] = {0, 0, 0};  // pass B at 3, 4, 5 resident CTAs per SM
   unsigned long long launches = 0;  // kernels launched by this context
@@ -171,7 +172,7 @@ struct cleo_b200_ctx {
     int cond_minb;        // pass-A variant (3, 4 or 5): resident 256-thread CTAs per SM it is
                           // compiled for
     uint32_t small_max;   // gridboxes up to this size go to the warp kernel
-    int small_minb;       // warp-kernel variant: resident CTAs per SM it is compiled for
+    int small_minb;       // 64-slot warp kernel: resident CTAs per SM it is compiled for
   };
   TuneCfg cfg{256, 3, SMALL_MAX, 2};
   std::vector<TuneCfg> cand;
@@ -304,8 +305,10 @@ k_motion(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, int
     const uint32_t g = c.sd.gbx[i];
     if (!incremental) vals[i] = i;
     if (g >= ng) {  // null superdroplet left by collisions: out of the domain
-      keys[i] = ng;
-      if (incremental) c.mv_scan[i] = 1;  // a mover, not one of its range's valid superdroplets
+      if (incremental)
+        c.mv_scan[i] = 1;  // a mover, not one of its range's valid superdroplets
+      else
+        keys[i] = ng;
       continue;
     }
     const Where w{c.err, g, i};
@@ -418,7 +421,7 @@ k_motion(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, int
       if (bad) w.fail(CLEO_ERR_OUT_OF_BOX);
     }
     const uint32_t key = idx < ng ? idx : ng;
-    keys[i] = key;
+    if (!incremental) keys[i] = key;  // the incremental re-sort takes min(gbx, ngbxs) instead
     // a superdroplet that changes gridbox (or leaves the domain) moves in the re-sort
     const bool mover = key != g;
     {  // count them (warp-aggregated) for the choice of the next re-sort
@@ -454,13 +457,14 @@ __global__ void k_mv_report(DevCtx c, uint32_t* __restrict__ out) {  // mapped h
 __device__ __forceinline__ uint32_t mv_before(const DevCtx& c, uint32_t i) {
   return c.mv_scan[i] + c.mv_tsums[i / SCAN_TILE];
 }
-__global__ void k_mv_list(DevCtx c, const uint32_t* __restrict__ keys, uint32_t* __restrict__ mk,
-                          uint32_t* __restrict__ mvp) {
+// the movers' keys: min(gbx, ngbxs) of the gridbox indices k_motion wrote
+__global__ void k_mv_list(DevCtx c, uint32_t* __restrict__ mk, uint32_t* __restrict__ mvp) {
   const uint32_t n = c.counters[0];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t p = mv_before(c, i);
     if (mv_before(c, i + 1) != p) {  // a mover: the exclusive scan steps over it
-      mk[p] = keys[i];
+      const uint32_t gbx = c.sd.gbx[i];
+      mk[p] = gbx < c.ngbxs ? gbx : c.ngbxs;
       mvp[p] = i;
     }
   }
@@ -507,12 +511,12 @@ __global__ void k_mv_shift_commit(DevCtx c) {
   }
 }
 __global__ void __launch_bounds__(256)
-k_mv_stayers(DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ keys) {
+k_mv_stayers(DevCtx c, Fields src, Fields dst) {
   constexpr int U = 2;  // superdroplets per thread and iteration, all loads issued first
   const uint32_t n = c.counters[0];
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += U * stride) {
-    uint32_t m[U], m1[U], g[U], gb[U];
+    uint32_t m[U], m1[U], gb[U];
     double c3[U], c1[U], c2[U], r[U], ms[U];
     unsigned long long xi[U], id[U];
     bool ok[U];
@@ -523,8 +527,7 @@ k_mv_stayers(DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ keys
       if (ok[u]) {
         m[u] = mv_before(c, i);
         m1[u] = mv_before(c, i + 1);
-        g[u] = keys[i];
-        gb[u] = src.gbx[i];
+        gb[u] = src.gbx[i];  // a stayer's key: its gridbox, unchanged
         c3[u] = src.c3[i];
         c1[u] = src.c1[i];
         c2[u] = src.c2[i];
@@ -537,7 +540,7 @@ k_mv_stayers(DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ keys
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (!ok[u] || m1[u] != m[u]) continue;  // beyond the range, or a mover
-      const uint32_t o = i0 + u * stride - m[u] + c.mv_shift[g[u]];
+      const uint32_t o = i0 + u * stride - m[u] + c.mv_shift[gb[u]];
       dst.gbx[o] = gb[u];
       dst.c3[o] = c3[u];
       dst.c1[o] = c1[u];
@@ -1221,7 +1224,7 @@ int sort_incremental(cleo_b200_ctx* x) {
   k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(d.mv_tsums, nscan, nullptr);
   x->launches += 2;
   const int gc = grid_for(d.capacity, 256), gg = grid_for((size_t)ng + 2, 256);
-  k_mv_list<<<gc, 256, 0, s>>>(d, x->keys[0], x->keys[1], x->vals[1]);
+  k_mv_list<<<gc, 256, 0, s>>>(d, x->keys[1], x->vals[1]);
   k_mv_count<<<1, 1, 0, s>>>(d, x->mv_count);
   x->launches += 2;
   // mover count = mv_scan[nrange]: read by the radix kernels through a device pointer
@@ -1244,7 +1247,7 @@ int sort_incremental(cleo_b200_ctx* x) {
   Fields& src = x->buf[x->cur];
   Fields& dst = x->buf[1 - x->cur];
   k_mv_shift_commit<<<gg, 256, 0, s>>>(d);
-  k_mv_stayers<<<gc, 256, 0, s>>>(d, src, dst, x->keys[0]);
+  k_mv_stayers<<<gc, 256, 0, s>>>(d, src, dst);
   k_mv_movers<<<gc, 256, 0, s>>>(d, src, dst, mk, mvp);
   x->launches += 3;
   x->cur = 1 - x->cur;
@@ -1352,13 +1355,12 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       const int ci = cond ? 1 : 0, li = coll ? 1 : 0;
       constexpr uint32_t SW = SmallLayout<WARP_MAX>::BYTES, SS = SmallLayout<SMALL_MAX>::BYTES;
       if (m3)
-        k_b_small<3, SMALL_MAX><<<x->grid_small[0][1], B_THREADS, SS, s>>>(d, b, ci, li, 0);
+        k_b_small<3, SMALL_MAX><<<x->grid_small[1], B_THREADS, SS, s>>>(d, b, ci, li, 0);
       else
-        k_b_small<2, SMALL_MAX><<<x->grid_small[0][0], B_THREADS, SS, s>>>(d, b, ci, li, 0);
-      if (wide && m3)
-        k_b_small<3, WARP_MAX><<<x->grid_small[1][1], B_THREADS, SW, s>>>(d, b, ci, li, 1);
-      else if (wide)
-        k_b_small<2, WARP_MAX><<<x->grid_small[1][0], B_THREADS, SW, s>>>(d, b, ci, li, 1);
+        k_b_small<2, SMALL_MAX><<<x->grid_small[0], B_THREADS, SS, s>>>(d, b, ci, li, 0);
+      // the 128-slot variant at 2 CTAs per SM whatever the 64-slot one's budget: at 3 it spills
+      // (measured: collisions 3.87 ms with both at 2, 3.67 ms with the 64-slot one at 3)
+      if (wide) k_b_small<2, WARP_MAX><<<x->grid_wide, B_THREADS, SW, s>>>(d, b, ci, li, 1);
       x->launches += wide;
       k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_SMEM, s>>>(d, b, cond ? 1 : 0,
                                                                            coll ? 1 : 0);
@@ -1727,20 +1729,15 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, SS));
     CUDA_TRY(cudaFuncSetAttribute(k_b_small<2, WARP_MAX>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, SW));
-    CUDA_TRY(cudaFuncSetAttribute(k_b_small<3, WARP_MAX>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SW));
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<2, SMALL_MAX>,
                                                            B_THREADS, SS));
-    x->grid_small[0][0] = sms * (occ > 0 ? occ : 1);
+    x->grid_small[0] = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<3, SMALL_MAX>,
                                                            B_THREADS, SS));
-    x->grid_small[0][1] = sms * (occ > 0 ? occ : 1);
+    x->grid_small[1] = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<2, WARP_MAX>,
                                                            B_THREADS, SW));
-    x->grid_small[1][0] = sms * (occ > 0 ? occ : 1);
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_small<3, WARP_MAX>,
-                                                           B_THREADS, SW));
-    x->grid_small[1][1] = sms * (occ > 0 ? occ : 1);
+    x->grid_wide = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<false>, B_THREADS,
                                                            (size_t)MEDIUM_SMEM));
     x->grid_medium = sms * (occ > 0 ? occ : 1);

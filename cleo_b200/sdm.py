@@ -185,7 +185,8 @@ def _main(argv=None):
     ap.add_argument("--plain", action="store_true", help="the plain schedule (default batched)")
     ap.add_argument("--launch-config", type=int, nargs=4, default=None,
                     help="pass-A block, pass-A CTAs per SM, warp-kernel gridbox limit, "
-                         "warp-kernel CTAs per SM (cleo_b200_set_launch_config)")
+                         "CTAs per SM of the warp kernel's 64-slot variant "
+                         "(cleo_b200_set_launch_config)")
     a = ap.parse_args(argv)
     build = W.uneven3d if a.workload == "uneven3d" else W.bubble3d
     w = build(ndims=tuple(a.ndims))

@@ -403,8 +403,9 @@ int cleo_b200_set_graphs(cleo_b200_ctx* ctx, int on);
  * SDM steps run as ordinary steps (same results) while each times one of four candidate launch
  * configurations per stage: for condensation pass A, the block size (128 or 256) and the
  * compiled variant's resident-CTA target (4 or 5 per SM, i.e. its register budget); for
- * collisions, the largest gridbox of the warp-per-gridbox kernel (64 or 128) and that kernel's
- * resident-CTA target (2 or 3). The fastest option of each stage is kept, and cached per process
+ * collisions, the largest gridbox of the warp-per-gridbox kernel (64 or 128) and the resident-CTA
+ * target (2 or 3) of its 64-slot variant (the 128-slot variant, for gridboxes of 65..128
+ * superdroplets, runs at 2). The fastest option of each stage is kept, and cached per process
  * by GPU name and domain size so that later contexts of that size start from it. Steps run
  * eagerly (with a stream synchronisation each) while tuning.
  */
@@ -414,7 +415,8 @@ int cleo_b200_autotune(cleo_b200_ctx* ctx, int reps);
 int cleo_b200_tuned_config(cleo_b200_ctx* ctx, int32_t cfg[4]);
 /* Set that configuration directly (ending a tuning run in progress): pass-A block 128 or 256,
  * pass-A CTA target 3, 4 or 5, warp-kernel gridbox limit 1..128 (gridboxes above it go to the
- * CTA-per-gridbox kernels), warp-kernel CTA target 2 or 3. Results do not depend on it. */
+ * CTA-per-gridbox kernels), CTA target 2 or 3 of the warp kernel's 64-slot variant. Results do
+ * not depend on it. */
 int cleo_b200_set_launch_config(cleo_b200_ctx* ctx, const int32_t cfg[4]);
 
 /*
