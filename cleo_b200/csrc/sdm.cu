@@ -273,6 +273,11 @@ __device__ __forceinline__ void bounds_of(const double* lo, const double* hi, ui
 // interpolation: predcorr.cpp:30-42
 __device__ __forceinline__ double interpolation(double blo, double bhi, double vlo, double vhi,
                                                 double sdcoord) {
+  // zero wind on both faces: with a finite positive extent the clamped coordinate gives alpha in
+  // [0, 1], so alpha * vhi + (1 - alpha) * vlo is exactly vhi + vlo (signed zeros included),
+  // without the division
+  const double extent = bhi - blo;
+  if (vlo == 0.0 && vhi == 0.0 && extent > 0.0 && extent <= DBLMAX) return vhi + vlo;
   const double coord = fmin(bhi, fmax(blo, sdcoord));
   const double alpha = (coord - blo) / (bhi - blo);
   return alpha * vhi + (1 - alpha) * vlo;
