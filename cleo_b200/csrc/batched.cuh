@@ -51,19 +51,20 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
 }
 
 // ---- effect_on_hydrometeor_states (movesupersindomain.hpp:95-136) ----
-// A warp takes 32 consecutive gridboxes: it sums their condensate one gridbox at a time over its
-// lanes (each lane in the order of its superdroplets, then the warp's fixed reduction tree; the
-// next gridbox's first 32 superdroplets are loaded while the current one is reduced), lane j
-// keeps gridbox j's sum, and the 32 gridboxes' qcond are then computed side by side, one per lane.
-__global__ void k_b_qcond(DevCtx c) {
+// A warp takes `batch` (1..32) consecutive gridboxes: it sums their condensate one gridbox at a
+// time over its lanes (each lane in the order of its superdroplets, then the warp's fixed
+// reduction tree; the next gridbox's first 32 superdroplets are loaded while the current one is
+// reduced), lane j keeps gridbox j's sum, and the batch's qcond values are then computed side by
+// side, one per lane. The host sizes the batch so that the warps still fill the GPU.
+__global__ void k_b_qcond(DevCtx c, uint32_t batch) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
-  for (uint32_t g0 = warp * 32u; g0 < c.ngbxs; g0 += nwarps * 32u) {
+  for (uint32_t g0 = warp * batch; g0 < c.ngbxs; g0 += nwarps * batch) {
+    const uint32_t nb = c.ngbxs - g0 < batch ? c.ngbxs - g0 : batch;
     const uint32_t gl = g0 + lane;
-    const bool own = gl < c.ngbxs;
+    const bool own = (uint32_t)lane < nb;
     const uint32_t my_base = own ? c.gstart[gl] : 0u, my_n = own ? c.gcount[gl] : 0u;
-    const uint32_t nb = c.ngbxs - g0 < 32u ? c.ngbxs - g0 : 32u;
     uint32_t base = __shfl_sync(0xFFFFFFFFu, my_base, 0), n = __shfl_sync(0xFFFFFFFFu, my_n, 0);
     double r = 0.0, ms = 0.0;
     unsigned long long xi = 0;

@@ -1305,9 +1305,13 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
   StageMark m(x, 2);
   const int gg = grid_for(d.ngbxs, 256);
   if (did_motion) {
-    const size_t batches = ((size_t)d.ngbxs + 31) / 32;  // a warp per 32 gridboxes
-    const size_t warps = batches < 1 ? 1 : (batches < (size_t)148 * 64 ? batches : (size_t)148 * 64);
-    k_b_qcond<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(d);
+    // gridboxes per warp: up to 32, as many as leave 64 warps per SM busy
+    const size_t full = (size_t)148 * 64;
+    size_t batch = ((size_t)d.ngbxs + full - 1) / full;
+    batch = batch < 1 ? 1 : (batch > 32 ? 32 : batch);
+    const size_t batches = ((size_t)d.ngbxs + batch - 1) / batch;
+    const size_t warps = batches < 1 ? 1 : (batches < full ? batches : full);
+    k_b_qcond<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(d, (uint32_t)batch);
     x->launches += 1;
   }
   k_b_reset<<<gg, 256, 0, s>>>(d, b, 1);
