@@ -111,8 +111,9 @@ def test_launch_configs_match_oracle(lib, cfg):
         o.run_step(k * w["tstep"], (k + 1) * w["tstep"])
     g.check()
     K.assert_same_domain(g.download_supers(), o.download_supers(), rtol=1e-12, what=str(cfg))
-    bad = (C.c_int32 * 4)(256, 3, 129, 2)
-    assert lib.cleo_b200_set_launch_config(g.ctx, bad) == abi.CODE["CLEO_ERR_ARGUMENT"]
+    for bad_cfg in ((256, 3, 129, 2), (256, 3, 64, 4)):
+        bad = (C.c_int32 * 4)(*bad_cfg)
+        assert lib.cleo_b200_set_launch_config(g.ctx, bad) == abi.CODE["CLEO_ERR_ARGUMENT"]
 
 
 def test_async_state_upload_matches_sync(lib):
