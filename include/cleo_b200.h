@@ -410,8 +410,8 @@ int cleo_b200_set_graphs(cleo_b200_ctx* ctx, int on);
  * eagerly (with a stream synchronisation each) while tuning.
  */
 int cleo_b200_autotune(cleo_b200_ctx* ctx, int reps);
-/* Current configuration {pass-A block, pass-A CTA target, warp-kernel gridbox limit, warp-kernel
- * CTA target}; returns 1 while tuning is still in progress, else CLEO_OK. */
+/* Current configuration {pass-A block, pass-A CTA target, warp-kernel gridbox limit, CTA target of
+ * the warp kernel's 64-slot variant}; returns 1 while tuning is still in progress, else CLEO_OK. */
 int cleo_b200_tuned_config(cleo_b200_ctx* ctx, int32_t cfg[4]);
 /* Set that configuration directly (ending a tuning run in progress): pass-A block 128 or 256,
  * pass-A CTA target 3, 4 or 5, warp-kernel gridbox limit 1..128 (gridboxes above it go to the
