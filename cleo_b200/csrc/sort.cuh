@@ -127,7 +127,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan_1024(uint32_t v, uint32
 
 // phase 1: scan each tile, write the tile's total
 __global__ void __launch_bounds__(SCAN_THREADS)
-k_scan_tiles(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint64_t n,
+k_scan_tiles(const uint32_t* in, uint32_t* out, uint64_t n,  // in == out: scanned in place
              uint32_t* __restrict__ tile_sums) {
   __shared__ uint32_t wsum[32];
   const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
