@@ -1,8 +1,10 @@
 // batched.cuh — the batched microphysics of one SDM step (exec_mode CLEO_EXEC_BATCHED).
 //
 // Same results as k_micro (one CTA per gridbox), scheduled for B200 occupancy:
-//   k_b_qcond      warp per gridbox: qcond from the moved superdroplets (after the sort)
-//   k_b_thermo     thread per gridbox: psat, supersaturation, diffusion factor, Kelvin factor
+//   k_b_qcond      warp per batch of up to 32 consecutive gridboxes: qcond from the moved
+//                  superdroplets (after the sort)
+//   k_b_thermo     thread per gridbox: psat, supersaturation, diffusion factor, the droplets'
+//                  Kohler factors that depend on temperature alone
 //   k_cond_a       thread per superdroplet: the mandatory two Newton iterations of every
 //                  implicit-Euler solve; solves needing more (sub-stepping, or a restart after two
 //                  unconverged iterations) are appended to a list keyed by their cost
@@ -14,12 +16,13 @@
 //   k_b_classify   gridboxes into size buckets (warp-aggregated atomics)
 //   k_b_small      persistent, warp per gridbox (n <= small_max <= 128; 64- and 128-slot
 //                  variants): reduction of the condensed mass and Newton iterations, state
-//                  update, collisions in registers + per-warp shared memory
+//                  update (32 gridboxes' updates side by side), collisions in registers +
+//                  per-warp shared memory
 //   k_b_cta<false> persistent, CTA per gridbox (small_max < n <= medium_max <= 1024): the same
 //                  with shared-memory staging
 //   k_b_cta<true>  CTA per gridbox (n > medium_max) with global scratch
 // small_max, the pass-A block size, the resident-CTA targets (register budgets) of pass A and of
-// the warp kernel are chosen by the autotuner (results do not depend on them).
+// the warp kernel's 64-slot variant are chosen by the autotuner (results do not depend on them).
 // Condensed mass per droplet goes through a scratch array and is summed per gridbox in a fixed
 // order, so budgets and states are deterministic.
 #pragma once
