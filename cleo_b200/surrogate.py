@@ -6,7 +6,7 @@ starts every Newton-Raphson iteration from ImplicitIterations::initialguess
 on pairs that the solver itself produces, on the GPU with the library's own forward/backward and
 Adam kernels, and attaches it to a context so that ``nr_seed = NRSEED_MLP`` starts the Newton
 iteration of the direct branch from the predicted post-step r^2. FP64 Newton polishing to the
-solver's own convergence test stays the judge of every result.
+solver's own convergence test still decides every result.
 
 Torch tensors are only device-memory plumbing here; all arithmetic runs in libcleo_b200.so.
 """
