@@ -188,3 +188,30 @@ def test_gpu_golovin_analytic(lib):
             g.run_step(t * 100, (t + 1) * 100)
         errs.append(golovin_l1(g.download_supers(), 1200))
     assert np.mean(errs) < 0.12, errs
+
+
+@pytest.mark.parametrize("ndims", [(16, 32, 32), (32, 64, 64)])
+def test_gpu_mid_size_domains_tuned_config(lib, ndims):
+    """Domains of 16,384 and 131,072 gridboxes (0.6 M and 5 M superdroplets) with the launch
+    configuration the autotuner picks on the 40 M-superdroplet workload: the qcond kernel takes 2
+    and 14 gridboxes per warp here (one on the smaller test domains), the warp collision kernel's
+    64-slot variant runs at 3 CTAs per SM and its 128-slot variant at 2. One step from identical
+    states: the per-gridbox sums' order differs from the oracle's in the last bits, which later
+    steps' condensation near activation could amplify in a rare droplet of a population this
+    large."""
+    w = W.uneven3d(ndims=ndims, seed=29)
+    w["params"].exec_mode = abi.EXEC_BATCHED
+    g = make_sdm(w, lib=lib)
+    cfg = (C.c_int32 * 4)(256, 5, 128, 3)
+    assert lib.cleo_b200_set_launch_config(g.ctx, cfg) == 0
+    o = make_sdm(w, lib=K.oracle_lib(), prefix="oc")
+    ts = w["tstep"]
+    g.run_step(0, ts)
+    o.run_step(0, ts)
+    g.check()
+    K.assert_same_domain(g.download_supers(), o.download_supers(), rtol=RTOL, what=str(ndims))
+    sg, so = g.download_state(), o.download_state()
+    for k in ("qcond", "qvap", "temp"):
+        assert K.max_rel(sg[k], so[k]) < RTOL, k
+    budget_close(g.download_budgets()[0], o.download_budgets()[0], str(ndims))
+    g.close()
