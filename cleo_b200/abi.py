@@ -51,6 +51,7 @@ NRSEED_REFERENCE, NRSEED_MLP = 0, 1
 EXEC_PLAIN, EXEC_BATCHED = 0, 1
 MLP_TCGEN05, MLP_MMA_SYNC, MLP_FP32 = 0, 1, 2
 MONITOR_MASSMOMENTS, MONITOR_RAINMASSMOMENTS, MONITOR_PRECIPITATION = 1, 2, 4
+NITERS_FAILED = 0x80000000  # or-ed into a batch solve's iteration count: that droplet aborted
 MLP_NFEATURES, MLP_NHIDDEN, MLP_NPARAMS, MLP_NNORM = 7, 64, 4737, 16
 # enum cleo_obs_var: superdroplet output variables, with their output types
 OBS_VARS = {"sdId": (1, np.uint32), "sdgbxindex": (2, np.uint32), "xi": (4, np.uint64),
@@ -281,7 +282,8 @@ def declare_api(lib: C.CDLL, prefix: str) -> C.CDLL:
 # Every symbol include/cleo_b200.h declares (checked by the CPU tests against the built library).
 EXPORTED = (
     "cleo_b200_create", "cleo_b200_destroy", "cleo_b200_upload_supers", "cleo_b200_upload_state",
-    "cleo_b200_step", "cleo_b200_status", "cleo_b200_domain_nsupers", "cleo_b200_download_supers",
+    "cleo_b200_step", "cleo_b200_status", "cleo_b200_clear_status", "cleo_b200_domain_nsupers",
+    "cleo_b200_download_supers",
     "cleo_b200_download_state", "cleo_b200_download_budgets", "cleo_b200_condensation_solve",
     "cleo_b200_stream", "cleo_b200_kernel_launches", "cleo_b200_set_profiling",
     "cleo_b200_stage_times", "cleo_b200_sort_by_gridbox_static", "cleo_b200_version",
@@ -342,6 +344,7 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
                            C.c_uint64, vp]),
             ("mlp_infer", [vp, C.c_size_t, vp, vp, C.c_int]),
             ("set_surrogate", [vp, vp]),
+            ("clear_status", [vp]),
             ("set_graphs", [vp, C.c_int]),
             ("autotune", [vp, C.c_int]),
             ("tuned_config", [vp, C.POINTER(C.c_int32)]),

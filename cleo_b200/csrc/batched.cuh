@@ -1,8 +1,8 @@
 // batched.cuh — the batched microphysics of one SDM step (exec_mode CLEO_EXEC_BATCHED).
 //
 // Same results as k_micro (one CTA per gridbox), scheduled for B200 occupancy:
-//   k_b_qcond      warp per batch of up to 32 consecutive gridboxes: qcond from the moved
-//                  superdroplets (after the sort)
+//   k_b_qcond      thread per gridbox: qcond from the moved superdroplets (after the sort), their
+//                  condensate masses added in order
 //   k_b_thermo     thread per gridbox: psat, supersaturation, diffusion factor, the droplets'
 //                  Kohler factors that depend on temperature alone
 //   k_cond_a       thread per superdroplet: the mandatory two Newton iterations of every
@@ -13,27 +13,24 @@
 //                  listed solves (the ones the reference guess did not settle in two iterations)
 //   k_cond_b       thread per listed solve, neighbouring lanes of similar cost, from the seed
 //                  where its residual beats the reference guess's
+//   k_b_commit     thread per gridbox: the condensed mass of its superdroplets added in their
+//                  order, their Newton iterations, and the state update
 //   k_b_classify   gridboxes into size buckets (warp-aggregated atomics)
 //   k_b_small      persistent, warp per gridbox (n <= small_max <= 128; 64- and 128-slot
-//                  variants): reduction of the condensed mass and Newton iterations, state
-//                  update (32 gridboxes' updates side by side), collisions in registers +
-//                  per-warp shared memory
+//                  variants): collisions in registers + per-warp shared memory
 //   k_b_cta<false> persistent, CTA per gridbox (small_max < n <= medium_max <= 1024): the same
 //                  with shared-memory staging
 //   k_b_cta<true>  CTA per gridbox (n > medium_max) with global scratch
 // small_max, the pass-A block size, the resident-CTA targets (register budgets) of pass A and of
 // the warp kernel's 64-slot variant are chosen by the autotuner (results do not depend on them).
-// Condensed mass per droplet goes through a scratch array and is summed per gridbox in a fixed
-// order, so budgets and states are deterministic.
+// Every per-gridbox sum of doubles adds its terms in the superdroplets' order, as the reference's
+// sequential loop does (seq_sum): condensed mass per droplet goes through a scratch array and is
+// summed per gridbox after the solves, so budgets and states are the sequential loop's doubles
+// whatever the schedule.
 #pragma once
 
 namespace {
 
-__device__ __forceinline__ double warp_sum_d(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
-  return __shfl_sync(0xFFFFFFFFu, v, 0);
-}
 __device__ __forceinline__ uint32_t warp_sum_u(uint32_t v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
@@ -54,59 +51,28 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
 }
 
 // ---- effect_on_hydrometeor_states (movesupersindomain.hpp:95-136) ----
-// A warp takes `batch` (1..32) consecutive gridboxes: it sums their condensate one gridbox at a
-// time over its lanes (each lane in the order of its superdroplets, then the warp's fixed
-// reduction tree; the next gridbox's first 32 superdroplets are loaded while the current one is
-// reduced), lane j keeps gridbox j's sum, and the batch's qcond values are then computed side by
-// side, one per lane. The host sizes the batch so that the warps still fill the GPU.
-__global__ void k_b_qcond(DevCtx c, uint32_t batch) {
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  for (uint32_t g0 = warp * batch; g0 < c.ngbxs; g0 += nwarps * batch) {
-    const uint32_t nb = c.ngbxs - g0 < batch ? c.ngbxs - g0 : batch;
-    const uint32_t gl = g0 + lane;
-    const bool own = (uint32_t)lane < nb;
-    const uint32_t my_base = own ? c.gstart[gl] : 0u, my_n = own ? c.gcount[gl] : 0u;
-    uint32_t base = __shfl_sync(0xFFFFFFFFu, my_base, 0), n = __shfl_sync(0xFFFFFFFFu, my_n, 0);
-    double r = 0.0, ms = 0.0;
-    unsigned long long xi = 0;
-    if ((uint32_t)lane < n) r = c.sd.r[base + lane], ms = c.sd.msol[base + lane], xi = c.sd.xi[base + lane];
-    double mine = 0.0;
-    for (uint32_t j = 0; j < nb; ++j) {
-      uint32_t base_n = 0, n_n = 0;
-      double r_n = 0.0, ms_n = 0.0;
-      unsigned long long xi_n = 0;
-      if (j + 1 < nb) {  // uniform across the warp
-        base_n = __shfl_sync(0xFFFFFFFFu, my_base, j + 1);
-        n_n = __shfl_sync(0xFFFFFFFFu, my_n, j + 1);
-        if ((uint32_t)lane < n_n)
-          r_n = c.sd.r[base_n + lane], ms_n = c.sd.msol[base_n + lane], xi_n = c.sd.xi[base_n + lane];
-      }
-      const uint32_t g = g0 + j;
-      double m = 0.0;
-      if ((uint32_t)lane < n) m += condensate_mass(r, ms, Where{c.err, g, base + lane}) * (double)xi;
-      for (uint32_t k = lane + 32u; k < n; k += 32u) {
-        const Where w{c.err, g, base + k};
-        m += condensate_mass(c.sd.r[base + k], c.sd.msol[base + k], w) * (double)c.sd.xi[base + k];
-      }
-      m = warp_sum_d(m);
-      if ((uint32_t)lane == j) mine = m;
-      base = base_n, n = n_n, r = r_n, ms = ms_n, xi = xi_n;
-    }
-    if (own) {
-      const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
-      const double rho_cond = mine / c.volume[gl] * R0cubed_VOL0;
-      c.qcond[gl] = rho_cond / dry_air_density(c.press[gl], c.temp[gl], c.qvap[gl]);
-    }
+// A thread per gridbox adds its superdroplets' condensate masses in their order (seq_sum), the
+// reference's sequential loop, so qcond is the same double.
+__global__ void k_b_qcond(DevCtx c) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs;
+       g += gridDim.x * blockDim.x) {
+    const uint32_t base = c.gstart[g], n = c.gcount[g];
+    const double m = seq_sum(n, [&](uint32_t k) {
+      const uint32_t i = base + k;
+      return condensate_mass(c.sd.r[i], c.sd.msol[i], Where{c.err, g, i}) * (double)c.sd.xi[i];
+    });
+    const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
+    const double rho_cond = m / c.volume[g] * R0cubed_VOL0;
+    c.qcond[g] = rho_cond / dry_air_density(c.press[g], c.temp[g], c.qvap[g]);
   }
 }
 
 // ---- per-gridbox thermodynamics of superdroplets_change (condensation.cpp:43-59) ----
+// (every gridbox, empty ones too: the reference evaluates psat for each, and its check of the
+// temperature with it)
 __global__ void k_b_thermo(DevCtx c, BatchScratch b) {
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x) {
     if (g == 0) b.ctr[0] = b.ctr[9] = 0;  // deferred solves, of which restarts
-    if (c.gcount[g] == 0) continue;
     const Where w{c.err, g, c.gstart[g]};
     const double temp = c.temp[g];
     const double psat = saturation_pressure(temp, w);
@@ -304,6 +270,21 @@ __device__ __forceinline__ void cond_commit(DevCtx& c, uint32_t g, double totmas
   c.nr_iters[g] += totits;
 }
 
+// ---- the gridboxes' share of a condensation sub-step after its solves ----
+// A thread per gridbox: the condensed mass of its superdroplets added in their order (seq_sum,
+// the reference's sequential reduction, condensation.cpp:29-35), their Newton iterations, then
+// the state update (cond_commit). Empty gridboxes commit a zero change, as the reference's do.
+__global__ void k_b_commit(DevCtx c, BatchScratch b) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs;
+       g += gridDim.x * blockDim.x) {
+    const uint32_t base = c.gstart[g], n = c.gcount[g];
+    const double m = seq_sum(n, [&](uint32_t k) { return b.dm[base + k]; });
+    unsigned long long it = 0;
+    for (uint32_t k = 0; k < n; ++k) it += b.its[base + k];
+    cond_commit(c, g, m, it);
+  }
+}
+
 // one pair (2jj, 2jj+1) of the shuffled gridbox: collisions.hpp:140-158. tvA, tvB: pair_tv of
 // dA, dB.
 __device__ __forceinline__ uint32_t collide_pair(const cleo_b200_params& p, Drop& dA, Drop& dB,
@@ -387,7 +368,7 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 
 template <int MINB, int CAP>
 __global__ void __launch_bounds__(B_THREADS, MINB)
-k_b_small(DevCtx c, BatchScratch b, int cond, int coll, int q) {
+k_b_small(DevCtx c, BatchScratch b, int q) {
   using L = SmallLayout<CAP>;
   constexpr int H = CAP / 32;
   static_assert(CAP % 32 == 0 && CAP <= 255, "slot indices are stored as bytes");
@@ -428,47 +409,27 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll, int q) {
   uint32_t g_next = item < count ? list[item] : 0u;
   uint32_t parity = 0;  // bit k: the phase of bar[k] to wait for
   int cur = 0;
-  // condensation commits of up to 32 gridboxes, lane j holding the j-th, made side by side
-  // (after the 32nd and after the warp's last gridbox)
-  uint32_t pend_g = 0, pend_it = 0, npend = 0;
-  double pend_m = 0.0;
-  const auto commit_pending = [&]() {
-    if ((uint32_t)lane < npend) cond_commit(c, pend_g, pend_m, pend_it);
-    npend = 0;
-  };
-  if (coll) {
-    if (lane == 0) {
-      mbar_init(&bar[0], 1);
-      mbar_init(&bar[1], 1);
-      if (item < count) stage(0, g_next);
-    }
-    __syncwarp();
+  if (lane == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    if (item < count) stage(0, g_next);
   }
+  __syncwarp();
   for (; item < count; item += nwarps) {
     const uint32_t g = g_next;
     const bool has_next = item + nwarps < count;
     if (has_next) g_next = list[item + nwarps];
     const uint32_t base = c.gstart[g];
     const uint32_t n = c.gcount[g];
-    if (cond) {
-      double m = 0.0;
-      uint32_t it = 0;
-      for (uint32_t k = lane; k < n; k += 32) {
-        m += b.dm[base + k];
-        it += b.its[base + k];
-      }
-      m = warp_sum_d(m);
-      it = warp_sum_u(it);
-      if ((uint32_t)lane == npend) pend_g = g, pend_m = m, pend_it = it;
-      if (++npend == 32u || !has_next) commit_pending();  // one call site: a smaller loop body
-    }
-    if (!coll) continue;
     // the next gridbox's copies go out before this one's wait
     if (has_next && lane == 0) stage(cur ^ 1, g_next);
     if (!mbar_wait_bounded(&bar[cur], (parity >> cur) & 1u, MBAR_TRIES)) {
+      // the step fails with CLEO_ERR_TIMEOUT; before the warp leaves, the copies still in flight
+      // into either buffer get a bounded wait to land
       if (lane == 0) Where{c.err, g, base}.fail(CLEO_ERR_TIMEOUT);
+      mbar_wait_bounded(&bar[cur], (parity >> cur) & 1u, MBAR_TRIES);
       if (has_next) mbar_wait_bounded(&bar[cur ^ 1], (parity >> (cur ^ 1)) & 1u, MBAR_TRIES);
-      return;  // the step fails with CLEO_ERR_TIMEOUT; pending commits are dropped
+      return;
     }
     parity ^= 1u << cur;
     const uint32_t off = base & 1u;
@@ -608,11 +569,9 @@ k_b_small(DevCtx c, BatchScratch b, int cond, int coll, int q) {
 // large: staged in global scratch arrays.
 template <bool LARGE>
 __global__ void __launch_bounds__(B_THREADS)
-k_b_cta(DevCtx c, BatchScratch b, int cond, int coll) {
+k_b_cta(DevCtx c, BatchScratch b) {
   const uint32_t t_sdm = *b.tsdm;
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ double shd[32];
-  __shared__ unsigned long long shu[32];
   __shared__ uint32_t shw[40];
   __shared__ uint32_t s_item;
   __shared__ uint64_t s_bar;  // completion of the medium path's bulk copies
@@ -637,18 +596,6 @@ k_b_cta(DevCtx c, BatchScratch b, int cond, int coll) {
     const uint32_t g = list[item];
     const uint32_t base = c.gstart[g];
     const uint32_t n = c.gcount[g];
-    if (cond) {
-      double m = 0.0;
-      unsigned long long it = 0;
-      for (uint32_t k = tid; k < n; k += B_THREADS) {
-        m += b.dm[base + k];
-        it += b.its[base + k];
-      }
-      const double totm = block_sum(m, shd);
-      const unsigned long long toti = block_sum(it, shu);
-      if (tid == 0) cond_commit(c, g, totm, toti);
-    }
-    if (!coll) continue;
     const uint64_t key = cleo_rng_key(p.seed, t_sdm, g);
     const uint64_t slot = b.slot[g];
     // medium: r, msol, xi staged in shared memory by bulk copies (TMA) from the even element at

@@ -71,12 +71,17 @@ __device__ __forceinline__ void record_error(DevError* e, int code, uint32_t gbx
   }
 }
 
-// context for error attribution of one droplet / pair
+// context for error attribution of one droplet / pair; `failed`, where set, also marks this
+// droplet's own failure (the batch solves report which droplets the reference would abort on)
 struct Where {
   DevError* err;
   uint32_t gbx;
   uint64_t index;
-  __device__ void fail(int code) const { record_error(err, code, gbx, index); }
+  uint32_t* failed = nullptr;
+  __device__ void fail(int code) const {
+    if (failed) *failed = 1u;
+    record_error(err, code, gbx, index);
+  }
 };
 
 // ---- SuperdropAttrs: superdrop_attrs.hpp:61-259, superdrop_attrs.cpp:34-62 ----

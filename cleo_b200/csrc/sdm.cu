@@ -121,11 +121,14 @@ struct cleo_b200_ctx {
   // sort scratch
   uint32_t *keys[2], *vals[2], *hist, *tile_sums;
   uint32_t *gs_tsums = nullptr, *mv_count = nullptr;  // incremental re-sort scratch
-  // re-sort choice: {movers, superdroplets} of the last motion step in mapped pinned memory,
-  // written by the device and read by the host without synchronisation (a value one step old
-  // only changes which of the two equal-result sorts runs)
+  // re-sort choice: {movers, superdroplets} of the previous motion step, written by the device
+  // into mapped pinned memory right after that step's motion kernel; an event recorded behind
+  // the write (an external event node inside a captured step) lets the host wait for exactly
+  // that step's values before it chooses the next step's sort, so the choice is deterministic
   uint32_t* h_motion = nullptr;
   uint32_t* d_motion = nullptr;
+  cudaEvent_t ev_report = nullptr;
+  bool report_recorded = false;
   bool sort_full = false;
   // asynchronous state upload (cleo_b200_upload_state_async): staging area for the 11 state
   // fields, a copy stream, and events for "copied" and "taken by a step"
@@ -698,7 +701,27 @@ __global__ void k_grave_commit(DevCtx c) {
   c.counters[1] = nd;
 }
 
-// ---- block reductions (fixed order: warp shuffles then warps in order) ----
+// The sum of a gridbox's n terms in the superdroplets' order, the way the reference's
+// reductions add them (condensation.cpp:29-35 and movesupersindomain.hpp:125-131 state the
+// sequential loop as their meaning): one thread adds term(0), term(1), ... one after another.
+// Four terms are loaded before they are added, so the loads overlap the chain of additions; the
+// additions keep their order, so the result is the sequential loop's double.
+template <class Term>
+__device__ __forceinline__ double seq_sum(uint32_t n, Term term) {
+  double acc = 0.0;
+  uint32_t k = 0;
+  for (; k + 4 <= n; k += 4) {
+    const double t0 = term(k), t1 = term(k + 1), t2 = term(k + 2), t3 = term(k + 3);
+    acc += t0;
+    acc += t1;
+    acc += t2;
+    acc += t3;
+  }
+  for (; k < n; ++k) acc += term(k);
+  return acc;
+}
+
+// ---- block reductions (fixed order: warp shuffles then warps in order; integers) ----
 template <class T>
 __device__ __forceinline__ T block_sum(T v, T* sh) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -752,7 +775,6 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* wsum, 
 __global__ void __launch_bounds__(MICRO_THREADS)
 k_micro(DevCtx c, uint32_t t_sdm, uint32_t t_sdm_next, int did_motion) {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ double shd[32];
   __shared__ unsigned long long shu[32];
   __shared__ uint32_t shw[40];
   const cleo_b200_params& p = c.p;
@@ -760,20 +782,25 @@ k_micro(DevCtx c, uint32_t t_sdm, uint32_t t_sdm_next, int did_motion) {
   for (uint32_t g = blockIdx.x; g < c.ngbxs; g += gridDim.x) {
     const uint32_t base = c.gstart[g];
     uint32_t n = c.gcount[g];
+    // per-superdroplet terms of the gridbox's sums (shared memory, or the gridbox's range of the
+    // global scratch beyond NSMEM), added in order by thread 0 (seq_sum)
+    double* terms = n <= NSMEM ? reinterpret_cast<double*>(smem) : c.scr_r + base;
     // effect_on_hydrometeor_states after motion (movesupersindomain.hpp:95-136)
     if (did_motion) {
-      double m = 0.0;
       for (uint32_t k = tid; k < n; k += blockDim.x) {
         const Where w{c.err, g, base + k};
-        m += condensate_mass(c.sd.r[base + k], c.sd.msol[base + k], w) * (double)c.sd.xi[base + k];
+        terms[k] = condensate_mass(c.sd.r[base + k], c.sd.msol[base + k], w) *
+                   (double)c.sd.xi[base + k];
       }
-      const double totmass_cond = block_sum(m, shd);
+      __syncthreads();
       if (tid == 0) {
+        const double totmass_cond = seq_sum(n, [&](uint32_t k) { return terms[k]; });
         const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
         const double rho_cond = totmass_cond / c.volume[g] * R0cubed_VOL0;
         const double rho_dry = dry_air_density(c.press[g], c.temp[g], c.qvap[g]);
         c.qcond[g] = rho_cond / rho_dry;
       }
+      __syncthreads();
     }
     const uint64_t key = cleo_rng_key(p.seed, t_sdm, g);
     uint64_t slot = 0;
@@ -787,7 +814,7 @@ k_micro(DevCtx c, uint32_t t_sdm, uint32_t t_sdm_next, int did_motion) {
         const double s_ratio = supersaturation_ratio(c.press[g], c.qvap[g], psat);
         const double ffactor = diffusion_factor(c.press[g], temp, psat);
         const NewtonCfg cfg{p.maxniters, p.rtol, p.atol};
-        double dm = 0.0;
+        double* dm = terms;  // (n only shrinks within the step: the choice of storage holds)
         unsigned long long its = 0;
         for (uint32_t k = tid; k < n; k += blockDim.x) {
           const uint32_t i = base + k;
@@ -801,12 +828,12 @@ k_micro(DevCtx c, uint32_t t_sdm, uint32_t t_sdm_next, int did_motion) {
                                                  akoh, bkoh, ffactor, r, 0.0, ni, w);
           const double rnew = max_dryradius(newr, msol);  // change_radius
           c.sd.r[i] = rnew;
-          dm += (condensate_mass(rnew, msol, w) - old_m_cond) * (double)c.sd.xi[i];
+          dm[k] = (condensate_mass(rnew, msol, w) - old_m_cond) * (double)c.sd.xi[i];
           its += ni;
         }
-        const double totmass = block_sum(dm, shd);
-        const unsigned long long totits = block_sum(its, shu);
+        const unsigned long long totits = block_sum(its, shu);  // (its barriers publish dm)
         if (tid == 0) {
+          const double totmass = seq_sum(n, [&](uint32_t k) { return dm[k]; });
           if (p.do_alter_thermo) {  // state_change: condensation.cpp:126-138
             const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
             const double totrho = totmass / c.volume[g] * R0cubed_VOL0;
@@ -929,7 +956,8 @@ __global__ void k_condsolve(DevCtx c, uint32_t n, const double* __restrict__ rad
                             double* __restrict__ out, uint32_t* __restrict__ niters_out) {
   const NewtonCfg cfg{c.p.maxniters, c.p.rtol, c.p.atol};
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const Where w{c.err, OOB, i};
+    uint32_t failed = 0;
+    const Where w{c.err, OOB, i, &failed};
     const double T = temp[i];
     const double psat = saturation_pressure(T, w);
     const double ffactor = diffusion_factor(press[i], T, psat);
@@ -940,7 +968,7 @@ __global__ void k_condsolve(DevCtx c, uint32_t n, const double* __restrict__ rad
                                            bkoh, ffactor, radius[i], seeds ? seeds[i] : 0.0, ni,
                                            w);
     out[i] = max_dryradius(newr, msol[i]);
-    if (niters_out) niters_out[i] = ni;
+    if (niters_out) niters_out[i] = ni | (failed ? CLEO_NITERS_FAILED : 0u);
   }
 }
 
@@ -1036,7 +1064,8 @@ k_cs_a(DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __
     bool defer = false;
     uint32_t key = 0;
     if (i < n) {
-      const Where w{c.err, OOB, i};
+      uint32_t failed = 0;
+      const Where w{c.err, OOB, i, &failed};
       const double T = temp[i], r = radius[i], dt = delt[i];
       const double psat = saturation_pressure(T, w);
       const double ffactor = diffusion_factor(press[i], T, psat);
@@ -1072,7 +1101,7 @@ k_cs_a(DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __
         }
         if (conv) {
           out[i] = max_dryradius(sqrt(e.z), msol[i]);
-          if (niters_out) niters_out[i] = ni;
+          if (niters_out) niters_out[i] = ni | (failed ? CLEO_NITERS_FAILED : 0u);
         } else {
           defer = true;  // restart until converged (impliciteuler.cpp:136-140), key 0
           // where pass B's restart continues; NaN after an abandoned seed (a full solve)
@@ -1082,7 +1111,7 @@ k_cs_a(DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __
         defer = true;
         key = deferred_key(dt, fmax(crit, c.p.cond_minsubdelt), true);
       }
-      if (defer && niters_out) niters_out[i] = carried;
+      if (defer && niters_out) niters_out[i] = carried | (failed ? CLEO_NITERS_FAILED : 0u);
     }
     const uint32_t pos = cs_warp_append(ctr, defer);
     if (defer) {
@@ -1105,7 +1134,8 @@ k_cs_b(DevCtx c, const double* __restrict__ radius, const double* __restrict__ m
        jr += gridDim.x * blockDim.x) {
     const uint32_t j = nl - 1 - jr;  // most expensive solves first (the list is sorted by cost)
     const uint32_t i = lvals[j];
-    const Where w{c.err, OOB, i};
+    uint32_t failed = 0;
+    const Where w{c.err, OOB, i, &failed};
     const double T = temp[i], r = radius[i], dt = delt[i];
     const double psat = saturation_pressure(T, w);
     const double ffactor = diffusion_factor(press[i], T, psat);
@@ -1129,7 +1159,7 @@ k_cs_b(DevCtx c, const double* __restrict__ radius, const double* __restrict__ m
                                 seed, ni, w);
     }
     out[i] = max_dryradius(newr, msol[i]);
-    if (niters_out) niters_out[i] += ni;
+    if (niters_out) niters_out[i] = (niters_out[i] + ni) | (failed ? CLEO_NITERS_FAILED : 0u);
   }
 }
 
@@ -1304,14 +1334,8 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
   cudaStream_t s = x->stream;
   StageMark m(x, 2);
   const int gg = grid_for(d.ngbxs, 256);
-  if (did_motion) {
-    // gridboxes per warp: up to 32, as many as leave 64 warps per SM busy
-    const size_t full = (size_t)148 * 64;
-    size_t batch = ((size_t)d.ngbxs + full - 1) / full;
-    batch = batch < 1 ? 1 : (batch > 32 ? 32 : batch);
-    const size_t batches = ((size_t)d.ngbxs + batch - 1) / batch;
-    const size_t warps = batches < 1 ? 1 : (batches < full ? batches : full);
-    k_b_qcond<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, s>>>(d, (uint32_t)batch);
+  if (did_motion) {  // qcond from the moved superdroplets, a thread per gridbox
+    k_b_qcond<<<gg, 256, 0, s>>>(d);
     x->launches += 1;
   }
   k_b_reset<<<gg, 256, 0, s>>>(d, b, 1);
@@ -1352,28 +1376,28 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
         k_cond_b<4><<<x->grid_condb[1], 256, 0, s>>>(d, b);
       else
         k_cond_b<3><<<x->grid_condb[0], 256, 0, s>>>(d, b);
-      x->launches += 1;
+      // every gridbox's condensed mass summed in order, its state updated
+      k_b_commit<<<gg, 256, 0, s>>>(d, b);
+      x->launches += 2;
     }
-    if (cond || coll) {
+    if (coll) {
       StageMark mk(x, 4);
       k_b_reset<<<1, 32, 0, s>>>(d, b, 0);
       k_b_classify<<<gg, 256, 0, s>>>(d, b);
       // the warp kernel's 64-slot variant takes gridboxes up to 64 superdroplets, its 128-slot
       // variant those of 65 .. small_max (when small_max > 64)
       const int wide = x->cfg.small_max > SMALL_MAX ? 1 : 0, m3 = x->cfg.small_minb == 3 ? 1 : 0;
-      const int ci = cond ? 1 : 0, li = coll ? 1 : 0;
       constexpr uint32_t SW = SmallLayout<WARP_MAX>::BYTES, SS = SmallLayout<SMALL_MAX>::BYTES;
       if (m3)
-        k_b_small<3, SMALL_MAX><<<x->grid_small[1], B_THREADS, SS, s>>>(d, b, ci, li, 0);
+        k_b_small<3, SMALL_MAX><<<x->grid_small[1], B_THREADS, SS, s>>>(d, b, 0);
       else
-        k_b_small<2, SMALL_MAX><<<x->grid_small[0], B_THREADS, SS, s>>>(d, b, ci, li, 0);
+        k_b_small<2, SMALL_MAX><<<x->grid_small[0], B_THREADS, SS, s>>>(d, b, 0);
       // the 128-slot variant at 2 CTAs per SM whatever the 64-slot one's budget: at 3 it spills
       // (measured: collisions 3.87 ms with both at 2, 3.67 ms with the 64-slot one at 3)
-      if (wide) k_b_small<2, WARP_MAX><<<x->grid_wide, B_THREADS, SW, s>>>(d, b, ci, li, 1);
+      if (wide) k_b_small<2, WARP_MAX><<<x->grid_wide, B_THREADS, SW, s>>>(d, b, 1);
       x->launches += wide;
-      k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_SMEM, s>>>(d, b, cond ? 1 : 0,
-                                                                           coll ? 1 : 0);
-      k_b_cta<true><<<x->grid_large, B_THREADS, 0, s>>>(d, b, cond ? 1 : 0, coll ? 1 : 0);
+      k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_SMEM, s>>>(d, b);
+      k_b_cta<true><<<x->grid_large, B_THREADS, 0, s>>>(d, b);
       x->launches += 5;
     }
     subt = min(next_step(d.p.condstep, subt), next_step(d.p.collstep, subt));
@@ -1405,6 +1429,15 @@ int run_sdm_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
       k_motion<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, x->keys[0], x->vals[0], inc ? 1 : 0);
       k_mv_report<<<1, 1, 0, s>>>(d, x->d_motion);
       x->launches += 2;
+      {  // inside a captured step the record becomes an external event node of the graph
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CUDA_TRY(cudaStreamIsCapturing(s, &cs));
+        if (cs == cudaStreamCaptureStatusActive)
+          CUDA_TRY(cudaEventRecordWithFlags(x->ev_report, s, cudaEventRecordExternal));
+        else
+          CUDA_TRY(cudaEventRecord(x->ev_report, s));
+      }
+      x->report_recorded = true;
       if (d.p.monitors & CLEO_MONITOR_PRECIPITATION) {  // before the sort moves the droplets
         k_mon_precip<<<gg, 256, 0, s>>>(d);
         x->launches += 1;
@@ -1651,7 +1684,8 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &d.mv_shift, ng);
   rc |= dalloc(x, &d.mv_total, 1);
   if (cudaHostAlloc(&x->h_motion, 2 * sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess ||
-      cudaHostGetDevicePointer(&x->d_motion, x->h_motion, 0) != cudaSuccess)
+      cudaHostGetDevicePointer(&x->d_motion, x->h_motion, 0) != cudaSuccess ||
+      cudaEventCreateWithFlags(&x->ev_report, cudaEventDisableTiming) != cudaSuccess)
     rc |= CLEO_ERR_CUDA;
   else
     x->h_motion[0] = x->h_motion[1] = 0;
@@ -1788,7 +1822,7 @@ void cleo_b200_destroy(cleo_b200_ctx* x) {
     cudaStreamSynchronize(cs);
     cudaStreamDestroy(cs);
   }
-  for (cudaEvent_t e : {x->ev_uploaded, x->ev_consumed, x->ev_snap, x->ev_snap_free})
+  for (cudaEvent_t e : {x->ev_uploaded, x->ev_consumed, x->ev_snap, x->ev_snap_free, x->ev_report})
     if (e) cudaEventDestroy(e);
   for (void* p : x->allocs) cudaFree(p);
   if (x->h_motion) cudaFreeHost(x->h_motion);
@@ -1966,7 +2000,10 @@ int cleo_b200_step(cleo_b200_ctx* x, uint32_t t_mdl, uint32_t t_next) {
   while (t_sdm < t_next) {
     const uint32_t next_move = next_step(x->d.p.motionstep, t_sdm);
     const uint32_t t_sdm_next = t_next < next_move ? t_next : next_move;
-    {  // full re-sort when more than a fifth of the superdroplets changed gridbox last time
+    {  // full re-sort when more than a fifth of the superdroplets changed gridbox in the
+       // previous motion step (whose report the event marks; it completes early in that step,
+       // while the rest of the step is still queued, so the device does not idle)
+      if (x->report_recorded) CUDA_TRY(cudaEventSynchronize(x->ev_report));
       const volatile uint32_t* hm = x->h_motion;
       const uint32_t movers = hm[0], nsd = hm[1];
       x->sort_full = (uint64_t)movers * 5 > (uint64_t)nsd;
@@ -2057,6 +2094,14 @@ int cleo_b200_status(cleo_b200_ctx* x, cleo_b200_error* err) {
     err->index = e.index;
   }
   return e.code;
+}
+
+int cleo_b200_clear_status(cleo_b200_ctx* x) {
+  if (!x) return CLEO_ERR_ARGUMENT;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  CUDA_TRY(cudaMemsetAsync(x->d.err, 0, sizeof(DevError), x->stream));
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  return CLEO_OK;
 }
 
 int cleo_b200_domain_nsupers(cleo_b200_ctx* x, size_t* n) {

@@ -7,7 +7,10 @@
 // that sorts with scratch memory held in a file-scope device array instead of allocating it.
 //
 // The scratch array is SCRATCH_BYTES (about 16.3 MiB) and lives in every GPU that loads the
-// library until the process exits. It bounds one call to SORT_STATIC_MAX superdroplets.
+// library until the process exits. It bounds one call to SORT_STATIC_MAX superdroplets. Under
+// CUDA's lazy module loading the driver allocates it when this file's code first reaches a
+// device, which is the first call's cudaGetSymbolAddress; hence the set-up call with n = 0 that
+// callers make at start-up, before they reserve device memory or enter their time loop.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -105,7 +108,8 @@ int scratch_for_current_device(uint32_t** out) {
 extern "C" int cleo_b200_sort_by_gridbox_static(const uint32_t* d_sdgbxindex, uint32_t n,
                                                 uint32_t ngbxs, uint32_t* d_order,
                                                 uint32_t* d_gstart, void* stream) {
-  if (!d_sdgbxindex || !d_order) return CLEO_ERR_ARGUMENT;
+  // n = 0: the set-up call a caller makes at start-up (the pointers may be NULL)
+  if (n > 0 && (!d_sdgbxindex || !d_order)) return CLEO_ERR_ARGUMENT;
   if (n > SORT_STATIC_MAX) {
     fprintf(stderr,
             "cleo_b200_sort_by_gridbox_static: %u superdroplets exceed the static scratch limit "

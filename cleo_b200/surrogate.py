@@ -151,28 +151,44 @@ def to_device(inputs: dict) -> dict:
             for k in INPUTS}
 
 
-def train_surrogate(solver_sdm, n_train: int = 1 << 24, steps: int = 20000, batch: int = 8192,
-                    lr: float = 2e-3, seed: int = 101, model_seed: int = 7, lib=None):
-    """Train a surrogate on n_train pairs that ``solver_sdm``'s condensation solver generates.
+def train_surrogate(solver_sdm, n_pairs: int = 1 << 24, steps: int = 20000, batch: int = 8192,
+                    lr: float = 2e-3, seed: int = 101, model_seed: int = 7, lib=None,
+                    chunk: int = 1 << 24):
+    """Train a surrogate on n_pairs pairs that ``solver_sdm``'s condensation solver generates.
 
-    The inputs follow the independent-droplet population of ``workloads.condsolve``; only the
-    droplets whose solve takes the direct branch (the branch a seed applies to) are kept.
+    The inputs follow the independent-droplet population of ``workloads.condsolve``, drawn in
+    chunks (seeds seed, seed + 1, ...) until n_pairs droplets whose solve takes the direct branch
+    (the branch a seed applies to) and converges have been collected; exactly n_pairs are kept.
     Returns (surrogate, info dict with the loss history and the training-set size).
     """
     import torch
     from . import workloads as W
-    inputs = to_device(W.condsolve(n_train, seed=seed))
-    # a rare droplet whose Newton iteration cannot meet a tight tolerance keeps its last iterate
-    r_new, _ = condensation_solve(solver_sdm, inputs, allow=("CLEO_ERR_NR_NOCONVERGE",))
     sur = Surrogate(seed=model_seed, lib=lib)
-    feats, tgt, direct = sur.features(inputs, radius_new=r_new)
-    keep = direct.bool()
-    feats, tgt = feats[keep].contiguous(), tgt[keep].contiguous()
-    del inputs, r_new
+    fs, ts = [], []
+    have, drawn, k = 0, 0, 0
+    while have < n_pairs:
+        inputs = to_device(W.condsolve(chunk, seed=seed + k))
+        # a rare droplet whose Newton iteration cannot meet the tolerance (the reference would
+        # abort on it) is marked in the iteration counts and left out
+        r_new, nit = condensation_solve(solver_sdm, inputs, allow=("CLEO_ERR_NR_NOCONVERGE",))
+        feats, tgt, direct = sur.features(inputs, radius_new=r_new)
+        ok = (nit.view(torch.int32) >= 0)  # the failure bit is the sign bit
+        keep = direct.bool() & ok
+        fs.append(feats[keep])
+        ts.append(tgt[keep])
+        have += int(keep.sum())
+        drawn += chunk
+        k += 1
+        del inputs, r_new, nit, feats, tgt, direct
+    feats = torch.cat(fs)[:n_pairs].contiguous()
+    tgt = torch.cat(ts)[:n_pairs].contiguous()
+    del fs, ts
+    if solver_sdm.status().code != 0:  # the droplets left out above recorded their failure
+        solver_sdm.lib.cleo_b200_clear_status(solver_sdm.ctx)
     sur.fit_normalisation(feats, tgt)
     hist = sur.train(feats, tgt, steps=steps, batch=batch, lr=lr, seed=seed)
     torch.cuda.synchronize()
-    return sur, {"n_pairs": int(tgt.numel()), "n_drawn": n_train,
+    return sur, {"n_pairs": int(tgt.numel()), "n_drawn": drawn,
                  "loss": hist.cpu().numpy(), "feats": feats, "target": tgt}
 
 

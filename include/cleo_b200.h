@@ -230,6 +230,11 @@ int cleo_b200_step(cleo_b200_ctx* ctx, uint32_t t_mdl, uint32_t t_next);
 /* Synchronise the context's stream and return the first recorded failure (CLEO_OK if none). */
 int cleo_b200_status(cleo_b200_ctx* ctx, cleo_b200_error* err);
 
+/* Forget the recorded failure (after a host that handled it, e.g. by leaving out the droplets a
+ * batch solve marked with CLEO_NITERS_FAILED, carries on; the reference would have aborted).
+ * No reference counterpart. Synchronises the context's stream. */
+int cleo_b200_clear_status(cleo_b200_ctx* ctx);
+
 /* Number of superdroplets inside the domain (SupersInDomain::domain_nsupers). Synchronises. */
 int cleo_b200_domain_nsupers(cleo_b200_ctx* ctx, size_t* n);
 
@@ -257,8 +262,11 @@ int cleo_b200_download_budgets(cleo_b200_ctx* ctx, double* cond_mass, uint64_t* 
  * thermodynamic_equations.cpp:93-114). Inputs are device pointers of length n: radius, msol,
  * temp, press, s_ratio and delt (dimensionless). Writes the new radius (after change_radius, i.e.
  * not below the dry radius) to radius_out and, if niters_out is non-NULL, the Newton iterations
- * spent per droplet. Uses the context's maxniters/rtol/atol/minsubdelt and nr_seed.
+ * spent per droplet, with CLEO_NITERS_FAILED or-ed in for each droplet whose solve hit one of the
+ * reference's aborts (no convergence within maxniters, impliciteuler.cpp:213-217; the status
+ * reports the first such droplet). Uses the context's maxniters/rtol/atol/minsubdelt and nr_seed.
  */
+#define CLEO_NITERS_FAILED 0x80000000u
 int cleo_b200_condensation_solve(cleo_b200_ctx* ctx, size_t n, const double* d_radius,
                                  const double* d_msol, const double* d_temp, const double* d_press,
                                  const double* d_s_ratio, const double* d_delt,
@@ -296,10 +304,14 @@ int cleo_b200_stage_times(cleo_b200_ctx* ctx, double ms[5], uint64_t count[5]);
  *                 (entry ngbxs = number of in-domain superdroplets, entry ngbxs + 1 = n)
  *   stream        cudaStream_t to enqueue on (as void*; NULL = default stream)
  * n must not exceed 1,048,576 (else CLEO_ERR_CAPACITY). The first call on a device looks up the
- * scratch array's device address (cudaGetSymbolAddress) with that device current; make that first
- * call before any stream capture. All calls share the one scratch array, so calls whose work
- * overlaps on the GPU (e.g. on two streams at once) race; each call writes every scratch word it
- * reads, so nothing needs clearing between calls. Asynchronous on `stream`.
+ * scratch array's device address (cudaGetSymbolAddress) with that device current. With CUDA's
+ * lazy module loading (the default) that lookup is what loads this code onto the device, so the
+ * ~16.3 MiB array is allocated by the driver then, and the device may synchronise. Make that
+ * first call once per device at start-up, before reserving the rest of device memory, entering
+ * the time loop or capturing a stream: a call with n = 0 (pointers may then be NULL) does only
+ * the set-up. All calls share the one scratch array, so calls whose work overlaps on the GPU
+ * (e.g. on two streams at once) race; each call writes every scratch word it reads, so nothing
+ * needs clearing between calls. Asynchronous on `stream`.
  */
 int cleo_b200_sort_by_gridbox_static(const uint32_t* d_sdgbxindex, uint32_t n, uint32_t ngbxs,
                                      uint32_t* d_order, uint32_t* d_gstart, void* stream);

@@ -7,6 +7,17 @@
  * reference's association and use the same libm calls (pow, exp, sqrt, floor, round, fmin, fmax),
  * so results differ from the reference only where libm does. Compile without FMA contraction.
  * Aborts of the reference become error codes (the first one is kept).
+ *
+ * Two builds (oracle/Makefile):
+ *   liboracle.so     pow and exp from the host libm, as the reference calls them: this build is
+ *                    pinned bit for bit to CLEO's own sources compiled here;
+ *   liboracle_cr.so  the same code with pow and exp correctly rounded (ORACLE_CR_LIBM, see
+ *                    oracle/crlibm.cpp), the arithmetic the CUDA path documents: there the CUDA
+ *                    path must agree bit for bit, and the two builds differ only where the host
+ *                    libm misrounds.
+ * The loops over gridboxes of one SDM step can run on OpenMP threads (oc_set_num_threads); every
+ * gridbox's work is independent of the others' within a loop, so results are the same doubles
+ * for any number of threads.
  */
 #include "cleo_oracle.h"
 
@@ -14,6 +25,14 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+
+#ifdef ORACLE_CR_LIBM
+/* correctly rounded pow and exp (oracle/crlibm.cpp) in place of the host libm's */
+double oc_cr_pow(double x, double y);
+double oc_cr_exp(double x);
+#define pow(x, y) oc_cr_pow((x), (y))
+#define exp(x) oc_cr_exp((x))
+#endif
 
 #include "../include/cleo_b200_rng.h"
 
@@ -105,10 +124,17 @@ struct oc_ctx {
   cleo_b200_error err;
 };
 
-static cleo_b200_error* g_err; /* error slot of the context being stepped */
-static uint64_t* g_iters;      /* Newton iteration counter of the current solve */
+/* per thread: the error slot of the context being stepped (or of this thread's share of a
+ * parallel loop) and the Newton iteration counter of the current solve */
+static _Thread_local cleo_b200_error* g_err;
+static _Thread_local uint64_t* g_iters;
+static int g_nthreads = 1; /* threads of the gridbox loops (oc_set_num_threads) */
+
+/* set by every abort of the current thread's work, cleared by the batch solves per droplet */
+static _Thread_local int g_failed;
 
 static void set_error(int code, uint32_t gbx, uint64_t index) {
+  g_failed = 1;
   if (g_err && g_err->code == CLEO_OK) {
     g_err->code = code;
     g_err->gbxindex = gbx;
@@ -117,8 +143,18 @@ static void set_error(int code, uint32_t gbx, uint64_t index) {
 }
 
 /* the superdroplet being processed (for error attribution) */
-static uint32_t g_cur_gbx = OOB;
-static uint64_t g_cur_sd = 0;
+static _Thread_local uint32_t g_cur_gbx = OOB;
+static _Thread_local uint64_t g_cur_sd = 0;
+
+/* A loop over gridboxes on several threads: each thread records its first error, that is the one
+ * of the lowest gridbox it visits (OpenMP hands a thread its iterations in increasing order), and
+ * the error of the lowest gridbox over all threads is the one the sequential loop meets first. */
+static void merge_error(cleo_b200_error* into, const cleo_b200_error* e) {
+  if (e->code == CLEO_OK) return;
+  if (into->code == CLEO_OK || e->gbxindex < into->gbxindex ||
+      (e->gbxindex == into->gbxindex && e->index < into->index))
+    *into = *e;
+}
 
 /* ------------------------------------------------------------------------------------------ */
 /* SuperdropAttrs: superdrop_attrs.hpp:61-259, superdrop_attrs.cpp:34-62                      */
@@ -1040,19 +1076,19 @@ static void sort_and_set_refs(oc_ctx* c) {
 }
 
 /* effect_on_hydrometeor_states: movesupersindomain.hpp:95-136, 259-267 */
-static void effect_on_qcond(oc_ctx* c) {
-  for (uint32_t g = 0; g < c->ngbxs; ++g) {
-    double totmass_cond = 0.0;
-    for (size_t k = c->refs0[g]; k < c->refs1[g]; ++k) {
-      g_cur_gbx = g;
-      g_cur_sd = k;
-      totmass_cond += condensate_mass(c->sd[k].r, c->sd[k].msol) * (double)c->sd[k].xi;
-    }
-    const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
-    const double rho_cond = totmass_cond / c->volume[g] * R0cubed_VOL0;
-    const double rho_dry = dry_air_density(c->press[g], c->temp[g], c->qvap[g]);
-    c->qcond[g] = rho_cond / rho_dry;
+static int effect_on_qcond(oc_ctx* c, uint32_t g, const void* arg) {
+  (void)arg;
+  double totmass_cond = 0.0;
+  for (size_t k = c->refs0[g]; k < c->refs1[g]; ++k) {
+    g_cur_gbx = g;
+    g_cur_sd = k;
+    totmass_cond += condensate_mass(c->sd[k].r, c->sd[k].msol) * (double)c->sd[k].xi;
   }
+  const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
+  const double rho_cond = totmass_cond / c->volume[g] * R0cubed_VOL0;
+  const double rho_dry = dry_air_density(c->press[g], c->temp[g], c->qvap[g]);
+  c->qcond[g] = rho_cond / rho_dry;
+  return 0;
 }
 
 /* ------------------------------------------------------------------------------------------ */
@@ -1109,9 +1145,11 @@ static void monitor_massmoments(oc_ctx* c, uint32_t g, const sd_t* supers, size_
     c->prev2[rain][g] = m2;
   }
 }
-static void monitor_motion(oc_ctx* c) { /* MonitorMassMomentsChange::monitor_motion :295-305 */
-  for (uint32_t g = 0; g < c->ngbxs; ++g)
-    monitor_massmoments(c, g, &c->sd[c->refs0[g]], c->refs1[g] - c->refs0[g], 1);
+/* MonitorMassMomentsChange::monitor_motion :295-305, for gridbox g */
+static int monitor_motion(oc_ctx* c, uint32_t g, const void* arg) {
+  (void)arg;
+  monitor_massmoments(c, g, &c->sd[c->refs0[g]], c->refs1[g] - c->refs0[g], 1);
+  return 0;
 }
 
 int oc_monitors_begin(oc_ctx* c) { /* before_timestepping: :75-82, reset_monitor */
@@ -1151,6 +1189,72 @@ int oc_download_monitors(oc_ctx* c, cleo_b200_monitors* o, int reset) {
   return CLEO_OK;
 }
 
+/* One step of a loop over all gridboxes (the reference's league of gridbox teams), on
+ * g_nthreads threads; returns the OR of f's results. Errors keep the sequential loop's order
+ * (merge_error) and never replace one the context already holds. */
+typedef int (*gbx_fn)(oc_ctx* c, uint32_t g, const void* arg);
+int oc_set_num_threads(int n) {
+  g_nthreads = n < 1 ? 1 : n;
+  return g_nthreads;
+}
+static int for_each_gridbox(oc_ctx* c, gbx_fn f, const void* arg) {
+  cleo_b200_error first = {CLEO_OK, OOB, 0};
+  int any = 0;
+  const long ng = (long)c->ngbxs;
+#pragma omp parallel num_threads(g_nthreads) if (g_nthreads > 1) reduction(| : any)
+  {
+    cleo_b200_error mine = {CLEO_OK, OOB, 0};
+    g_err = &mine;
+#pragma omp for schedule(dynamic, 64)
+    for (long g = 0; g < ng; ++g) any |= f(c, (uint32_t)g, arg);
+#pragma omp critical(oc_first_error)
+    merge_error(&first, &mine);
+    g_err = NULL;
+  }
+  g_err = &c->err;
+  if (c->err.code == CLEO_OK && first.code != CLEO_OK) c->err = first;
+  return any;
+}
+
+/* movesupersindomain.hpp:47-93: every superdroplet of gridbox g moved */
+static int move_gridbox(oc_ctx* c, uint32_t g, const void* arg) {
+  (void)arg;
+  for (size_t k = c->refs0[g]; k < c->refs1[g]; ++k) {
+    g_cur_gbx = g;
+    g_cur_sd = k;
+    move_superdrop(c, g, &c->sd[k]);
+  }
+  return 0;
+}
+
+/* the SDM microphysics of gridbox g between t_sdm and t_sdm_next: run_subtimestepping
+ * (sdmmethods.hpp:70-84) with Condensation >> Collisions, then monitor_microphysics
+ * (sdmmethods.hpp:76); returns 1 if collisions left null superdroplets */
+typedef struct {
+  uint32_t t_sdm, t_sdm_next;
+} micro_span;
+static int micro_gridbox(oc_ctx* c, uint32_t g, const void* arg) {
+  const micro_span* sp = (const micro_span*)arg;
+  const cleo_b200_params* p = &c->p;
+  sd_t* supers = &c->sd[c->refs0[g]];
+  size_t n = c->refs1[g] - c->refs0[g];
+  const size_t nbefore = n;
+  const uint64_t key = cleo_rng_key(p->seed, sp->t_sdm, g);
+  uint64_t slot = 0;
+  uint32_t subt = sp->t_sdm;
+  while (subt < sp->t_sdm_next) {
+    if (on_step(p->condstep, subt)) do_condensation(c, g, supers, n, c->refs0[g]);
+    if (on_step(p->collstep, subt)) {
+      n = do_collisions(p, supers, n, c->volume[g], key, &slot, g, c->refs0[g]);
+    }
+    const uint32_t a = next_step(p->condstep, subt);
+    const uint32_t b = next_step(p->collstep, subt);
+    subt = (a < b) ? a : b;
+  }
+  monitor_massmoments(c, g, supers, n, 0);
+  return n != nbefore;
+}
+
 int oc_step(oc_ctx* c, uint32_t t_mdl, uint32_t t_next) {
   const cleo_b200_params* p = &c->p;
   g_err = &c->err;
@@ -1162,41 +1266,15 @@ int oc_step(oc_ctx* c, uint32_t t_mdl, uint32_t t_next) {
 
     /* superdrops_movement -> MoveSupersInDomain::run_step (movesupersindomain.hpp:292-301) */
     if (on_step(p->motionstep, t_sdm)) {
-      for (uint32_t g = 0; g < c->ngbxs; ++g) {
-        for (size_t k = c->refs0[g]; k < c->refs1[g]; ++k) {
-          g_cur_gbx = g;
-          g_cur_sd = k;
-          move_superdrop(c, g, &c->sd[k]);
-        }
-      }
+      for_each_gridbox(c, move_gridbox, NULL);
       sort_and_set_refs(c); /* CartesianTransportAcrossDomain on 1 process: sort_totsupers */
-      effect_on_qcond(c);
-      monitor_motion(c); /* movesupersindomain.hpp:297 */
+      for_each_gridbox(c, effect_on_qcond, NULL);
+      for_each_gridbox(c, monitor_motion, NULL); /* movesupersindomain.hpp:297 */
     }
 
     /* sdm_microphysics: sdmmethods.hpp:184-230 */
-    int any_change = 0;
-    for (uint32_t g = 0; g < c->ngbxs; ++g) {
-      sd_t* supers = &c->sd[c->refs0[g]];
-      size_t n = c->refs1[g] - c->refs0[g];
-      const size_t nbefore = n;
-      const uint64_t key = cleo_rng_key(p->seed, t_sdm, g);
-      uint64_t slot = 0;
-      /* run_subtimestepping: sdmmethods.hpp:70-84 with Condensation >> Collisions */
-      uint32_t subt = t_sdm;
-      while (subt < t_sdm_next) {
-        if (on_step(p->condstep, subt)) do_condensation(c, g, supers, n, c->refs0[g]);
-        if (on_step(p->collstep, subt)) {
-          n = do_collisions(p, supers, n, c->volume[g], key, &slot, g, c->refs0[g]);
-        }
-        const uint32_t a = next_step(p->condstep, subt);
-        const uint32_t b = next_step(p->collstep, subt);
-        subt = (a < b) ? a : b;
-      }
-      monitor_massmoments(c, g, supers, n, 0); /* monitor_microphysics, sdmmethods.hpp:76 */
-      if (n != nbefore) any_change = 1;
-    }
-    if (any_change) sort_and_set_refs(c);
+    const micro_span sp = {t_sdm, t_sdm_next};
+    if (for_each_gridbox(c, micro_gridbox, &sp)) sort_and_set_refs(c);
 
     t_sdm = t_sdm_next;
   }
@@ -1352,28 +1430,40 @@ static int solve_batch(const cleo_b200_params* p, size_t n, const double* radius
                        const double* msol, const double* temp, const double* press,
                        const double* s_ratio, const double* delt, const double* seed,
                        double* radius_out, uint32_t* niters_out) {
-  cleo_b200_error e = {CLEO_OK, OOB, 0};
-  g_err = &e;
   const implit_t it = {p->maxniters, p->rtol, p->atol};
-  for (size_t i = 0; i < n; ++i) {
-    uint64_t iters = 0;
-    g_iters = &iters;
-    g_cur_gbx = OOB;
-    g_cur_sd = i;
-    const double psat = saturation_pressure(temp[i]);
-    const double ffactor = diffusion_factor(press[i], temp[i], psat);
-    double akoh, bkoh;
-    kohler_factors(msol[i], temp[i], &akoh, &bkoh);
-    sd_t d = {0, 0, 0, 0, 1, radius[i], msol[i], 0};
-    const double newr = solve_condensation(&it, delt[i], p->cond_minsubdelt, s_ratio[i], akoh,
-                                           bkoh, ffactor, radius[i], seed ? seed[i] : 0.0);
-    change_radius(&d, newr);
-    radius_out[i] = d.r;
-    if (niters_out) niters_out[i] = (uint32_t)iters;
+  cleo_b200_error first = {CLEO_OK, OOB, 0};
+  const long nn = (long)n;
+  /* droplets are independent: any number of threads, the first error by droplet index */
+#pragma omp parallel num_threads(g_nthreads) if (g_nthreads > 1)
+  {
+    cleo_b200_error mine = {CLEO_OK, OOB, 0};
+    g_err = &mine;
+#pragma omp for schedule(dynamic, 256)
+    for (long ii = 0; ii < nn; ++ii) {
+      const size_t i = (size_t)ii;
+      uint64_t iters = 0;
+      g_iters = &iters;
+      g_failed = 0;
+      g_cur_gbx = OOB;
+      g_cur_sd = i;
+      const double psat = saturation_pressure(temp[i]);
+      const double ffactor = diffusion_factor(press[i], temp[i], psat);
+      double akoh, bkoh;
+      kohler_factors(msol[i], temp[i], &akoh, &bkoh);
+      sd_t d = {0, 0, 0, 0, 1, radius[i], msol[i], 0};
+      const double newr = solve_condensation(&it, delt[i], p->cond_minsubdelt, s_ratio[i], akoh,
+                                             bkoh, ffactor, radius[i], seed ? seed[i] : 0.0);
+      change_radius(&d, newr);
+      radius_out[i] = d.r;
+      /* the droplets the reference would abort on are marked (CLEO_NITERS_FAILED) */
+      if (niters_out) niters_out[i] = (uint32_t)iters | (g_failed ? CLEO_NITERS_FAILED : 0u);
+    }
+    g_iters = NULL;
+#pragma omp critical(oc_first_error)
+    merge_error(&first, &mine);
+    g_err = NULL;
   }
-  g_iters = NULL;
-  g_err = NULL;
-  return e.code;
+  return first.code;
 }
 
 int oc_condensation_solve(const cleo_b200_params* p, size_t n, const double* radius,

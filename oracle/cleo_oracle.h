@@ -33,6 +33,10 @@ int oc_download_budgets(oc_ctx* c, double* cond_mass, uint64_t* nr_iters);
 int oc_monitors_begin(oc_ctx* c);
 int oc_download_monitors(oc_ctx* c, cleo_b200_monitors* out, int reset);
 
+/* Threads of the loops over gridboxes inside oc_step (OpenMP; 1 = sequential, the default).
+ * Results do not depend on it. Returns the number set. */
+int oc_set_num_threads(int n);
+
 /* Batch of independent implicit-Euler condensation solves (host arrays). */
 int oc_condensation_solve(const cleo_b200_params* p, size_t n, const double* radius,
                           const double* msol, const double* temp, const double* press,

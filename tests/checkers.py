@@ -1,6 +1,9 @@
 """Loading the CPU checkers and comparing domain states (test infrastructure).
 
-* the oracle: oracle/liboracle.so, the C restatement of the hot path (built by oracle/Makefile);
+* the oracle: oracle/liboracle.so, the C restatement of the hot path with the host libm, pinned
+  bit for bit to CLEO's own sources (built by oracle/Makefile);
+* the correctly rounded oracle: oracle/liboracle_cr.so, the same restatement with correctly
+  rounded pow and exp, which the CUDA path must match bit for bit;
 * the reference build: oracle/_ref/libcleo_ref.so, CLEO's own sources compiled against the
   Kokkos-API shim (present only where CLEO's sources were available to build it).
 """
@@ -14,20 +17,24 @@ from cleo_b200 import abi
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+ORACLE_CR_SO = os.path.join(ROOT, "oracle", "liboracle_cr.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libcleo_ref.so")
 
-_oracle = None
+_oracle = {}
 _ref = None
 
 
-def oracle_lib():
-    global _oracle
-    if _oracle is None:
-        if not os.path.exists(ORACLE_SO):
+def oracle_lib(cr=False):
+    """The oracle (host libm), or with cr=True its correctly rounded build."""
+    if cr not in _oracle:
+        path = ORACLE_CR_SO if cr else ORACLE_SO
+        if not os.path.exists(path):
             subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True,
                            capture_output=True)
-        lib = C.CDLL(ORACLE_SO)
+        lib = C.CDLL(path)
         abi.declare_api(lib, "oc")
+        lib.oc_set_num_threads.argtypes = [C.c_int]
+        lib.oc_set_num_threads.restype = C.c_int
         P = C.POINTER(abi.Params)
         d = C.POINTER(C.c_double)
         lib.oc_condensation_solve.argtypes = [P, C.c_size_t] + [d] * 6 + [d, C.POINTER(C.c_uint32)]
@@ -47,8 +54,14 @@ def oracle_lib():
         lib.oc_pair_probability.argtypes = [P, C.c_double, C.c_uint64, C.c_double, C.c_double,
                                             C.c_uint64, C.c_double, C.c_double]
         lib.oc_pair_probability.restype = C.c_double
-        _oracle = lib
-    return _oracle
+        _oracle[cr] = lib
+    return _oracle[cr]
+
+
+def oracle_threads(lib, n=None):
+    """Run the oracle's gridbox loops on n threads (default: every host core); results do not
+    depend on the count."""
+    return lib.oc_set_num_threads(int(n if n is not None else (os.cpu_count() or 1)))
 
 
 def ref_available():
@@ -125,6 +138,39 @@ def assert_same_domain(a: dict, b: dict, rtol=1e-12, what=""):
     ia = np.sort(a["sdid"][nd:])
     ib = np.sort(b["sdid"][nd:])
     assert np.array_equal(ia, ib), (what, "oob ids differ")
+
+
+def assert_identical_domain(a: dict, b: dict, what=""):
+    """Every field of every in-domain superdroplet bit for bit (order included); the same set of
+    out-of-domain ids."""
+    assert a["n_domain"] == b["n_domain"], (what, a["n_domain"], b["n_domain"])
+    assert a["n_total"] == b["n_total"], (what, a["n_total"], b["n_total"])
+    nd = a["n_domain"]
+    for k in ("sdid", "sdgbxindex", "xi", "radius", "msol", "coord3", "coord1", "coord2"):
+        x, y = a[k][:nd], b[k][:nd]
+        same = (x.view(np.uint64) == y.view(np.uint64)) if x.dtype == np.float64 else (x == y)
+        bad = np.nonzero(~same)[0]
+        rel = (float(np.max(np.abs(x[bad] - y[bad]) / np.maximum(np.abs(y[bad]), 1e-300)))
+               if bad.size and x.dtype == np.float64 else None)
+        assert bad.size == 0, (what, k, f"{bad.size} of {nd} differ (max rel {rel})", bad[:10],
+                               x[bad[:5]], y[bad[:5]])
+    assert np.array_equal(np.sort(a["sdid"][nd:]), np.sort(b["sdid"][nd:])), (what, "oob ids")
+
+
+def assert_identical_run(g, o, what=""):
+    """Two SDM contexts after the same steps: superdroplets, gridbox states and budgets (condensed
+    mass and Newton iterations) bit for bit."""
+    assert_identical_domain(g.download_supers(), o.download_supers(), what)
+    sg, so = g.download_state(), o.download_state()
+    for f in abi.STATE_FIELDS:
+        bad = np.nonzero(sg[f].view(np.uint64) != so[f].view(np.uint64))[0]
+        assert bad.size == 0, (what, f, f"{bad.size} gridboxes differ",
+                               max_rel(sg[f][bad], so[f][bad]))
+    cg, ig = g.download_budgets()
+    co, io = o.download_budgets()
+    assert np.array_equal(cg.view(np.uint64), co.view(np.uint64)), (what, "condensed mass",
+                                                                    max_rel(cg, co))
+    assert np.array_equal(ig, io), (what, "newton iterations")
 
 
 def max_rel(x, y):

@@ -39,15 +39,11 @@ def test_graphs_match_eager_and_oracle(lib, pattern):
             s.run_step(k * ts, (k + 1) * ts)
         s.check()
         runs[name] = s
-    o = make_sdm(w, lib=K.oracle_lib(), prefix="oc")
+    o = make_sdm(w, lib=K.oracle_lib(cr=True), prefix="oc")
     for k in range(6):
         o.run_step(k * w["tstep"], (k + 1) * w["tstep"])
-    a, b = runs["graph"].download_supers(), runs["eager"].download_supers()
-    K.assert_same_domain(a, b, rtol=0.0, what="graph vs eager")
-    K.assert_same_domain(a, o.download_supers(), rtol=1e-12, what="graph vs oracle")
-    ca, ia = runs["graph"].download_budgets()
-    cb, ib = runs["eager"].download_budgets()
-    assert np.array_equal(ia, ib) and np.array_equal(ca, cb)
+    K.assert_identical_run(runs["graph"], runs["eager"], "graph vs eager")
+    K.assert_identical_run(runs["graph"], o, "graph vs oracle")
 
 
 def test_graph_step_after_irregular_call(lib):
@@ -105,12 +101,12 @@ def test_launch_configs_match_oracle(lib, cfg):
     assert lib.cleo_b200_set_launch_config(g.ctx, arr) == 0
     got = (C.c_int32 * 4)()
     assert lib.cleo_b200_tuned_config(g.ctx, got) == 0 and tuple(got) == cfg
-    o = make_sdm(w, lib=K.oracle_lib(), prefix="oc")
+    o = make_sdm(w, lib=K.oracle_lib(cr=True), prefix="oc")
     for k in range(4):
         g.run_step(k * w["tstep"], (k + 1) * w["tstep"])
         o.run_step(k * w["tstep"], (k + 1) * w["tstep"])
     g.check()
-    K.assert_same_domain(g.download_supers(), o.download_supers(), rtol=1e-12, what=str(cfg))
+    K.assert_identical_run(g, o, str(cfg))
     for bad_cfg in ((256, 3, 129, 2), (256, 3, 64, 4)):
         bad = (C.c_int32 * 4)(*bad_cfg)
         assert lib.cleo_b200_set_launch_config(g.ctx, bad) == abi.CODE["CLEO_ERR_ARGUMENT"]

@@ -1,10 +1,12 @@
 """The allocation-free gridbox sort (cleo_b200_sort_by_gridbox_static) against the context's sort.
 
 For callers that cannot allocate device memory while they run, the library offers one sort whose
-scratch lives in a static device array. These checks call it through the C ABI twice in a row, on
-two different populations, and compare each result bit for bit with the order that the context's
-own sort (cleo_b200_upload_supers) produces for the same superdroplets; then they check that sizes
-beyond the array's limit are refused. Kept in a file of its own that pytest collects last.
+scratch lives in a static device array. As such a caller would, the checks first make the set-up
+call (n = 0) that loads the array onto the device at start-up; then they call the sort through the
+C ABI twice in a row, on two different populations, and compare each result bit for bit with the
+order that the context's own sort (cleo_b200_upload_supers) produces for the same superdroplets;
+then they check that sizes beyond the array's limit are refused. Kept in a file of its own that
+pytest collects last.
 """
 import ctypes as C
 
@@ -35,6 +37,8 @@ def test_static_sort_matches_context_sort_twice():
     assert torch.cuda.is_available()
     lib = abi.load_library()
     stream = torch.cuda.current_stream()
+    # start-up: the set-up call, before any other device memory of this test is taken
+    assert lib.cleo_b200_sort_by_gridbox_static(None, 0, 0, None, None, None) == 0
     for call, (seed, ndims) in enumerate(((41, (8, 16, 16)), (42, (12, 20, 10)))):
         w = shuffled_population(seed, ndims)
         sd = w["supers"]
