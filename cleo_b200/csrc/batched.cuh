@@ -1,8 +1,8 @@
 // batched.cuh — the batched microphysics of one SDM step (exec_mode CLEO_EXEC_BATCHED).
 //
 // Same results as k_micro (one CTA per gridbox), scheduled for B200 occupancy:
-//   k_b_qcond      thread per gridbox: qcond from the moved superdroplets (after the sort), their
-//                  condensate masses added in order
+//   k_b_qcond      warp per 32 gridboxes: qcond from the moved superdroplets (after the sort),
+//                  their condensate masses added in order (warp_batch_sums)
 //   k_b_thermo     thread per gridbox: psat, supersaturation, diffusion factor, the droplets'
 //                  Kohler factors that depend on temperature alone
 //   k_cond_a       thread per superdroplet: the mandatory two Newton iterations of every
@@ -13,8 +13,8 @@
 //                  listed solves (the ones the reference guess did not settle in two iterations)
 //   k_cond_b       thread per listed solve, neighbouring lanes of similar cost, from the seed
 //                  where its residual beats the reference guess's
-//   k_b_commit     thread per gridbox: the condensed mass of its superdroplets added in their
-//                  order, their Newton iterations, and the state update
+//   k_b_commit     warp per 32 gridboxes: the condensed mass of each one's superdroplets added
+//                  in their order, their Newton iterations, and the state update
 //   k_b_classify   gridboxes into size buckets (warp-aggregated atomics)
 //   k_b_small      persistent, warp per gridbox (n <= small_max <= 128; 64- and 128-slot
 //                  variants): collisions in registers + per-warp shared memory
@@ -24,7 +24,7 @@
 // small_max, the pass-A block size, the resident-CTA targets (register budgets) of pass A and of
 // the warp kernel's 64-slot variant are chosen by the autotuner (results do not depend on them).
 // Every per-gridbox sum of doubles adds its terms in the superdroplets' order, as the reference's
-// sequential loop does (seq_sum): condensed mass per droplet goes through a scratch array and is
+// sequential loop does (warp_batch_sums): condensed mass per droplet goes through a scratch array and is
 // summed per gridbox after the solves, so budgets and states are the sequential loop's doubles
 // whatever the schedule.
 #pragma once
@@ -50,27 +50,79 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
   return base + __popc(m & ((1u << lane) - 1u));
 }
 
+// ---- sums over gridboxes in the superdroplets' order, a warp per 32 consecutive gridboxes ----
+// Consecutive gridboxes' ranges follow each other, so a batch of up to 32 gridboxes is one
+// contiguous range [gstart[g0], gstart[g0 + nb]). The warp reads it coalesced, SEQ_WIN elements
+// at a time, into its shared buffers (term(k) -> dbuf, iters(k) -> ubuf), and lane j adds the
+// terms of gridbox g0 + j's valid superdroplets [gstart, gstart + gcount) one after another: the
+// reference's sequential loop (seq_sum's order), with every element of the range loaded once.
+constexpr uint32_t SEQ_WIN = 256;
+constexpr int SEQ_THREADS = 256;
+template <class Term, class Iters>
+__device__ __forceinline__ void warp_batch_sums(const DevCtx& c, uint32_t g0, uint32_t nb,
+                                                double* dbuf, uint32_t* ubuf, Term term,
+                                                Iters iters, double& sum,
+                                                unsigned long long& its) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t lo = c.gstart[g0], hi = c.gstart[g0 + nb];
+  const bool own = (uint32_t)lane < nb;
+  const uint32_t s = own ? c.gstart[g0 + lane] : hi;
+  const uint32_t e = own ? s + c.gcount[g0 + lane] : hi;
+  double acc = 0.0;
+  unsigned long long it = 0;
+  for (uint32_t w0 = lo; w0 < hi; w0 += SEQ_WIN) {
+    const uint32_t w1 = hi - w0 < SEQ_WIN ? hi : w0 + SEQ_WIN;
+    for (uint32_t k = w0 + lane; k < w1; k += 32) {
+      dbuf[k - w0] = term(k);
+      ubuf[k - w0] = iters(k);
+    }
+    __syncwarp();
+    const uint32_t a = s > w0 ? s : w0, b = e < w1 ? e : w1;
+    for (uint32_t k = a; k < b; ++k) {
+      acc += dbuf[k - w0];
+      it += ubuf[k - w0];
+    }
+    __syncwarp();
+  }
+  sum = acc;
+  its = it;
+}
+
 // ---- effect_on_hydrometeor_states (movesupersindomain.hpp:95-136) ----
-// A thread per gridbox adds its superdroplets' condensate masses in their order (seq_sum), the
-// reference's sequential loop, so qcond is the same double.
-__global__ void k_b_qcond(DevCtx c) {
-  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs;
-       g += gridDim.x * blockDim.x) {
-    const uint32_t base = c.gstart[g], n = c.gcount[g];
-    const double m = seq_sum(n, [&](uint32_t k) {
-      const uint32_t i = base + k;
-      return condensate_mass(c.sd.r[i], c.sd.msol[i], Where{c.err, g, i}) * (double)c.sd.xi[i];
-    });
-    const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
-    const double rho_cond = m / c.volume[g] * R0cubed_VOL0;
-    c.qcond[g] = rho_cond / dry_air_density(c.press[g], c.temp[g], c.qvap[g]);
+// qcond of every gridbox from its (moved and sorted) superdroplets' condensate masses, added in
+// their order (warp_batch_sums)
+__global__ void __launch_bounds__(SEQ_THREADS) k_b_qcond(const __grid_constant__ DevCtx c) {
+  __shared__ double dbuf[SEQ_THREADS / 32][SEQ_WIN];
+  __shared__ uint32_t ubuf[SEQ_THREADS / 32][SEQ_WIN];
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t g0 = warp * 32; g0 < c.ngbxs; g0 += nwarps * 32) {
+    const uint32_t nb = c.ngbxs - g0 < 32 ? c.ngbxs - g0 : 32;
+    double m;
+    unsigned long long unused;
+    warp_batch_sums(
+        c, g0, nb, dbuf[wib], ubuf[wib],
+        [&](uint32_t i) {
+          const uint32_t g = c.sd.gbx[i];
+          return g < c.ngbxs ? condensate_mass(c.sd.r[i], c.sd.msol[i], Where{c.err, g, i}) *
+                                   (double)c.sd.xi[i]
+                             : 0.0;
+        },
+        [](uint32_t) { return 0u; }, m, unused);
+    if ((uint32_t)lane < nb) {
+      const uint32_t g = g0 + lane;
+      const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
+      const double rho_cond = m / c.volume[g] * R0cubed_VOL0;
+      c.qcond[g] = rho_cond / dry_air_density(c.press[g], c.temp[g], c.qvap[g]);
+    }
   }
 }
 
 // ---- per-gridbox thermodynamics of superdroplets_change (condensation.cpp:43-59) ----
 // (every gridbox, empty ones too: the reference evaluates psat for each, and its check of the
 // temperature with it)
-__global__ void k_b_thermo(DevCtx c, BatchScratch b) {
+__global__ void k_b_thermo(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b) {
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x) {
     if (g == 0) b.ctr[0] = b.ctr[9] = 0;  // deferred solves, of which restarts
     const Where w{c.err, g, c.gstart[g]};
@@ -122,7 +174,7 @@ __device__ __forceinline__ uint32_t deferred_key(double delt, double mindelt, bo
 // ---- pass A: superdrop_mass_change (condensation.cpp:98-112) up to two Newton iterations ----
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB)
-k_cond_a(DevCtx c, BatchScratch b) {
+k_cond_a(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b) {
   const cleo_b200_params& p = c.p;
   const uint32_t n = c.counters[0];
   const NewtonCfg cfg{p.maxniters, p.rtol, p.atol};
@@ -185,7 +237,7 @@ k_cond_a(DevCtx c, BatchScratch b) {
 // ---- pass B: the deferred solves, in order of cost ----
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB)
-k_cond_b(DevCtx c, BatchScratch b) {
+k_cond_b(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b) {
   const cleo_b200_params& p = c.p;
   const uint32_t nl = b.ctr[0];
   const NewtonCfg cfg{p.maxniters, p.rtol, p.atol};
@@ -235,7 +287,7 @@ k_cond_b(DevCtx c, BatchScratch b) {
 }
 
 // ---- size buckets of the gridboxes that hold superdroplets ----
-__global__ void k_b_classify(DevCtx c, BatchScratch b) {
+__global__ void k_b_classify(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b) {
   const uint32_t ng = c.ngbxs;
   for (uint32_t g0 = blockIdx.x * blockDim.x; g0 < ng; g0 += gridDim.x * blockDim.x) {
     const uint32_t g = g0 + threadIdx.x;
@@ -255,7 +307,7 @@ __global__ void k_b_classify(DevCtx c, BatchScratch b) {
 
 // reduction of the condensed mass and iterations of one gridbox + state update and budgets
 // (effect_on_thermodynamic_state, condensation.cpp:72-80 and :126-138; monitor, condensation.hpp:149)
-__device__ __forceinline__ void cond_commit(DevCtx& c, uint32_t g, double totmass,
+__device__ __forceinline__ void cond_commit(const DevCtx& c, uint32_t g, double totmass,
                                             unsigned long long totits) {
   if (c.p.do_alter_thermo) {
     const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
@@ -271,17 +323,24 @@ __device__ __forceinline__ void cond_commit(DevCtx& c, uint32_t g, double totmas
 }
 
 // ---- the gridboxes' share of a condensation sub-step after its solves ----
-// A thread per gridbox: the condensed mass of its superdroplets added in their order (seq_sum,
-// the reference's sequential reduction, condensation.cpp:29-35), their Newton iterations, then
-// the state update (cond_commit). Empty gridboxes commit a zero change, as the reference's do.
-__global__ void k_b_commit(DevCtx c, BatchScratch b) {
-  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs;
-       g += gridDim.x * blockDim.x) {
-    const uint32_t base = c.gstart[g], n = c.gcount[g];
-    const double m = seq_sum(n, [&](uint32_t k) { return b.dm[base + k]; });
-    unsigned long long it = 0;
-    for (uint32_t k = 0; k < n; ++k) it += b.its[base + k];
-    cond_commit(c, g, m, it);
+// The condensed mass of each gridbox's superdroplets added in their order (warp_batch_sums, the
+// reference's sequential reduction, condensation.cpp:29-35), their Newton iterations, then the
+// state update (cond_commit). Empty gridboxes commit a zero change, as the reference's do.
+__global__ void __launch_bounds__(SEQ_THREADS) k_b_commit(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b) {
+  __shared__ double dbuf[SEQ_THREADS / 32][SEQ_WIN];
+  __shared__ uint32_t ubuf[SEQ_THREADS / 32][SEQ_WIN];
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t g0 = warp * 32; g0 < c.ngbxs; g0 += nwarps * 32) {
+    const uint32_t nb = c.ngbxs - g0 < 32 ? c.ngbxs - g0 : 32;
+    double m;
+    unsigned long long it;
+    // (positions past a gridbox's valid superdroplets are loaded but not added)
+    warp_batch_sums(
+        c, g0, nb, dbuf[wib], ubuf[wib], [&](uint32_t i) { return b.dm[i]; },
+        [&](uint32_t i) { return b.its[i]; }, m, it);
+    if ((uint32_t)lane < nb) cond_commit(c, g0 + lane, m, it);
   }
 }
 
@@ -368,7 +427,7 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 
 template <int MINB, int CAP>
 __global__ void __launch_bounds__(B_THREADS, MINB)
-k_b_small(DevCtx c, BatchScratch b, int q) {
+k_b_small(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b, int q) {
   using L = SmallLayout<CAP>;
   constexpr int H = CAP / 32;
   static_assert(CAP % 32 == 0 && CAP <= 255, "slot indices are stored as bytes");
@@ -564,12 +623,65 @@ k_b_small(DevCtx c, BatchScratch b, int q) {
   }
 }
 
+// Origins of the shuffled positions of a gridbox of n (2 .. CHAIN_MAX) superdroplets for a whole
+// CTA, by the chains the warp kernel follows (see k_b_small): FIRST[v] = the first swap index s
+// with J[s] = v, NEXT[s] = the next swap index after s with the same J value. The pairs
+// (J[s], s), s = 1 .. n-1, are ordered by a bitonic sort of the 32-bit keys J[s] << 16 | s in
+// shared memory (`keys`, a power of two >= n - 1 entries), so that equal values lie together in
+// increasing s; FIRST and NEXT (n entries each, any memory) are read off the sorted keys, and
+// each thread then walks the chains of its positions (about ln n lookups each). P receives the
+// origins, as fy_origin computes them. Ends with a barrier.
+constexpr uint32_t CHAIN_MAX = 16384;  // keys of up to 16384 swaps: 64 KB of shared memory
+constexpr uint32_t LARGE_SMEM = CHAIN_MAX * 4;
+__device__ void cta_fy_origins(const uint32_t* J, uint32_t n, uint32_t* keys, uint32_t* FIRST,
+                               uint32_t* NEXT, uint32_t* P) {
+  constexpr uint32_t NONE = 0xFFFFFFFFu;
+  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  const uint32_t m = n - 1;  // swaps s = 1 .. n-1
+  uint32_t mp = 1;
+  while (mp < m) mp <<= 1;
+  for (uint32_t i = tid; i < mp; i += nt) keys[i] = i < m ? (J[i + 1] << 16) | (i + 1) : NONE;
+  for (uint32_t v = tid; v < n; v += nt) FIRST[v] = NEXT[v] = NONE;
+  __syncthreads();
+  for (uint32_t k = 2; k <= mp; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = tid; i < mp; i += nt) {
+        const uint32_t l = i ^ j;
+        if (l > i) {
+          const uint32_t a = keys[i], bk = keys[l];
+          if ((a > bk) == ((i & k) == 0)) {
+            keys[i] = bk;
+            keys[l] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (uint32_t i = tid; i < m; i += nt) {
+    const uint32_t v = keys[i] >> 16, sidx = keys[i] & 0xFFFFu;
+    if (i == 0 || (keys[i - 1] >> 16) != v) FIRST[v] = sidx;
+    if (i + 1 < m && (keys[i + 1] >> 16) == v) NEXT[sidx] = keys[i + 1] & 0xFFFFu;
+  }
+  __syncthreads();
+  for (uint32_t k = tid; k < n; k += nt) {
+    uint32_t cur = k == 0 ? 0u : J[k];
+    uint32_t nx = k == 0 ? FIRST[0] : NEXT[k];
+    while (nx != NONE) {  // strictly increasing, so at most n hops
+      cur = nx;
+      nx = FIRST[cur];
+    }
+    P[k] = cur;
+  }
+  __syncthreads();
+}
+
 // ---- medium and large gridboxes: one CTA per gridbox ----
 // medium: staged in shared memory with the non-staged fields permuted through registers;
-// large: staged in global scratch arrays.
+// large: staged in global scratch arrays, the shuffle's chain keys in LARGE_SMEM of shared memory.
 template <bool LARGE>
 __global__ void __launch_bounds__(B_THREADS)
-k_b_cta(DevCtx c, BatchScratch b) {
+k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b) {
   const uint32_t t_sdm = *b.tsdm;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint32_t shw[40];
@@ -644,6 +756,10 @@ k_b_cta(DevCtx c, BatchScratch b) {
     __syncthreads();
     if (n <= FY_PARALLEL_MAX) {  // every thread traces its own positions
       for (uint32_t k = tid; k < n; k += B_THREADS) P[k] = fy_origin(J, n, k);
+    } else if (LARGE && n <= CHAIN_MAX) {  // chains, as in the warp kernel (keys in smem)
+      cta_fy_origins(J, n, reinterpret_cast<uint32_t*>(smem),
+                     reinterpret_cast<uint32_t*>(c.scr_c3 + base),
+                     reinterpret_cast<uint32_t*>(c.scr_c1 + base), P);
     } else {
       for (uint32_t k = tid; k < n; k += B_THREADS) P[k] = k;
       __syncthreads();
@@ -757,7 +873,7 @@ k_b_cta(DevCtx c, BatchScratch b) {
 __global__ void k_b_set_t(BatchScratch b, uint32_t t) { *b.tsdm = t; }
 __global__ void k_b_advance_t(BatchScratch b, uint32_t dt) { *b.tsdm += dt; }
 
-__global__ void k_b_reset(DevCtx c, BatchScratch b, int slots) {
+__global__ void k_b_reset(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b, int slots) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (slots)
     for (uint32_t g = i; g < c.ngbxs; g += gridDim.x * blockDim.x) b.slot[g] = 0;

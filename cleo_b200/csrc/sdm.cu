@@ -304,7 +304,7 @@ __device__ __forceinline__ bool beyond_domainboundary(uint32_t gbxindex, uint32_
 // (predcorrmotion.hpp:85-106) with get_no_decomposition_bounding_gridbox (cartesianmaps.cpp:278)
 // and CartesianCheckBounds. Writes the sort key min(gbx, ngbxs) and the position.
 __global__ void __launch_bounds__(256, 4)  // 64 registers: measured 15% faster than 80
-k_motion(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, int incremental) {
+k_motion(const __grid_constant__ DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, int incremental) {
   const uint32_t n = c.counters[0];
   const uint32_t ng = c.ngbxs;
   const double delt = c.p.motion_delt;
@@ -448,7 +448,7 @@ k_motion(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, int
     }
   }
 }
-__global__ void k_mv_report(DevCtx c, uint32_t* __restrict__ out) {  // mapped host memory
+__global__ void k_mv_report(const __grid_constant__ DevCtx c, uint32_t* __restrict__ out) {  // mapped host memory
   out[0] = *c.mv_total;
   out[1] = c.counters[0];
 }
@@ -466,7 +466,7 @@ __device__ __forceinline__ uint32_t mv_before(const DevCtx& c, uint32_t i) {
   return c.mv_scan[i] + c.mv_tsums[i / SCAN_TILE];
 }
 // the movers' keys: min(gbx, ngbxs) of the gridbox indices k_motion wrote
-__global__ void k_mv_list(DevCtx c, uint32_t* __restrict__ mk, uint32_t* __restrict__ mvp) {
+__global__ void k_mv_list(const __grid_constant__ DevCtx c, uint32_t* __restrict__ mk, uint32_t* __restrict__ mvp) {
   const uint32_t n = c.counters[0];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t p = mv_before(c, i);
@@ -477,20 +477,20 @@ __global__ void k_mv_list(DevCtx c, uint32_t* __restrict__ mk, uint32_t* __restr
     }
   }
 }
-__global__ void k_mv_counts(DevCtx c) {
+__global__ void k_mv_counts(const __grid_constant__ DevCtx c) {
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x) {
     const uint32_t stay = c.gcount[g] - c.mv_leave[g];
     c.mv_stay[g] = stay;
     c.gstart_new[g] = stay + c.mv_arrive[g];  // scanned in place to the new starts
   }
 }
-__global__ void k_mv_ends(DevCtx c) {  // after the scan: gstart_new[ngbxs] = in-domain count
+__global__ void k_mv_ends(const __grid_constant__ DevCtx c) {  // after the scan: gstart_new[ngbxs] = in-domain count
   c.gstart_new[c.ngbxs + 1] = c.counters[0];
 }
-__global__ void k_mv_count(DevCtx c, uint32_t* __restrict__ count) {  // number of movers
+__global__ void k_mv_count(const __grid_constant__ DevCtx c, uint32_t* __restrict__ count) {  // number of movers
   *count = mv_before(c, c.counters[0]);
 }
-__global__ void k_mv_arrivals(DevCtx c) {  // to be scanned: first sorted mover of each key
+__global__ void k_mv_arrivals(const __grid_constant__ DevCtx c) {  // to be scanned: first sorted mover of each key
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x)
     c.mv_mstart[g] = c.mv_arrive[g];
 }
@@ -508,7 +508,7 @@ __device__ __forceinline__ void mv_copy(const Fields& s, const Fields& d, uint32
 // shift[g] = gstart_new[g] + mv_below[g] - gstart[g] + (movers before gstart[g]); computed per
 // gridbox together with the commit of the new gridbox starts (which nothing after this reads
 // in their old form)
-__global__ void k_mv_shift_commit(DevCtx c) {
+__global__ void k_mv_shift_commit(const __grid_constant__ DevCtx c) {
   const uint32_t ng = c.ngbxs;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ng + 2; k += gridDim.x * blockDim.x) {
     if (k < ng) {
@@ -519,7 +519,7 @@ __global__ void k_mv_shift_commit(DevCtx c) {
   }
 }
 __global__ void __launch_bounds__(256)
-k_mv_stayers(DevCtx c, Fields src, Fields dst) {
+k_mv_stayers(const __grid_constant__ DevCtx c, Fields src, Fields dst) {
   constexpr int U = 2;  // superdroplets per thread and iteration, all loads issued first
   const uint32_t n = c.counters[0];
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -560,7 +560,7 @@ k_mv_stayers(DevCtx c, Fields src, Fields dst) {
     }
   }
 }
-__global__ void k_mv_movers(DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ mk,
+__global__ void k_mv_movers(const __grid_constant__ DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ mk,
                             const uint32_t* __restrict__ mvp) {
   const uint32_t n = c.counters[0];
   const uint32_t nm = mv_before(c, n);
@@ -582,12 +582,12 @@ struct ObsOut {
   uint64_t* xi;
   float *r, *msol, *c3, *c1, *c2;
 };
-__global__ void k_obs_counts(DevCtx c, uint32_t* __restrict__ start) {  // scanned to out offsets
+__global__ void k_obs_counts(const __grid_constant__ DevCtx c, uint32_t* __restrict__ start) {  // scanned to out offsets
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x)
     start[g] = c.gcount[g];
 }
 __global__ void __launch_bounds__(256)
-k_obs_gather(DevCtx c, ObsOut o, const uint32_t* __restrict__ start) {
+k_obs_gather(const __grid_constant__ DevCtx c, ObsOut o, const uint32_t* __restrict__ start) {
   const uint32_t n = c.counters[0];
   const uint32_t ng = c.ngbxs;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -622,7 +622,7 @@ __global__ void k_wait_check(uint32_t max_tries, int* __restrict__ out) {
 }
 
 // sort keys of freshly uploaded droplets
-__global__ void k_keys_from_gbx(DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+__global__ void k_keys_from_gbx(const __grid_constant__ DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
   const uint32_t n = c.counters[0];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t g = c.sd.gbx[i];
@@ -650,7 +650,7 @@ __global__ void k_gather(Fields src, Fields dst, const uint32_t* __restrict__ pe
 
 // gridbox refs from the sorted keys: gstart[k] = lower_bound(keys, k) for k in [0, ngbxs + 1]
 // (find_refs by partition point, findrefs.hpp:54-126)
-__global__ void k_refs(DevCtx c, const uint32_t* __restrict__ keys) {
+__global__ void k_refs(const __grid_constant__ DevCtx c, const uint32_t* __restrict__ keys) {
   const uint32_t n = c.counters[0];
   const uint32_t nk = c.ngbxs + 2;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += gridDim.x * blockDim.x) {
@@ -671,14 +671,14 @@ __global__ void k_refs(DevCtx c, const uint32_t* __restrict__ keys) {
   }
 }
 
-__global__ void k_counts(DevCtx c) {
+__global__ void k_counts(const __grid_constant__ DevCtx c) {
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x)
     c.gcount[g] = c.gstart[g + 1] - c.gstart[g];
   if (blockIdx.x == 0 && threadIdx.x == 0) c.counters[1] = c.gstart[c.ngbxs];
 }
 
 // append [ndomain, nrange) to the out-of-domain store, then nrange = ndomain
-__global__ void k_to_grave(DevCtx c) {
+__global__ void k_to_grave(const __grid_constant__ DevCtx c) {
   const uint32_t nd = c.gstart[c.ngbxs];
   const uint32_t n = c.counters[0];
   const uint32_t ng0 = c.counters[2];
@@ -694,7 +694,7 @@ __global__ void k_to_grave(DevCtx c) {
     c.grave.id[o] = c.sd.id[j];
   }
 }
-__global__ void k_grave_commit(DevCtx c) {
+__global__ void k_grave_commit(const __grid_constant__ DevCtx c) {
   const uint32_t nd = c.gstart[c.ngbxs];
   c.counters[2] += c.counters[0] - nd;
   c.counters[0] = nd;
@@ -773,7 +773,7 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* wsum, 
 // k_micro: SDMMicrophysicsFunctor (sdmmethods.hpp:54-93) for one gridbox per CTA
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(MICRO_THREADS)
-k_micro(DevCtx c, uint32_t t_sdm, uint32_t t_sdm_next, int did_motion) {
+k_micro(const __grid_constant__ DevCtx c, uint32_t t_sdm, uint32_t t_sdm_next, int did_motion) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned long long shu[32];
   __shared__ uint32_t shw[40];
@@ -949,7 +949,7 @@ k_micro(DevCtx c, uint32_t t_sdm, uint32_t t_sdm_next, int did_motion) {
 }
 
 // batched implicit-Euler solves of independent droplets
-__global__ void k_condsolve(DevCtx c, uint32_t n, const double* __restrict__ radius,
+__global__ void k_condsolve(const __grid_constant__ DevCtx c, uint32_t n, const double* __restrict__ radius,
                             const double* __restrict__ msol, const double* __restrict__ temp,
                             const double* __restrict__ press, const double* __restrict__ s_ratio,
                             const double* __restrict__ delt, const double* __restrict__ seeds,
@@ -996,7 +996,7 @@ __device__ __forceinline__ void mon_moments(const DevCtx& c, uint32_t g, int rai
 }
 // fetch_delta_massmoments (monitor_massmoments_change.hpp:99-121); which = 0 after
 // microphysics, 1 after motion; begin != 0: before_timestepping (moments become the baseline)
-__global__ void k_mon_mm(DevCtx c, int which, int begin) {
+__global__ void k_mon_mm(const __grid_constant__ DevCtx c, int which, int begin) {
   const int mask = c.p.monitors;
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs;
        g += gridDim.x * blockDim.x) {
@@ -1019,7 +1019,7 @@ __global__ void k_mon_mm(DevCtx c, int which, int begin) {
 }
 // the precipitation contributions of each gridbox's superdroplets, in their order (the
 // reference adds them one by one as it moves the gridbox's superdroplets)
-__global__ void k_mon_precip(DevCtx c) {
+__global__ void k_mon_precip(const __grid_constant__ DevCtx c) {
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs;
        g += gridDim.x * blockDim.x) {
     const uint32_t base = c.gstart[g], n = c.gcount[g];
@@ -1052,7 +1052,7 @@ __device__ __forceinline__ uint32_t cs_warp_append(uint32_t* ctr, bool flag) {
   return base + __popc(m & ((1u << lane) - 1u));
 }
 __global__ void __launch_bounds__(256)
-k_cs_a(DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __restrict__ msol,
+k_cs_a(const __grid_constant__ DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __restrict__ msol,
        const double* __restrict__ temp, const double* __restrict__ press,
        const double* __restrict__ s_ratio, const double* __restrict__ delt,
        double* __restrict__ seeds, double* __restrict__ out, uint32_t* __restrict__ niters_out,
@@ -1121,7 +1121,7 @@ k_cs_a(DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __
   }
 }
 __global__ void __launch_bounds__(256)
-k_cs_b(DevCtx c, const double* __restrict__ radius, const double* __restrict__ msol,
+k_cs_b(const __grid_constant__ DevCtx c, const double* __restrict__ radius, const double* __restrict__ msol,
        const double* __restrict__ temp, const double* __restrict__ press,
        const double* __restrict__ s_ratio, const double* __restrict__ delt,
        const double* __restrict__ seeds, double* __restrict__ out,
@@ -1334,8 +1334,10 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
   cudaStream_t s = x->stream;
   StageMark m(x, 2);
   const int gg = grid_for(d.ngbxs, 256);
-  if (did_motion) {  // qcond from the moved superdroplets, a thread per gridbox
-    k_b_qcond<<<gg, 256, 0, s>>>(d);
+  // warps of 32 gridboxes each
+  const int gw = grid_for(((size_t)d.ngbxs + 31) / 32 * 32, SEQ_THREADS);
+  if (did_motion) {  // qcond from the moved superdroplets
+    k_b_qcond<<<gw, SEQ_THREADS, 0, s>>>(d);
     x->launches += 1;
   }
   k_b_reset<<<gg, 256, 0, s>>>(d, b, 1);
@@ -1377,7 +1379,7 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       else
         k_cond_b<3><<<x->grid_condb[0], 256, 0, s>>>(d, b);
       // every gridbox's condensed mass summed in order, its state updated
-      k_b_commit<<<gg, 256, 0, s>>>(d, b);
+      k_b_commit<<<gw, SEQ_THREADS, 0, s>>>(d, b);
       x->launches += 2;
     }
     if (coll) {
@@ -1397,7 +1399,7 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       if (wide) k_b_small<2, WARP_MAX><<<x->grid_wide, B_THREADS, SW, s>>>(d, b, 1);
       x->launches += wide;
       k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_SMEM, s>>>(d, b);
-      k_b_cta<true><<<x->grid_large, B_THREADS, 0, s>>>(d, b);
+      k_b_cta<true><<<x->grid_large, B_THREADS, LARGE_SMEM, s>>>(d, b);
       x->launches += 5;
     }
     subt = min(next_step(d.p.condstep, subt), next_step(d.p.collstep, subt));
@@ -1784,7 +1786,10 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<false>, B_THREADS,
                                                            (size_t)MEDIUM_SMEM));
     x->grid_medium = sms * (occ > 0 ? occ : 1);
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<true>, B_THREADS, 0));
+    CUDA_TRY(cudaFuncSetAttribute(k_b_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)LARGE_SMEM));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<true>, B_THREADS,
+                                                           LARGE_SMEM));
     x->grid_large = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cond_b<3>, 256, 0));
     x->grid_condb[0] = 2 * sms * (occ > 0 ? occ : 1);

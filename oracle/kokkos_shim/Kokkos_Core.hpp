@@ -163,11 +163,13 @@ struct ViewTraits;
 template <class T>
 struct ViewTraits<T*> {
   using value_type = T;
+  using non_const_data_type = std::remove_const_t<T>*;
   static constexpr size_t static_extent = 0;
 };
 template <class T, size_t N>
 struct ViewTraits<T[N]> {
   using value_type = T;
+  using non_const_data_type = std::remove_const_t<T>[N];
   static constexpr size_t static_extent = N;
 };
 
@@ -179,7 +181,8 @@ class View {
   using non_const_value_type = std::remove_const_t<value_type>;
   using pointer_type = value_type*;
   using reference_type = value_type&;
-  using HostMirror = View<DataType>;
+  /* as in Kokkos, a host mirror holds non-const data (here: the same memory) */
+  using HostMirror = View<typename traits::non_const_data_type>;
   using memory_space = HostSpace;
   using execution_space = Serial;
 
@@ -204,6 +207,13 @@ class View {
   const std::shared_ptr<void>& owner() const { return own_; }
   std::string label() const { return ""; }
   void reallocate(size_t n) { allocate(n); }  // contents not kept (Kokkos::realloc)
+  HostMirror mirror_alias() const {
+    HostMirror m;
+    m.own_ = own_;
+    m.ptr_ = const_cast<non_const_value_type*>(ptr_);
+    m.n_ = n_;
+    return m;
+  }
 
  private:
   void allocate(size_t n) {
@@ -239,17 +249,18 @@ View<D, P...> subview(const View<D, P...>& v, const std::pair<I, I>& r) {
   return subview(v, pair<I, I>(r.first, r.second));
 }
 
+/* host mirrors: host memory is the only memory, so a mirror aliases the view's data */
 template <class V>
-V create_mirror_view(const V& v) {
-  return v;
+typename V::HostMirror create_mirror_view(const V& v) {
+  return v.mirror_alias();
 }
 template <class S, class V>
-V create_mirror_view(const S&, const V& v) {
-  return v;
+typename V::HostMirror create_mirror_view(const S&, const V& v) {
+  return v.mirror_alias();
 }
 template <class S, class V>
-V create_mirror_view_and_copy(const S&, const V& v) {
-  return v;
+typename V::HostMirror create_mirror_view_and_copy(const S&, const V& v) {
+  return v.mirror_alias();
 }
 template <class D1, class... P1, class D2, class... P2>
 void deep_copy(const View<D1, P1...>& dst, const View<D2, P2...>& src) {

@@ -64,8 +64,76 @@ def oracle_threads(lib, n=None):
     return lib.oc_set_num_threads(int(n if n is not None else (os.cpu_count() or 1)))
 
 
+ADAPTER_SO = os.path.join(ROOT, "oracle", "_ref", "libcleo_adapter.so")
+_adapter = None
+
+
 def ref_available():
     return os.path.exists(REF_SO)
+
+
+def adapter_available():
+    return os.path.exists(ADAPTER_SO)
+
+
+def adapter_lib():
+    """CLEO's RunCLEO with the B200 SDMMethods or CLEO's own (oracle/adapter_harness.cpp)."""
+    global _adapter
+    if _adapter is None:
+        abi.load_library()  # the harness links libcleo_b200.so: load it from the package first
+        lib = C.CDLL(ADAPTER_SO)
+        vp = C.c_void_p
+        lib.adp_run_cleo.argtypes = [C.POINTER(abi.Params), C.POINTER(abi.Grid),
+                                     C.POINTER(abi.GbxState), C.POINTER(abi.Supers), C.c_size_t,
+                                     C.c_uint, C.c_uint32, C.c_uint32, C.c_double, C.c_int,
+                                     C.POINTER(vp)]
+        lib.adp_run_cleo.restype = C.c_int
+        lib.adp_error.argtypes = [vp]
+        lib.adp_error.restype = C.c_char_p
+        lib.adp_nobs.argtypes = [vp]
+        lib.adp_nobs.restype = C.c_size_t
+        lib.adp_obs.argtypes = [vp, C.c_size_t, C.POINTER(C.c_uint32), C.POINTER(C.c_size_t),
+                                C.POINTER(abi.Supers), C.c_size_t, C.POINTER(abi.GbxState)]
+        lib.adp_obs.restype = C.c_int
+        lib.adp_free.argtypes = [vp]
+        lib.adp_free.restype = None
+        _adapter = lib
+    return _adapter
+
+
+def run_cleo(w, t_end, obsstep, b200, amp=0.0, nspacedims=3):
+    """RunCLEO over the workload from t = 0 to t_end (model steps), coupling every motion step:
+    the list of observations (t, domain superdroplets dict, gridbox states dict), one every
+    obsstep."""
+    lib = adapter_lib()
+    g = abi.grid_struct(w["grid"])
+    st = abi.state_struct(w["state"])
+    sd = w["supers"]
+    n = len(sd["xi"])
+    arrs = {k: np.ascontiguousarray(v) for k, v in sd.items()}
+    sup = abi.supers_struct(arrs)
+    run = C.c_void_p()
+    rc = lib.adp_run_cleo(C.byref(w["params"]), C.byref(g), C.byref(st), C.byref(sup), n,
+                          int(nspacedims), int(t_end), int(obsstep),
+                          float(amp), int(b200), C.byref(run))
+    try:
+        if rc != 0:
+            raise RuntimeError(lib.adp_error(run).decode())
+        out = []
+        ng = int(w["grid"]["ngbxs"])
+        for i in range(lib.adp_nobs(run)):
+            o_sd = {k: np.zeros(n, dtype=v.dtype) for k, v in arrs.items()}
+            o_st = {f: np.zeros(ng) for f in abi.STATE_FIELDS}
+            t, nd = C.c_uint32(), C.c_size_t()
+            so, stt = abi.supers_struct(o_sd), abi.state_struct(o_st)
+            assert lib.adp_obs(run, i, C.byref(t), C.byref(nd), C.byref(so), n,
+                               C.byref(stt)) == 0
+            k = int(nd.value)
+            out.append((int(t.value), {kk: v[:k] for kk, v in o_sd.items()} | {"n_domain": k},
+                        o_st))
+        return out
+    finally:
+        lib.adp_free(run)
 
 
 def ref_lib():

@@ -14,7 +14,11 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CLEO = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+# CLEO's sources: the first argument, else $CLEO_SRC, else a checkout named "reference" beside
+# this repository
+CLEO = (sys.argv[1] if len(sys.argv) > 1 else
+        os.environ.get("CLEO_SRC", os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(
+            os.path.abspath(__file__)))), "..", "reference")))
 COORD0 = 1000.0
 R0 = 1e-6
 MASS0 = R0 ** 3 * (100000.0 / (1004.64 * 273.15))

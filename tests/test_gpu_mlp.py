@@ -41,7 +41,8 @@ def _solver(lib, nr_seed=abi.NRSEED_REFERENCE, **tol):
 @pytest.fixture(scope="module")
 def trained(lib):
     solver = _solver(lib)
-    sur, info = train_surrogate(solver, n_train=1 << 18, steps=3000, batch=8192, lr=2e-3,
+    sur, info = train_surrogate(solver, n_pairs=1 << 17, chunk=1 << 18, steps=3000, batch=8192,
+                                lr=2e-3,
                                 seed=11, lib=lib)
     yield sur, info
     sur.close()
@@ -111,7 +112,7 @@ def test_inference_paths_agree(lib, n):
 def test_training_lowers_loss(trained):
     sur, info = trained
     loss = info["loss"]
-    assert info["n_pairs"] > 0.2 * info["n_drawn"]
+    assert info["n_pairs"] == 1 << 17 and info["n_pairs"] > 0.2 * info["n_drawn"]
     assert np.all(np.isfinite(loss))
     assert loss[-100:].mean() < 0.05 * loss[:10].mean(), (loss[:10].mean(), loss[-100:].mean())
 
