@@ -159,8 +159,7 @@ struct SdmListSeedIO {
   }
   __device__ __forceinline__ void store(uint32_t j, float t) const {
     const uint32_t i = list[j];
-    const double ri = r[i];
-    seed[i] = ri * ri * exp((double)t);
+    seed[i] = mlp::seed_from(r[i], t);
   }
 };
 

@@ -87,19 +87,24 @@ __device__ __forceinline__ float bf16_round(float x) {
   return __bfloat162float(__float2bfloat16_rn(x));
 }
 
-// raw features of one droplet (Koehler factors as condensation.cpp:49-51)
+// raw features of one droplet (Koehler factors as condensation.cpp:49-51). The network is FP32
+// with BF16 weights, so the logarithms are taken in single precision: they shape a seed that the
+// FP64 Newton iteration then judges, and FP64 logarithms would cost as much as several Newton
+// iterations.
 __device__ __forceinline__ void raw_features(double r, double msol, double temp, double press,
                                              double s_ratio, double delt, float x[NIN]) {
   double akoh, bkoh;
   kohler_factors(msol, temp, akoh, bkoh);
-  x[0] = (float)log(r);
-  x[1] = (float)log(msol);
+  x[0] = logf((float)r);
+  x[1] = logf((float)msol);
   x[2] = (float)(s_ratio - 1.0);
   x[3] = (float)temp;
   x[4] = (float)press;
   x[5] = (float)delt;
-  x[6] = (float)log(3.0 * bkoh / akoh);
+  x[6] = logf((float)(3.0 * bkoh / akoh));
 }
+// the Newton seed r^2 exp(t) from the network's output t = log(z_new / r^2)
+__device__ __forceinline__ double seed_from(double r, float t) { return r * r * (double)expf(t); }
 
 // standardised features from raw ones
 __device__ __forceinline__ void normalise(const float* fw, float x[NIN]) {

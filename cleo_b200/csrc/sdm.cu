@@ -79,13 +79,17 @@ struct DevCtx {
   unsigned long long* prev0[2];
   float *prev1[2], *prev2[2];
   double *precip, *precip_c, *gbxarea;  // per gridbox, per superdroplet, per gridbox
-  // incremental re-sort after motion: mover flags then their exclusive scan (capacity + 1),
-  // per gridbox the valid superdroplets that leave, the arrivals and the arrivals from lower
-  // positions, the stayers, and the new gridbox starts (ngbxs + 2)
-  uint32_t *mv_scan, *mv_leave, *mv_arrive, *mv_below, *mv_stay, *gstart_new, *mv_mstart,
-      *mv_shift;
+  // re-sort after motion (pages.cuh): mover flags then their exclusive scan (slots + 1); a full
+  // sort's per-key first sorted positions (ngbxs + 2)
+  uint32_t *mv_scan, *gstart_new;
   uint32_t* mv_tsums;  // the flag scan's tile offsets (the scan's readers add them: mv_before)
   uint32_t* mv_total;  // valid superdroplets that changed gridbox in the last motion step
+  // paged layout (pages.cuh): pages of PAGE_GBXS gridboxes, their slot starts (npages + 1), the
+  // touched-page flags and list, the re-sort's counters, the movers' records; slots = the SoA
+  // buffers' length (capacity plus the pages' slack)
+  uint32_t npages, slots;
+  uint32_t *pstart, *pg_flag, *pg_list, *pg_ctr;
+  Fields mvrec;
   // scratch
   double *scr_r, *scr_m, *scr_c3, *scr_c1, *scr_c2;
   unsigned long long *scr_x, *scr_id;
@@ -101,10 +105,29 @@ struct CondSeedIO {
     mlp::raw_features(radius[i], msol[i], temp[i], press[i], s_ratio[i], delt[i], x);
   }
   __device__ __forceinline__ void store(uint32_t i, float t) const {
-    const double r = radius[i];
-    seed[i] = r * r * exp((double)t);
+    seed[i] = mlp::seed_from(radius[i], t);
   }
   __device__ __forceinline__ uint32_t rows(uint32_t n) const { return n; }
+};
+// the same for the batched form: row j is the j-th entry of pass A's sorted list, whose first
+// *count entries are the direct solves (key 0)
+struct CondListSeedIO {
+  const double *radius, *msol, *temp, *press, *s_ratio, *delt;
+  const uint32_t* list;
+  const uint32_t* count;
+  double* seed;
+  __device__ __forceinline__ void features(uint32_t j, float x[mlp::NIN]) const {
+    const uint32_t i = list[j];
+    mlp::raw_features(radius[i], msol[i], temp[i], press[i], s_ratio[i], delt[i], x);
+  }
+  __device__ __forceinline__ void store(uint32_t j, float t) const {
+    const uint32_t i = list[j];
+    seed[i] = mlp::seed_from(radius[i], t);
+  }
+  __device__ __forceinline__ uint32_t rows(uint32_t n) const {
+    const uint32_t c = *count;
+    return c < n ? c : n;
+  }
 };
 
 }  // namespace
@@ -120,7 +143,8 @@ struct cleo_b200_ctx {
   int device = 0;
   // sort scratch
   uint32_t *keys[2], *vals[2], *hist, *tile_sums;
-  uint32_t *gs_tsums = nullptr, *mv_count = nullptr;  // incremental re-sort scratch
+  uint32_t *gs_tsums = nullptr, *mv_count = nullptr;  // scan tile totals, the mover count
+  uint32_t *pstart_new = nullptr, *ps_tsums = nullptr;  // page re-sort: repacked page starts
   // re-sort choice: {movers, superdroplets} of the previous motion step, written by the device
   // into mapped pinned memory right after that step's motion kernel; an event recorded behind
   // the write (an external event node inside a captured step) lets the host wait for exactly
@@ -273,6 +297,12 @@ __device__ __forceinline__ void bounds_of(const double* lo, const double* hi, ui
   }
 }
 
+}  // namespace
+
+#include "pages.cuh"
+
+namespace {
+
 // interpolation: predcorr.cpp:30-42
 __device__ __forceinline__ double interpolation(double blo, double bhi, double vlo, double vhi,
                                                 double sdcoord) {
@@ -302,7 +332,9 @@ __device__ __forceinline__ bool beyond_domainboundary(uint32_t gbxindex, uint32_
 // k_motion: MoveSupersInGridboxesFunctor (movesupersindomain.hpp:47-93) for every droplet:
 // PredCorr::operator() (predcorr.hpp:156-171), cfl_criteria, PredCorrMotion::superdrop_gbx
 // (predcorrmotion.hpp:85-106) with get_no_decomposition_bounding_gridbox (cartesianmaps.cpp:278)
-// and CartesianCheckBounds. Writes the sort key min(gbx, ngbxs) and the position.
+// and CartesianCheckBounds. For the full re-sort it writes each slot's sort key (its new
+// gridbox, ngbxs out of the domain, ngbxs + 1 for a free slot) and position; for the page re-sort
+// it flags the movers (pages.cuh).
 __global__ void __launch_bounds__(256, 4)  // 64 registers: measured 15% faster than 80
 k_motion(const __grid_constant__ DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, int incremental) {
   const uint32_t n = c.counters[0];
@@ -312,11 +344,12 @@ k_motion(const __grid_constant__ DevCtx c, uint32_t* __restrict__ keys, uint32_t
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t g = c.sd.gbx[i];
     if (!incremental) vals[i] = i;
-    if (g >= ng) {  // null superdroplet left by collisions: out of the domain
+    if (g >= ng) {  // a null superdroplet left by collisions (out of the domain), or a free slot
+      const bool hole = is_hole(c.sd, i);
       if (incremental)
-        c.mv_scan[i] = 1;  // a mover, not one of its range's valid superdroplets
+        c.mv_scan[i] = hole ? 0u : 1u;  // a null one moves to the out-of-domain store
       else
-        keys[i] = ng;
+        keys[i] = hole ? ng + 1 : ng;
       continue;
     }
     const Where w{c.err, g, i};
@@ -439,13 +472,6 @@ k_motion(const __grid_constant__ DevCtx c, uint32_t* __restrict__ keys, uint32_t
     }
     if (!incremental) continue;
     c.mv_scan[i] = mover ? 1u : 0u;
-    if (mover) {
-      atomicAdd(&c.mv_leave[g], 1u);
-      if (key < ng) {
-        atomicAdd(&c.mv_arrive[key], 1u);
-        if (i < c.gstart[key]) atomicAdd(&c.mv_below[key], 1u);
-      }
-    }
   }
 }
 __global__ void k_mv_report(const __grid_constant__ DevCtx c, uint32_t* __restrict__ out) {  // mapped host memory
@@ -453,13 +479,7 @@ __global__ void k_mv_report(const __grid_constant__ DevCtx c, uint32_t* __restri
   out[1] = c.counters[0];
 }
 
-// ---- incremental re-sort (stable by gridbox, equal to the full radix sort) ----
-// Before motion, gridbox g's superdroplets occupy [gstart[g], gstart[g + 1]): its gcount[g] valid
-// ones first, then the nulls its collisions left. In a stable sort by the new keys, gridbox k
-// receives, in order: the movers into k from positions before its range, its stayers (valid,
-// key unchanged: gcount[k] less the valid ones that left), the movers into k from positions
-// after it; out-of-domain ones and nulls follow all gridboxes in position order. Only the
-// movers are sorted.
+// ---- the movers of a page re-sort (pages.cuh), listed in position order ----
 // the exclusive scan of the mover flags at position i: the scan within its tile plus the tile's
 // offset (the scan's own pass adding the offsets in place is left out; its readers add them)
 __device__ __forceinline__ uint32_t mv_before(const DevCtx& c, uint32_t i) {
@@ -477,103 +497,9 @@ __global__ void k_mv_list(const __grid_constant__ DevCtx c, uint32_t* __restrict
     }
   }
 }
-__global__ void k_mv_counts(const __grid_constant__ DevCtx c) {
-  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x) {
-    const uint32_t stay = c.gcount[g] - c.mv_leave[g];
-    c.mv_stay[g] = stay;
-    c.gstart_new[g] = stay + c.mv_arrive[g];  // scanned in place to the new starts
-  }
+__global__ void k_mv_count(const __grid_constant__ DevCtx c, uint32_t* __restrict__ count) {
+  *count = mv_before(c, c.counters[0]);  // number of movers
 }
-__global__ void k_mv_ends(const __grid_constant__ DevCtx c) {  // after the scan: gstart_new[ngbxs] = in-domain count
-  c.gstart_new[c.ngbxs + 1] = c.counters[0];
-}
-__global__ void k_mv_count(const __grid_constant__ DevCtx c, uint32_t* __restrict__ count) {  // number of movers
-  *count = mv_before(c, c.counters[0]);
-}
-__global__ void k_mv_arrivals(const __grid_constant__ DevCtx c) {  // to be scanned: first sorted mover of each key
-  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x)
-    c.mv_mstart[g] = c.mv_arrive[g];
-}
-__device__ __forceinline__ void mv_copy(const Fields& s, const Fields& d, uint32_t i, uint32_t o) {
-  d.gbx[o] = s.gbx[i];
-  d.c3[o] = s.c3[i];
-  d.c1[o] = s.c1[i];
-  d.c2[o] = s.c2[i];
-  d.xi[o] = s.xi[i];
-  d.r[o] = s.r[i];
-  d.msol[o] = s.msol[i];
-  d.id[o] = s.id[i];
-}
-// a stayer of gridbox g at position i goes to i - (movers before i) + shift[g]:
-// shift[g] = gstart_new[g] + mv_below[g] - gstart[g] + (movers before gstart[g]); computed per
-// gridbox together with the commit of the new gridbox starts (which nothing after this reads
-// in their old form)
-__global__ void k_mv_shift_commit(const __grid_constant__ DevCtx c) {
-  const uint32_t ng = c.ngbxs;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ng + 2; k += gridDim.x * blockDim.x) {
-    if (k < ng) {
-      const uint32_t g0 = c.gstart[k];
-      c.mv_shift[k] = c.gstart_new[k] + c.mv_below[k] - g0 + mv_before(c, g0);
-    }
-    c.gstart[k] = c.gstart_new[k];
-  }
-}
-__global__ void __launch_bounds__(256)
-k_mv_stayers(const __grid_constant__ DevCtx c, Fields src, Fields dst) {
-  constexpr int U = 2;  // superdroplets per thread and iteration, all loads issued first
-  const uint32_t n = c.counters[0];
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += U * stride) {
-    uint32_t m[U], m1[U], gb[U];
-    double c3[U], c1[U], c2[U], r[U], ms[U];
-    unsigned long long xi[U], id[U];
-    bool ok[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const uint32_t i = i0 + u * stride;
-      ok[u] = i < n;
-      if (ok[u]) {
-        m[u] = mv_before(c, i);
-        m1[u] = mv_before(c, i + 1);
-        gb[u] = src.gbx[i];  // a stayer's key: its gridbox, unchanged
-        c3[u] = src.c3[i];
-        c1[u] = src.c1[i];
-        c2[u] = src.c2[i];
-        xi[u] = src.xi[i];
-        r[u] = src.r[i];
-        ms[u] = src.msol[i];
-        id[u] = src.id[i];
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (!ok[u] || m1[u] != m[u]) continue;  // beyond the range, or a mover
-      const uint32_t o = i0 + u * stride - m[u] + c.mv_shift[gb[u]];
-      dst.gbx[o] = gb[u];
-      dst.c3[o] = c3[u];
-      dst.c1[o] = c1[u];
-      dst.c2[o] = c2[u];
-      dst.xi[o] = xi[u];
-      dst.r[o] = r[u];
-      dst.msol[o] = ms[u];
-      dst.id[o] = id[u];
-    }
-  }
-}
-__global__ void k_mv_movers(const __grid_constant__ DevCtx c, Fields src, Fields dst, const uint32_t* __restrict__ mk,
-                            const uint32_t* __restrict__ mvp) {
-  const uint32_t n = c.counters[0];
-  const uint32_t nm = mv_before(c, n);
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nm; j += gridDim.x * blockDim.x) {
-    const uint32_t k = mk[j];
-    const uint32_t r = j - c.mv_mstart[k];  // rank among the sorted movers of key k
-    const uint32_t o = k < c.ngbxs
-                           ? c.gstart_new[k] + (r < c.mv_below[k] ? r : c.mv_stay[k] + r)
-                           : c.gstart_new[c.ngbxs] + r;
-    mv_copy(src, dst, mvp[j], o);
-  }
-}
-
 // ---- superdroplet output: the domain superdroplets, gathered in gridbox order and converted
 // the way the reference's Collect* functors convert them (superdrops_observer.hpp:139-464) ----
 struct ObsOut {
@@ -619,86 +545,6 @@ __global__ void k_wait_check(uint32_t max_tries, int* __restrict__ out) {
   const bool completed = mlp::mbar_wait_bounded(&bar, 0, max_tries);
   const int all = __syncthreads_or(completed ? 1 : 0);
   if (threadIdx.x == 0) *out = all ? CLEO_OK : CLEO_ERR_TIMEOUT;
-}
-
-// sort keys of freshly uploaded droplets
-__global__ void k_keys_from_gbx(const __grid_constant__ DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
-  const uint32_t n = c.counters[0];
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t g = c.sd.gbx[i];
-    keys[i] = g < c.ngbxs ? g : c.ngbxs;
-    vals[i] = i;
-  }
-}
-
-// permute every field of the current buffer into the other one
-__global__ void k_gather(Fields src, Fields dst, const uint32_t* __restrict__ perm,
-                         const uint32_t* __restrict__ n_ptr) {
-  const uint32_t n = *n_ptr;
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-    const uint32_t s = perm[j];
-    dst.gbx[j] = src.gbx[s];
-    dst.c3[j] = src.c3[s];
-    dst.c1[j] = src.c1[s];
-    dst.c2[j] = src.c2[s];
-    dst.xi[j] = src.xi[s];
-    dst.r[j] = src.r[s];
-    dst.msol[j] = src.msol[s];
-    dst.id[j] = src.id[s];
-  }
-}
-
-// gridbox refs from the sorted keys: gstart[k] = lower_bound(keys, k) for k in [0, ngbxs + 1]
-// (find_refs by partition point, findrefs.hpp:54-126)
-__global__ void k_refs(const __grid_constant__ DevCtx c, const uint32_t* __restrict__ keys) {
-  const uint32_t n = c.counters[0];
-  const uint32_t nk = c.ngbxs + 2;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += gridDim.x * blockDim.x) {
-    uint32_t lo = 0, len = n;
-    while (len > 0) {
-      const uint32_t half = len >> 1;
-      if (keys[lo + half] < k) {
-        lo = lo + half + 1;
-        len -= half + 1;
-      } else {
-        len = half;
-      }
-    }
-    c.gstart[k] = lo;
-    if (k > 0 && k <= c.ngbxs) {
-      // gcount of gridbox k-1 written once gstart[k-1] is known: computed below
-    }
-  }
-}
-
-__global__ void k_counts(const __grid_constant__ DevCtx c) {
-  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x)
-    c.gcount[g] = c.gstart[g + 1] - c.gstart[g];
-  if (blockIdx.x == 0 && threadIdx.x == 0) c.counters[1] = c.gstart[c.ngbxs];
-}
-
-// append [ndomain, nrange) to the out-of-domain store, then nrange = ndomain
-__global__ void k_to_grave(const __grid_constant__ DevCtx c) {
-  const uint32_t nd = c.gstart[c.ngbxs];
-  const uint32_t n = c.counters[0];
-  const uint32_t ng0 = c.counters[2];
-  for (uint32_t j = nd + blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-    const uint32_t o = ng0 + (j - nd);
-    c.grave.gbx[o] = c.sd.gbx[j];
-    c.grave.c3[o] = c.sd.c3[j];
-    c.grave.c1[o] = c.sd.c1[j];
-    c.grave.c2[o] = c.sd.c2[j];
-    c.grave.xi[o] = c.sd.xi[j];
-    c.grave.r[o] = c.sd.r[j];
-    c.grave.msol[o] = c.sd.msol[j];
-    c.grave.id[o] = c.sd.id[j];
-  }
-}
-__global__ void k_grave_commit(const __grid_constant__ DevCtx c) {
-  const uint32_t nd = c.gstart[c.ngbxs];
-  c.counters[2] += c.counters[0] - nd;
-  c.counters[0] = nd;
-  c.counters[1] = nd;
 }
 
 // The sum of a gridbox's n terms in the superdroplets' order, the way the reference's
@@ -1040,9 +886,12 @@ namespace {
 
 // Two-pass form of the batch solve (the batched schedule), as k_cond_a / k_cond_b do for the
 // SDM step: pass A finishes every direct solve that converges within its first two iterations
-// (or within the seeded attempt) and lists the rest, keyed by sub-step count; pass B solves the
-// listed ones after the list has been sorted by that key, so that neighbouring lanes carry
-// similar work. Iterations spent in pass A on an abandoned seed are carried in niters_out.
+// and lists the rest, keyed by sub-step count; pass B solves the listed ones after the list has
+// been sorted by that key, so that neighbouring lanes carry similar work. With the surrogate
+// (defer_direct), pass A lists every direct solve at once (key 0, counted in ctr[1]) and leaves
+// them to the seeded solve of pass B: of independent droplets, nearly nine in ten direct solves
+// need more than two iterations from the reference guess, and the surrogate then only runs on the
+// direct solves, which are the ones that can use a seed (the sub-stepping solves cannot).
 __device__ __forceinline__ uint32_t cs_warp_append(uint32_t* ctr, bool flag) {
   const unsigned m = __ballot_sync(0xFFFFFFFFu, flag);
   uint32_t base = 0;
@@ -1054,8 +903,8 @@ __device__ __forceinline__ uint32_t cs_warp_append(uint32_t* ctr, bool flag) {
 __global__ void __launch_bounds__(256)
 k_cs_a(const __grid_constant__ DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __restrict__ msol,
        const double* __restrict__ temp, const double* __restrict__ press,
-       const double* __restrict__ s_ratio, const double* __restrict__ delt,
-       double* __restrict__ seeds, double* __restrict__ out, uint32_t* __restrict__ niters_out,
+       const double* __restrict__ s_ratio, const double* __restrict__ delt, bool defer_direct,
+       double* __restrict__ out, uint32_t* __restrict__ niters_out,
        double* __restrict__ zres, uint32_t* __restrict__ lkeys, uint32_t* __restrict__ lvals,
        uint32_t* __restrict__ ctr) {
   const NewtonCfg cfg{c.p.maxniters, c.p.rtol, c.p.atol};
@@ -1075,48 +924,41 @@ k_cs_a(const __grid_constant__ DevCtx c, uint32_t n, const double* __restrict__ 
       const double z0 = initialguess(o, r);
       const bool ucrit1 = first_unique_criteria(o, r, z0);
       double crit = 0.0;
-      uint32_t ni = 0, carried = 0;
+      uint32_t ni = 0;
       if (ucrit1 || below_critical_timestep(o, dt, crit)) {
-        bool conv = false, seeded = false, conv1 = false;
-        double z1 = 0.0;
-        GEval e = eval_g(o, dt, r, z0);
-        if (seeds && seed_ok(seeds[i])) {  // the surrogate's seed, when its residual is smaller
-          const GEval es = eval_g(o, dt, r, seeds[i]);
-          if (fabs(es.g) < fabs(e.g)) {
-            double zs;
-            conv = integrate_seeded(cfg, o, dt, r, es, ni, zs) && seeded_root_ok(o, ucrit1, zs);
-            e.z = zs;
-            seeded = true;
-            if (!conv) {
-              seeds[i] = -1.0;  // pass B starts from the reference guess
-              carried = ni;
-            }
-          }
-        }
-        if (!seeded) {
+        if (defer_direct) {
+          defer = true;  // a full solve in pass B, from the surrogate's seed
+          zres[i] = __longlong_as_double(0x7FF8000000000000ll);
+        } else {
+          bool conv = false, conv1 = false;
+          double z1 = 0.0;
+          GEval e = eval_g(o, dt, r, z0);
           e = nr_iterate(cfg, o, dt, r, e, conv, ni);
           conv1 = conv;
           z1 = e.z;
           e = nr_iterate(cfg, o, dt, r, e, conv, ni);
-        }
-        if (conv) {
-          out[i] = max_dryradius(sqrt(e.z), msol[i]);
-          if (niters_out) niters_out[i] = ni | (failed ? CLEO_NITERS_FAILED : 0u);
-        } else {
-          defer = true;  // restart until converged (impliciteuler.cpp:136-140), key 0
-          // where pass B's restart continues; NaN after an abandoned seed (a full solve)
-          zres[i] = seeded ? __longlong_as_double(0x7FF8000000000000ll) : (conv1 ? -z1 : e.z);
+          if (conv) {
+            out[i] = max_dryradius(sqrt(e.z), msol[i]);
+            if (niters_out) niters_out[i] = ni | (failed ? CLEO_NITERS_FAILED : 0u);
+          } else {
+            defer = true;  // restart until converged (impliciteuler.cpp:136-140), key 0
+            zres[i] = conv1 ? -z1 : e.z;  // where pass B's restart continues
+          }
         }
       } else {
         defer = true;
         key = deferred_key(dt, fmax(crit, c.p.cond_minsubdelt), true);
       }
-      if (defer && niters_out) niters_out[i] = carried | (failed ? CLEO_NITERS_FAILED : 0u);
+      if (defer && niters_out) niters_out[i] = failed ? CLEO_NITERS_FAILED : 0u;
     }
     const uint32_t pos = cs_warp_append(ctr, defer);
     if (defer) {
       lkeys[pos] = key;
       lvals[pos] = i;
+    }
+    if (defer_direct) {  // the key-0 rows that lead the sorted list: the surrogate's rows
+      const unsigned dm = __ballot_sync(0xFFFFFFFFu, defer && key == 0u);
+      if (dm && (threadIdx.x & 31) == (unsigned)(__ffs(dm) - 1)) atomicAdd(&ctr[1], __popc(dm));
     }
   }
 }
@@ -1154,7 +996,8 @@ k_cs_b(const __grid_constant__ DevCtx c, const double* __restrict__ radius, cons
       if (code) w.fail(code);
       newr = sqrt(rsqrd);
     } else {
-      const double seed = seeds ? seeds[i] : 0.0;
+      // seeds exist for the key-0 rows only (the direct solves pass A left to pass B)
+      const double seed = (seeds && lkeys[j] == 0u) ? seeds[i] : 0.0;
       newr = solve_condensation(cfg, dt, c.p.cond_minsubdelt, s_ratio[i], akoh, bkoh, ffactor, r,
                                 seed, ni, w);
     }
@@ -1202,7 +1045,21 @@ int grid_for(size_t n, int threads) {
   return (int)b;
 }
 
-// stable sort of the current buffer's [0, nrange) by key, then gather, refs and store append
+// exclusive scan of a[0, n) on the context's stream, in place, the total into a[n] (tsums: the
+// scan's tile totals, (n + SCAN_TILE) / SCAN_TILE + 1 words)
+void scan_u32(cleo_b200_ctx* x, uint32_t* a, uint32_t n, uint32_t* tsums) {
+  cudaStream_t s = x->stream;
+  const uint32_t nt = (uint32_t)(((uint64_t)n + SCAN_TILE - 1) / SCAN_TILE);
+  k_scan_tiles<<<nt ? nt : 1, SCAN_THREADS, 0, s>>>(a, a, n, tsums);
+  k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(tsums, nt ? nt : 1, a + n);
+  k_scan_add<<<(unsigned)((n + 255) / 256 + 1), 256, 0, s>>>(a, n, tsums);
+  x->launches += 3;
+}
+
+// Full re-sort (pages.cuh): stable radix sort of the current buffer's slots [0, nrange) by the
+// keys in keys[0] (gridbox, out of domain, free slot), then the in-domain superdroplets written
+// into the other buffer page by page with PAGE_SLACK free slots after each page, the gridboxes'
+// ranges, and the out-of-domain ones appended to their store.
 int sort_current(cleo_b200_ctx* x) {
   DevCtx& d = x->d;
   cudaStream_t s = x->stream;
@@ -1227,14 +1084,19 @@ int sort_current(cleo_b200_ctx* x) {
   // sorted (key, position) now in kin/vin
   Fields& src = x->buf[x->cur];
   Fields& dst = x->buf[1 - x->cur];
-  k_gather<<<grid_for(d.capacity, 256), 256, 0, s>>>(src, dst, vin, d.counters);
+  uint32_t* gp = d.gstart_new;
+  const int gs = grid_for(d.slots, 256), gp2 = grid_for((size_t)d.ngbxs + 2, 256);
+  k_lower_bounds<<<gp2, 256, 0, s>>>(d, kin, gp);
+  k_pg_sizes_full<<<grid_for(d.npages, 256), 256, 0, s>>>(d, gp, d.pstart);
+  x->launches += 2;
+  scan_u32(x, d.pstart, d.npages, x->ps_tsums);
+  k_gather_paged<<<gs, 256, 0, s>>>(d, src, dst, kin, vin, gp);
+  k_pg_fill_full<<<grid_for(std::max(d.npages, d.ngbxs), 256), 256, 0, s>>>(d, dst, gp);
+  k_grave_sorted<<<gs, 256, 0, s>>>(d, src, vin, gp);
+  k_full_commit<<<1, 1, 0, s>>>(d, gp);
+  x->launches += 4;
   x->cur = 1 - x->cur;
   d.sd = x->buf[x->cur];
-  k_refs<<<grid_for((size_t)d.ngbxs + 2, 256), 256, 0, s>>>(d, kin);
-  k_counts<<<grid_for(d.ngbxs, 256), 256, 0, s>>>(d);
-  k_to_grave<<<grid_for(d.capacity, 256), 256, 0, s>>>(d);
-  k_grave_commit<<<1, 1, 0, s>>>(d);
-  x->launches += 5;
   CUDA_TRY(cudaGetLastError());
   return CLEO_OK;
 }
@@ -1243,53 +1105,48 @@ int radix_pairs_on(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, u
                    const uint32_t* n_ptr, uint32_t bits, uint32_t* hist, uint32_t* tile_sums,
                    uint32_t nt);
 
-// the re-sort after motion, incremental (k_motion flagged the movers and counted them per
-// gridbox): scan of the flags, list of the movers in position order, stable radix sort of the
-// movers by key, the new gridbox starts, then every superdroplet copied once to its place
+// The page re-sort after motion (pages.cuh; k_motion flagged the movers): scan of the flags, the
+// movers listed in position order and stably radix-sorted by key, copied out to the mover
+// buffer; the touched pages rewritten in place, or, when one would outgrow its slots, every page
+// rewritten into the other buffer and copied back (the device decides; both paths are launched);
+// movers out of the domain appended to their store. The current buffer stays current.
 int sort_incremental(cleo_b200_ctx* x) {
   DevCtx& d = x->d;
   cudaStream_t s = x->stream;
-  const uint32_t ng = d.ngbxs;
-  const uint64_t n1 = (uint64_t)d.capacity + 1;
+  const uint64_t n1 = (uint64_t)d.slots + 1;
   const uint32_t nscan = (uint32_t)((n1 + SCAN_TILE - 1) / SCAN_TILE);
-  // exclusive scan of capacity + 1 flags (entries past nrange are stale but only move the
-  // values after index nrange, which nothing reads)
-  // (readers add the tile offsets: mv_before)
+  k_pg_reset<<<1, 1, 0, s>>>(d);
+  // exclusive scan of slots + 1 flags (entries past nrange are stale but only move the values
+  // after index nrange, which nothing reads) (readers add the tile offsets: mv_before)
   k_scan_tiles<<<nscan, SCAN_THREADS, 0, s>>>(d.mv_scan, d.mv_scan, n1, d.mv_tsums);
   k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(d.mv_tsums, nscan, nullptr);
-  x->launches += 2;
-  const int gc = grid_for(d.capacity, 256), gg = grid_for((size_t)ng + 2, 256);
-  k_mv_list<<<gc, 256, 0, s>>>(d, x->keys[1], x->vals[1]);
+  x->launches += 3;
+  const int gs = grid_for(d.slots, 256);
+  k_mv_list<<<gs, 256, 0, s>>>(d, x->keys[1], x->vals[1]);
   k_mv_count<<<1, 1, 0, s>>>(d, x->mv_count);
   x->launches += 2;
-  // mover count = mv_scan[nrange]: read by the radix kernels through a device pointer
+  // the movers stably by key (the mover count is read by the radix kernels on the device)
   const int where = radix_pairs_on(x, x->keys[1], x->vals[1], d.scr_p, d.scr_j, x->mv_count,
                                    x->key_bits, x->hist, x->tile_sums, x->ntiles_max);
-  uint32_t* mk = where == 0 ? x->keys[1] : d.scr_p;
-  uint32_t* mvp = where == 0 ? x->vals[1] : d.scr_j;
-  // new gridbox starts (exclusive scan of stayers + arrivals; the total is the in-domain count)
-  // and the first sorted mover of every key (exclusive scan of the arrivals)
-  k_mv_counts<<<gg, 256, 0, s>>>(d);
-  k_mv_arrivals<<<gg, 256, 0, s>>>(d);
-  const uint32_t ns2 = (uint32_t)(((uint64_t)ng + SCAN_TILE - 1) / SCAN_TILE);
-  for (uint32_t* arr : {d.gstart_new, d.mv_mstart}) {
-    k_scan_tiles<<<ns2 ? ns2 : 1, SCAN_THREADS, 0, s>>>(arr, arr, ng, x->gs_tsums);
-    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(x->gs_tsums, ns2 ? ns2 : 1, arr + ng);
-    k_scan_add<<<(unsigned)((ng + 255) / 256 + 1), 256, 0, s>>>(arr, ng, x->gs_tsums);
-  }
-  k_mv_ends<<<1, 1, 0, s>>>(d);
-  x->launches += 9;
-  Fields& src = x->buf[x->cur];
-  Fields& dst = x->buf[1 - x->cur];
-  k_mv_shift_commit<<<gg, 256, 0, s>>>(d);
-  k_mv_stayers<<<gc, 256, 0, s>>>(d, src, dst);
-  k_mv_movers<<<gc, 256, 0, s>>>(d, src, dst, mk, mvp);
-  x->launches += 3;
-  x->cur = 1 - x->cur;
-  d.sd = x->buf[x->cur];
-  k_counts<<<grid_for(ng, 256), 256, 0, s>>>(d);
-  k_to_grave<<<gc, 256, 0, s>>>(d);
-  k_grave_commit<<<1, 1, 0, s>>>(d);
+  const uint32_t* mk = where == 0 ? x->keys[1] : d.scr_p;
+  const uint32_t* mvp = where == 0 ? x->vals[1] : d.scr_j;
+  const int pgrid = 148 * 8;  // CTAs over the touched pages (persistent loop)
+  Fields& cur = x->buf[x->cur];
+  Fields& other = x->buf[1 - x->cur];
+  k_mv_gather<<<gs, 256, 0, s>>>(d, cur, mvp, x->mv_count);
+  k_pg_touch<<<gs, 256, 0, s>>>(d, mk, mvp, x->mv_count);
+  k_pg_plan<<<pgrid, 256, 0, s>>>(d, mk, mvp, x->mv_count);
+  k_grave_movers<<<gs, 256, 0, s>>>(d, x->mv_count);
+  k_grave_movers_commit<<<1, 1, 0, s>>>(d, x->mv_count);
+  k_pg_write<false><<<pgrid, 256, 0, s>>>(d, cur, mk, mvp, x->mv_count, d.pstart);
+  x->launches += 6;
+  // the repack path: its kernels return at once unless k_pg_plan chose it
+  k_pg_sizes_repack<<<pgrid, 256, 0, s>>>(d, mk, mvp, x->mv_count, x->pstart_new);
+  x->launches += 1;
+  scan_u32(x, x->pstart_new, d.npages, x->ps_tsums);
+  k_pg_write<true><<<pgrid, 256, 0, s>>>(d, other, mk, mvp, x->mv_count, x->pstart_new);
+  k_pg_copy_back<<<gs, 256, 0, s>>>(d, other, x->pstart_new);
+  k_pg_commit<<<grid_for((size_t)d.npages + 1, 256), 256, 0, s>>>(d, x->pstart_new);
   x->launches += 3;
   CUDA_TRY(cudaGetLastError());
   return CLEO_OK;
@@ -1351,11 +1208,11 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       k_b_thermo<<<gg, 256, 0, s>>>(d, b);
       x->launches += 1;
       if (x->cfg.cond_minb == 5)
-        k_cond_a<5><<<grid_for(d.capacity, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
+        k_cond_a<5><<<grid_for(d.slots, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
       else if (x->cfg.cond_minb == 4)
-        k_cond_a<4><<<grid_for(d.capacity, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
+        k_cond_a<4><<<grid_for(d.slots, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
       else
-        k_cond_a<3><<<grid_for(d.capacity, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
+        k_cond_a<3><<<grid_for(d.slots, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
       x->launches += 1;
       const int where = radix_pairs(x, b.lkeys, b.lvals, x->keys[1], x->vals[1], b.ctr, 16);
       if (where != 0) return CLEO_ERR_CUDA;  // 16 key bits: two passes, result back in place
@@ -1366,9 +1223,9 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
         w.err = reinterpret_cast<uint32_t*>(&d.err->code);
         const SdmListSeedIO io{d.sd.gbx, d.sd.r,  d.sd.msol, d.temp, d.press, b.th_s,
                                d.p.cond_delt, b.lvals, b.ctr + 9, b.dm};
-        const uint32_t tiles = (d.capacity + mlp::TILE_M - 1) / mlp::TILE_M;
+        const uint32_t tiles = (d.slots + mlp::TILE_M - 1) / mlp::TILE_M;
         mlp::k_mlp_tc<SdmListSeedIO><<<tiles < 148u * 4u ? tiles : 148u * 4u, 128, mlp::TC_SMEM,
-                                       s>>>(w, io, d.capacity);
+                                       s>>>(w, io, d.slots);
         x->launches += 1;
       }
       // pass B with the register budget of pass A's variant (grid: twice its resident CTAs)
@@ -1421,14 +1278,8 @@ int run_sdm_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
     {
       StageMark m(x, 0);
       const bool inc = !x->sort_full;
-      const size_t ngb = (size_t)(d.ngbxs ? d.ngbxs : 1) * 4;
-      if (inc) {
-        CUDA_TRY(cudaMemsetAsync(d.mv_leave, 0, ngb, s));
-        CUDA_TRY(cudaMemsetAsync(d.mv_arrive, 0, ngb, s));
-        CUDA_TRY(cudaMemsetAsync(d.mv_below, 0, ngb, s));
-      }
       CUDA_TRY(cudaMemsetAsync(d.mv_total, 0, 4, s));
-      k_motion<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, x->keys[0], x->vals[0], inc ? 1 : 0);
+      k_motion<<<grid_for(d.slots, 256), 256, 0, s>>>(d, x->keys[0], x->vals[0], inc ? 1 : 0);
       k_mv_report<<<1, 1, 0, s>>>(d, x->d_motion);
       x->launches += 2;
       {  // inside a captured step the record becomes an external event node of the graph
@@ -1605,6 +1456,10 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
                      cleo_b200_ctx** out) {
   if (!params || !grid || !out) return CLEO_ERR_ARGUMENT;
   if (capacity >= 0xFFFFFFFFull || grid->ngbxs >= 0xFFFFFFF0u) return CLEO_ERR_CAPACITY;
+  // the SoA buffers hold the pages' free slots too (pages.cuh)
+  const uint64_t npages = ((uint64_t)grid->ngbxs + PAGE_GBXS - 1) / PAGE_GBXS;
+  if ((uint64_t)capacity + (npages ? npages : 1) * PAGE_SLACK >= 0xFFFFFFF0ull)
+    return CLEO_ERR_CAPACITY;
   if (params->condstep != CLEO_STEP_OFF && params->cond_delt < params->cond_minsubdelt)
     return CLEO_ERR_SUBDELT;  // ImplicitEuler ctor, impliciteuler.hpp:320-326
   if (params->condstep == 0 || params->collstep == 0 || params->motionstep == 0)
@@ -1629,7 +1484,9 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   d.ngbxs = grid->ngbxs;
   for (int i = 0; i < 3; ++i) d.ndims[i] = grid->ndims[i];
   d.capacity = (uint32_t)capacity;
-  const size_t ng = grid->ngbxs, cap = capacity;
+  d.npages = (uint32_t)(npages ? npages : 1);
+  d.slots = (uint32_t)(capacity + (size_t)d.npages * PAGE_SLACK);
+  const size_t ng = grid->ngbxs, cap = d.slots;  // position-indexed arrays cover every slot
   int rc = 0;
   double* maps[6];
   for (int k = 0; k < 6; ++k) rc |= dalloc(x, &maps[k], ng);
@@ -1641,7 +1498,14 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &d.nr_iters, ng);
   rc |= alloc_fields(x, x->buf[0], cap);
   rc |= alloc_fields(x, x->buf[1], cap);
-  rc |= alloc_fields(x, d.grave, cap);
+  rc |= alloc_fields(x, d.grave, capacity);
+  rc |= alloc_fields(x, d.mvrec, capacity);
+  rc |= dalloc(x, &d.pstart, (size_t)d.npages + 1);
+  rc |= dalloc(x, &d.pg_flag, d.npages);
+  rc |= dalloc(x, &d.pg_list, d.npages);
+  rc |= dalloc(x, &d.pg_ctr, 4);
+  rc |= dalloc(x, &x->pstart_new, (size_t)d.npages + 1);
+  rc |= dalloc(x, &x->ps_tsums, ((size_t)d.npages + SCAN_TILE) / SCAN_TILE + 1);
   rc |= dalloc(x, &d.gstart, ng + 2);
   rc |= dalloc(x, &d.gcount, ng);
   rc |= dalloc(x, &d.counters, 4);
@@ -1678,12 +1542,6 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &x->bs.tsdm, 1);
   rc |= dalloc(x, &x->tile_sums, ((size_t)256 * x->ntiles_max + SCAN_TILE - 1) / SCAN_TILE + 1);
   rc |= dalloc(x, &d.mv_scan, (size_t)cap + 1);
-  rc |= dalloc(x, &d.mv_leave, ng);
-  rc |= dalloc(x, &d.mv_arrive, ng);
-  rc |= dalloc(x, &d.mv_below, ng);
-  rc |= dalloc(x, &d.mv_stay, ng);
-  rc |= dalloc(x, &d.mv_mstart, (size_t)ng + 1);
-  rc |= dalloc(x, &d.mv_shift, ng);
   rc |= dalloc(x, &d.mv_total, 1);
   if (cudaHostAlloc(&x->h_motion, 2 * sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess ||
       cudaHostGetDevicePointer(&x->d_motion, x->h_motion, 0) != cudaSuccess ||
@@ -1744,6 +1602,9 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   CUDA_TRY(cudaMemsetAsync(d.counters, 0, 16, x->stream));
   CUDA_TRY(cudaMemsetAsync(d.gstart, 0, (ng + 2) * 4, x->stream));
   CUDA_TRY(cudaMemsetAsync(d.gcount, 0, (ng ? ng : 1) * 4, x->stream));
+  CUDA_TRY(cudaMemsetAsync(d.pstart, 0, ((size_t)d.npages + 1) * 4, x->stream));
+  CUDA_TRY(cudaMemsetAsync(d.pg_flag, 0, (size_t)d.npages * 4, x->stream));
+  CUDA_TRY(cudaMemsetAsync(d.pg_ctr, 0, 16, x->stream));
   CUDA_TRY(cudaMemsetAsync(d.err, 0, sizeof(DevError), x->stream));
   CUDA_TRY(cudaFuncSetAttribute(k_micro, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MICRO_SMEM));
   CUDA_TRY(cudaMemsetAsync(x->bs.ctr, 0, 48, x->stream));
@@ -1892,7 +1753,7 @@ int cleo_b200_upload_supers(cleo_b200_ctx* x, const cleo_b200_supers* h, size_t 
   }
   const uint32_t cnt[4] = {(uint32_t)n, 0, 0, 0};
   CUDA_TRY(cudaMemcpyAsync(x->d.counters, cnt, 16, cudaMemcpyHostToDevice, s));
-  k_keys_from_gbx<<<grid_for(x->d.capacity, 256), 256, 0, s>>>(x->d, x->keys[0], x->vals[0]);
+  k_keys_paged<<<grid_for(x->d.slots, 256), 256, 0, s>>>(x->d, x->keys[0], x->vals[0]);
   x->launches += 1;
   const int rc = sort_current(x);  // SupersInDomain ctor: supersindomain.hpp:55-62
   if (rc) return rc;
@@ -2152,7 +2013,7 @@ int cleo_b200_gather_supers(cleo_b200_ctx* x, uint32_t vars, const cleo_b200_obs
   k_scan_tiles<<<ns ? ns : 1, SCAN_THREADS, 0, s>>>(x->obs_start, x->obs_start, ng, x->obs_tsums);
   k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(x->obs_tsums, ns ? ns : 1, x->obs_start + ng);
   k_scan_add<<<(unsigned)((ng + 255) / 256 + 1), 256, 0, s>>>(x->obs_start, ng, x->obs_tsums);
-  k_obs_gather<<<grid_for(d.capacity, 256), 256, 0, s>>>(d, o, x->obs_start);
+  k_obs_gather<<<grid_for(d.slots, 256), 256, 0, s>>>(d, o, x->obs_start);
   x->launches += 5;
   CUDA_TRY(cudaGetLastError());
   uint32_t total = 0;
@@ -2227,9 +2088,12 @@ int cleo_b200_download_supers(cleo_b200_ctx* x, cleo_b200_supers* h, size_t* n_d
   for (size_t g = 0; g < ng; ++g)
     for (uint32_t k = gstart[g]; k < gstart[g] + gcount[g]; ++k) put(dom, k);
   const size_t nd = o;
-  for (size_t g = 0; g < ng; ++g)  // null superdroplets still inside gridbox ranges
-    for (uint32_t k = gstart[g] + gcount[g]; k < gstart[g + 1]; ++k) put(dom, k);
-  for (uint32_t k = gstart[ng]; k < nrange; ++k) put(dom, k);
+  // null superdroplets still inside gridbox ranges (a page's free slots are not superdroplets)
+  for (size_t g = 0; g < ng; ++g)
+    for (uint32_t k = gstart[g] + gcount[g]; k < gstart[g + 1]; ++k)
+      if (dom.id[k] != HOLE_ID) put(dom, k);
+  for (uint32_t k = gstart[ng]; k < nrange; ++k)
+    if (dom.id[k] != HOLE_ID) put(dom, k);
   for (uint32_t k = 0; k < ngrave; ++k) put(grv, k);
   if (n_domain) *n_domain = nd;
   if (n_total) *n_total = o;
@@ -2340,10 +2204,7 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_rad
   const uint32_t tiles = (uint32_t)((n + mlp::TILE_M - 1) / mlp::TILE_M);
   const uint32_t tc_grid = tiles < 148u * 4u ? tiles : 148u * 4u;
   const double* seeds = seeded ? x->seed_buf : nullptr;
-  // every solve seeded up front: most direct solves of independent droplets need more than the
-  // two iterations of pass A, so the seed saves them (the batched SDM step instead seeds only the
-  // solves that two iterations did not settle)
-  if (seeded) {
+  if (seeded && !batched) {  // the plain form seeds every solve up front
     const CondSeedIO io{d_radius, d_msol, d_temp, d_press, d_s_ratio, d_delt, x->seed_buf};
     mlp::k_mlp_tc<CondSeedIO><<<tc_grid, 128, mlp::TC_SMEM, x->stream>>>(w, io, (uint32_t)n);
     x->launches += 1;
@@ -2369,7 +2230,7 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_rad
       ok = ok && cudaMalloc(q, n * sizeof(uint32_t)) == cudaSuccess;
     ok = ok && cudaMalloc(&cs.hist, nh * sizeof(uint32_t)) == cudaSuccess;
     ok = ok && cudaMalloc(&cs.tsums, nsums * sizeof(uint32_t)) == cudaSuccess;
-    ok = ok && cudaMalloc(&cs.ctr, sizeof(uint32_t)) == cudaSuccess;
+    ok = ok && cudaMalloc(&cs.ctr, 2 * sizeof(uint32_t)) == cudaSuccess;
     ok = ok && cudaMalloc(&cs.zres, n * sizeof(double)) == cudaSuccess;
     if (!ok) {
       x->free_cs();
@@ -2379,14 +2240,21 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_rad
     cs.cap = n;
     cs.nt = nt;
   }
-  CUDA_TRY(cudaMemsetAsync(cs.ctr, 0, sizeof(uint32_t), x->stream));
+  // ctr[0]: listed solves, ctr[1]: the direct ones among them (with the surrogate)
+  CUDA_TRY(cudaMemsetAsync(cs.ctr, 0, 2 * sizeof(uint32_t), x->stream));
   k_cs_a<<<grid_for(n, 256), 256, 0, x->stream>>>(
-      x->d, (uint32_t)n, d_radius, d_msol, d_temp, d_press, d_s_ratio, d_delt,
-      seeded ? x->seed_buf : nullptr, d_radius_out, d_niters_out, cs.zres, cs.k0, cs.v0, cs.ctr);
+      x->d, (uint32_t)n, d_radius, d_msol, d_temp, d_press, d_s_ratio, d_delt, seeded,
+      d_radius_out, d_niters_out, cs.zres, cs.k0, cs.v0, cs.ctr);
   x->launches += 1;
   const int where = radix_pairs_on(x, cs.k0, cs.v0, cs.k1, cs.v1, cs.ctr, 16, cs.hist, cs.tsums,
                                    cs.nt);
   if (where != 0) return CLEO_ERR_CUDA;  // two 8-bit passes leave the result in (k0, v0)
+  if (seeded) {  // seeds for the direct solves, which lead the sorted list
+    const CondListSeedIO io{d_radius, d_msol, d_temp,  d_press,    d_s_ratio,
+                            d_delt,   cs.v0,  cs.ctr + 1, x->seed_buf};
+    mlp::k_mlp_tc<CondListSeedIO><<<tc_grid, 128, mlp::TC_SMEM, x->stream>>>(w, io, (uint32_t)n);
+    x->launches += 1;
+  }
   k_cs_b<<<x->grid_flat * 2, 256, 0, x->stream>>>(x->d, d_radius, d_msol, d_temp, d_press,
                                                   d_s_ratio, d_delt, seeds, d_radius_out,
                                                   d_niters_out, cs.zres, cs.k0, cs.v0, cs.ctr);
