@@ -285,7 +285,8 @@ EXPORTED = (
     "cleo_b200_step", "cleo_b200_status", "cleo_b200_clear_status", "cleo_b200_domain_nsupers",
     "cleo_b200_download_supers",
     "cleo_b200_download_state", "cleo_b200_download_budgets", "cleo_b200_condensation_solve",
-    "cleo_b200_stream", "cleo_b200_kernel_launches", "cleo_b200_set_profiling",
+    "cleo_b200_stream", "cleo_b200_kernel_launches", "cleo_b200_resort_stats",
+    "cleo_b200_set_profiling",
     "cleo_b200_stage_times", "cleo_b200_sort_by_gridbox_static", "cleo_b200_version",
     "cleo_b200_mlp_create", "cleo_b200_mlp_destroy", "cleo_b200_mlp_set_params",
     "cleo_b200_mlp_get_params", "cleo_b200_mlp_features", "cleo_b200_mlp_fit_normalisation",
@@ -323,6 +324,8 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
     lib.cleo_b200_stream.restype = vp
     lib.cleo_b200_kernel_launches.argtypes = [vp, C.POINTER(C.c_uint64)]
     lib.cleo_b200_kernel_launches.restype = C.c_int
+    lib.cleo_b200_resort_stats.argtypes = [vp, C.POINTER(C.c_uint64)]
+    lib.cleo_b200_resort_stats.restype = C.c_int
     lib.cleo_b200_set_profiling.argtypes = [vp, C.c_int]
     lib.cleo_b200_set_profiling.restype = C.c_int
     lib.cleo_b200_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]

@@ -15,7 +15,9 @@
 //                  where its residual beats the reference guess's
 //   k_b_commit     warp per 32 gridboxes: the condensed mass of each one's superdroplets added
 //                  in their order, their Newton iterations, and the state update
-//   k_b_classify   gridboxes into size buckets (warp-aggregated atomics)
+//   k_b_classify   gridboxes into size buckets (warp-aggregated atomics); the warp kernel's
+//                  buckets as records {gridbox, start, count, RNG slot}
+//   k_b_tv         thread per superdroplet: the pair terminal velocities the warp kernel stages
 //   k_b_small      persistent, warp per gridbox (n <= small_max <= 128; 64- and 128-slot
 //                  variants): collisions in registers + per-warp shared memory
 //   k_b_cta<false> persistent, CTA per gridbox (small_max < n <= medium_max <= 1024): the same
@@ -91,6 +93,12 @@ __device__ __forceinline__ void warp_batch_sums(const DevCtx& c, uint32_t g0, ui
 // ---- effect_on_hydrometeor_states (movesupersindomain.hpp:95-136) ----
 // qcond of every gridbox from its (moved and sorted) superdroplets' condensate masses, added in
 // their order (warp_batch_sums)
+// qcond of gridbox g from the sum m of its superdroplets' condensate masses x xi
+__device__ __forceinline__ void set_qcond(const DevCtx& c, uint32_t g, double m) {
+  const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
+  const double rho_cond = m / c.volume[g] * R0cubed_VOL0;
+  c.qcond[g] = rho_cond / dry_air_density(c.press[g], c.temp[g], c.qvap[g]);
+}
 __global__ void __launch_bounds__(SEQ_THREADS) k_b_qcond(const __grid_constant__ DevCtx c) {
   __shared__ double dbuf[SEQ_THREADS / 32][SEQ_WIN];
   __shared__ uint32_t ubuf[SEQ_THREADS / 32][SEQ_WIN];
@@ -110,12 +118,7 @@ __global__ void __launch_bounds__(SEQ_THREADS) k_b_qcond(const __grid_constant__
                              : 0.0;
         },
         [](uint32_t) { return 0u; }, m, unused);
-    if ((uint32_t)lane < nb) {
-      const uint32_t g = g0 + lane;
-      const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
-      const double rho_cond = m / c.volume[g] * R0cubed_VOL0;
-      c.qcond[g] = rho_cond / dry_air_density(c.press[g], c.temp[g], c.qvap[g]);
-    }
+    if ((uint32_t)lane < nb) set_qcond(c, g0 + lane, m);
   }
 }
 
@@ -186,6 +189,8 @@ k_cond_a(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch 
       if (g < c.ngbxs) {
         const Where w{c.err, g, i};
         const double r = c.sd.r[i], msol = c.sd.msol[i];
+        // the condensate mass qcond sums (k_b_qcond's term), for the commit to add in order
+        if (b.qm) b.qm[i] = condensate_mass(r, msol, w) * (double)c.sd.xi[i];
         const double ffactor_fv = b.th_ff[g] / ventilation_factor(r);
         const OdeConsts o{b.th_s[g], b.th_ak[g], kohler_b(msol), ffactor_fv};
         const double z0 = initialguess_a3(o, r, b.th_a3[g]);
@@ -285,6 +290,15 @@ k_cond_b(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch 
   }
 }
 
+// ---- the pair terminal velocity of every superdroplet (for the warp kernel), a thread each:
+// the same pair_tv the kernel would evaluate, with every lane busy ----
+__global__ void __launch_bounds__(256) k_b_tv(const __grid_constant__ DevCtx c,
+                                              const __grid_constant__ BatchScratch b) {
+  const uint32_t n = c.counters[0];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (c.sd.gbx[i] < c.ngbxs) b.tv[i] = pair_tv(c.p, c.sd.r[i]);
+}
+
 // ---- size buckets of the gridboxes that hold superdroplets ----
 __global__ void k_b_classify(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b) {
   const uint32_t ng = c.ngbxs;
@@ -299,7 +313,11 @@ __global__ void k_b_classify(const __grid_constant__ DevCtx c, const __grid_cons
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const uint32_t pos = warp_append(&b.ctr[1 + q], bk == q);
-      if (bk == q) b.bucket[(size_t)q * ng + pos] = g;
+      if (bk == q) {
+        b.bucket[(size_t)q * ng + pos] = g;
+        // the warp kernel reads its gridboxes' ranges and RNG slots with the list entry
+        if (q < 2) b.brec[(size_t)q * ng + pos] = make_uint4(g, c.gstart[g], n, b.slot[g]);
+      }
     }
   }
 }
@@ -335,6 +353,12 @@ __global__ void __launch_bounds__(SEQ_THREADS) k_b_commit(const __grid_constant_
     const uint32_t nb = c.ngbxs - g0 < 32 ? c.ngbxs - g0 : 32;
     double m;
     unsigned long long it;
+    if (b.qm) {  // qcond from the moved superdroplets first (k_b_qcond's sums, from pass A)
+      warp_batch_sums(
+          c, g0, nb, dbuf[wib], ubuf[wib], [&](uint32_t i) { return b.qm[i]; },
+          [](uint32_t) { return 0u; }, m, it);
+      if ((uint32_t)lane < nb) set_qcond(c, g0 + lane, m);
+    }
     // (positions past a gridbox's valid superdroplets are loaded but not added)
     warp_batch_sums(
         c, g0, nb, dbuf[wib], ubuf[wib], [&](uint32_t i) { return b.dm[i]; },
@@ -343,24 +367,58 @@ __global__ void __launch_bounds__(SEQ_THREADS) k_b_commit(const __grid_constant_
   }
 }
 
-// one pair (2jj, 2jj+1) of the shuffled gridbox: collisions.hpp:140-158. tvA, tvB: pair_tv of
-// dA, dB.
-__device__ __forceinline__ uint32_t collide_pair(const cleo_b200_params& p, Drop& dA, Drop& dB,
+// One pair (2jj, 2jj+1) of the shuffled gridbox, collisions.hpp:140-158, on the drops at indexes
+// a and bb of the staged arrays (tvA, tvB: their pair_tv). The probability and the first random
+// number decide whether the pair's collision happens, which is rare; only then does the
+// out-of-line collide_enact draw the second number (the generator is counter based, so drawing it
+// only then gives the same number) and enact the collision on the staged drops. Pairs that do not
+// collide leave the staged arrays untouched, and the pair loop keeps few registers live.
+static __device__ __noinline__ uint32_t collide_enact(const cleo_b200_params& p,
+                                                      unsigned long long* sx, double* sr,
+                                                      double* sm, uint32_t i1, uint32_t i2,
+                                                      double prob, double phi_coll, uint64_t key,
+                                                      uint64_t slot_out, double tv1, double tv2,
+                                                      const Where& w) {
+  Drop d1{sx[i1], sr[i1], sm[i1]};
+  Drop d2{sx[i2], sr[i2], sm[i2]};
+  const double phi_out = cleo_rng_to_unit(cleo_rng_u64(key, slot_out));
+  // the pair's terminal velocities are the flag's too when both are Simmel's (pair_tv)
+  const bool tv_known = p.coll_prob == CLEO_PROB_LONG && p.flag_tv == CLEO_TV_SIMMEL;
+  const uint32_t nn = enact_collision(p, d1, d2, prob, phi_coll, phi_out, w, tv_known, tv1, tv2);
+  sx[i1] = d1.xi;
+  sr[i1] = d1.r;
+  sm[i1] = d1.msol;
+  sx[i2] = d2.xi;
+  sr[i2] = d2.r;
+  sm[i2] = d2.msol;
+  return nn;
+}
+// whether enact_collision changes anything: coalescence (alone or in CoalBuRe) when its gamma
+// (coalescence_gamma, whose min with xi1 / xi2 >= 1 keeps it nonzero) is nonzero, breakup when
+// phi_coll is below the fractional probability
+__device__ __forceinline__ bool collision_happens(const cleo_b200_params& p, double prob,
+                                                  double phi_coll) {
+  if (p.coll_enact == CLEO_ENACT_BREAKUP) return phi_coll < (prob - floor(prob));
+  uint64_t gamma = (uint64_t)floor(prob);
+  if (phi_coll < (prob - (double)gamma)) ++gamma;
+  return gamma != 0;
+}
+__device__ __forceinline__ uint32_t collide_pair(const cleo_b200_params& p, unsigned long long* sx,
+                                                 double* sr, double* sm, uint32_t a, uint32_t bb,
                                                  double tvA, double tvB, double scale_p,
                                                  double VOLUME, uint64_t key, uint64_t slot_pairs,
                                                  uint32_t jj, const Where& w) {
-  const bool swap = dA.xi < dB.xi;
-  Drop& d1 = swap ? dB : dA;
-  Drop& d2 = swap ? dA : dB;
+  const unsigned long long xa = sx[a], xb = sx[bb];
+  const bool swap = xa < xb;  // d1 is the droplet of larger xi
+  const uint32_t i1 = swap ? bb : a, i2 = swap ? a : bb;
   const double tv1 = swap ? tvB : tvA, tv2 = swap ? tvA : tvB;
-  const double prob_jk = pair_prob_tv(p, d1.r, d2.r, tv1, tv2, VOLUME);
-  const double large_xi = (double)d1.xi;
+  const double prob_jk = pair_prob_tv(p, sr[i1], sr[i2], tv1, tv2, VOLUME);
+  const double large_xi = (double)(swap ? xb : xa);
   const double prob = scale_p * large_xi * prob_jk;
   const double phi_coll = cleo_rng_to_unit(cleo_rng_u64(key, slot_pairs + 2ull * jj));
-  const double phi_out = cleo_rng_to_unit(cleo_rng_u64(key, slot_pairs + 2ull * jj + 1));
-  // the pair's terminal velocities are the flag's too when both are Simmel's (pair_tv)
-  const bool tv_known = p.coll_prob == CLEO_PROB_LONG && p.flag_tv == CLEO_TV_SIMMEL;
-  return enact_collision(p, d1, d2, prob, phi_coll, phi_out, w, tv_known, tv1, tv2);
+  if (!collision_happens(p, prob, phi_coll)) return 0;
+  return collide_enact(p, sx, sr, sm, i1, i2, prob, phi_coll, key, slot_pairs + 2ull * jj + 1,
+                       tv1, tv2, w);
 }
 
 // Fisher-Yates (shuffle.hpp:80-87) applies swap(p[i], p[J[i]]) for i = n-1 down to 1 to the
@@ -393,15 +451,16 @@ using mlp::smem_u32;
 // The 64-slot variant stages all seven 8-byte fields (r, msol, xi, coordinates, id), so its
 // write-back reads shared memory instead of gathering the coordinates and ids from global memory
 // in shuffled order; the 128-slot variant stages r, msol and xi (seven fields of 128 slots would
-// leave room for fewer CTAs per SM than its registers allow).
+// leave room for fewer CTAs per SM than its registers allow). Both stage the pair terminal
+// velocities k_b_tv computed (the last field).
 template <int CAP>
 struct SmallLayout {
   static constexpr bool ALL = CAP <= 64;
-  static constexpr uint32_t NF = ALL ? 7 : 3;  // staged fields per buffer
+  static constexpr uint32_t NF = ALL ? 8 : 4;  // staged fields per buffer
+  static constexpr uint32_t F_TV = NF - 1;
   static constexpr uint32_t BUF = CAP + 2;  // elements per staged field
   static constexpr uint32_t FIELD = BUF * 8;
-  static constexpr uint32_t OFF_TV = 2 * NF * FIELD;
-  static constexpr uint32_t OFF_P = OFF_TV + CAP * 8;
+  static constexpr uint32_t OFF_P = 2 * NF * FIELD;
   static constexpr uint32_t OFF_J = OFF_P + CAP;
   static constexpr uint32_t OFF_F = OFF_J + CAP;  // first index of each swap target (chains)
   static constexpr uint32_t OFF_BAR = (OFF_F + CAP + 15) / 16 * 16;
@@ -435,17 +494,16 @@ k_b_small(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch
   const cleo_b200_params& p = c.p;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   unsigned char* wsm = smem_small + wib * L::WARP_BYTES;
-  double* s_tv = reinterpret_cast<double*>(wsm + L::OFF_TV);
   uint8_t* s_p = wsm + L::OFF_P;
   uint8_t* s_j = wsm + L::OFF_J;
   uint8_t* s_f = wsm + L::OFF_F;
   uint64_t* bar = reinterpret_cast<uint64_t*>(wsm + L::OFF_BAR);
   const auto field = [&](int buf, int f) { return wsm + (buf * L::NF + f) * L::FIELD; };
   const uint32_t count = b.ctr[1 + q];
-  const uint32_t* list = b.bucket + (size_t)q * c.ngbxs;
-  // stage gridbox g's r, msol, xi into buffer buf (lane 0)
-  const auto stage = [&](int buf, uint32_t g) {
-    const uint32_t base = c.gstart[g], n = c.gcount[g];
+  const uint4* list = b.brec + (size_t)q * c.ngbxs;  // {gridbox, start, count, RNG slot}
+  // stage a gridbox's fields into buffer buf (lane 0)
+  const auto stage = [&](int buf, const uint4& rec) {
+    const uint32_t base = rec.y, n = rec.z;
     const uint32_t a0 = base & ~1u;
     const uint32_t bytes = ((n + (base & 1u) + 1u) & ~1u) * 8u;
     fence_async_smem();  // earlier generic accesses of the buffer precede the async writes
@@ -453,6 +511,7 @@ k_b_small(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch
     bulk_g2s(field(buf, 0), c.sd.r + a0, bytes, &bar[buf]);
     bulk_g2s(field(buf, 1), c.sd.msol + a0, bytes, &bar[buf]);
     bulk_g2s(field(buf, 2), c.sd.xi + a0, bytes, &bar[buf]);
+    bulk_g2s(field(buf, L::F_TV), b.tv + a0, bytes, &bar[buf]);
     if constexpr (L::ALL) {
       bulk_g2s(field(buf, 3), c.sd.c3 + a0, bytes, &bar[buf]);
       bulk_g2s(field(buf, 4), c.sd.c1 + a0, bytes, &bar[buf]);
@@ -460,27 +519,30 @@ k_b_small(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch
       bulk_g2s(field(buf, 6), c.sd.id + a0, bytes, &bar[buf]);
     }
   };
-  // static assignment (item = warp + k * warps): no shared counter, and the next gridbox's list
-  // entry is loaded a whole gridbox ahead
+  // static assignment (item = warp + k * warps): no shared counter; a gridbox's list record is
+  // loaded two gridboxes ahead and its copies are issued one gridbox ahead
   const uint32_t nwarps = gridDim.x * B_WARPS;
   uint32_t item = blockIdx.x * B_WARPS + wib;
-  uint32_t g_next = item < count ? list[item] : 0u;
+  const uint4 none = make_uint4(0u, 0u, 0u, 0u);
+  uint4 rec_next = item < count ? list[item] : none;
+  uint4 rec_after = item + nwarps < count ? list[item + nwarps] : none;
   uint32_t parity = 0;  // bit k: the phase of bar[k] to wait for
   int cur = 0;
   if (lane == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
-    if (item < count) stage(0, g_next);
+    if (item < count) stage(0, rec_next);
   }
   __syncwarp();
   for (; item < count; item += nwarps) {
-    const uint32_t g = g_next;
+    const uint4 rec = rec_next;
+    const uint32_t g = rec.x, base = rec.y, n = rec.z;
     const bool has_next = item + nwarps < count;
-    if (has_next) g_next = list[item + nwarps];
-    const uint32_t base = c.gstart[g];
-    const uint32_t n = c.gcount[g];
+    rec_next = rec_after;
+    rec_after = item + 2 * nwarps < count ? list[item + 2 * nwarps] : none;
     // the next gridbox's copies go out before this one's wait
-    if (has_next && lane == 0) stage(cur ^ 1, g_next);
+    if (has_next && lane == 0) stage(cur ^ 1, rec_next);
+    const double VOLUME = c.volume[g] * VOL0;  // issued before the wait
     if (!mbar_wait_bounded(&bar[cur], (parity >> cur) & 1u, MBAR_TRIES)) {
       // the step fails with CLEO_ERR_TIMEOUT; before the warp leaves, the copies still in flight
       // into either buffer get a bounded wait to land
@@ -494,13 +556,11 @@ k_b_small(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch
     double* s_r = reinterpret_cast<double*>(field(cur, 0)) + off;
     double* s_m = reinterpret_cast<double*>(field(cur, 1)) + off;
     unsigned long long* s_x = reinterpret_cast<unsigned long long*>(field(cur, 2)) + off;
+    const double* s_tv = reinterpret_cast<const double*>(field(cur, L::F_TV)) + off;
     const uint64_t key = cleo_rng_key(p.seed, t_sdm, g);
-    const uint64_t slot = b.slot[g];
-    for (uint32_t k = lane; k < n; k += 32) {
-      s_tv[k] = pair_tv(p, s_r[k]);
-      if (k >= 1)
-        s_j[k] = (uint8_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - k)), 0, (uint64_t)k + 1);
-    }
+    const uint64_t slot = rec.w;
+    for (uint32_t k = 1 + lane; k < n; k += 32)
+      s_j[k] = (uint8_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - k)), 0, (uint64_t)k + 1);
     __syncwarp();
     {
       // origins of the shuffled positions (what fy_origin computes), by chains: tracing position
@@ -547,17 +607,12 @@ k_b_small(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch
     const uint64_t slot_pairs = slot + (n >= 1 ? n - 1 : 0);
     const uint32_t npairs = n / 2;
     const double scale_p = (double)n * ((double)n - 1.0) / (2.0 * (double)npairs);
-    const double VOLUME = c.volume[g] * VOL0;
     uint32_t nnull = 0;
     for (uint32_t jj = lane; jj < npairs; jj += 32) {
       const uint32_t a = s_p[2 * jj], bb = s_p[2 * jj + 1];
       const Where w{c.err, g, (uint64_t)base + 2 * jj};
-      Drop dA{s_x[a], s_r[a], s_m[a]};
-      Drop dB{s_x[bb], s_r[bb], s_m[bb]};
-      nnull += collide_pair(p, dA, dB, s_tv[a], s_tv[bb], scale_p, VOLUME, key, slot_pairs, jj,
-                            w);
-      s_x[a] = dA.xi; s_r[a] = dA.r; s_m[a] = dA.msol;
-      s_x[bb] = dB.xi; s_r[bb] = dB.r; s_m[bb] = dB.msol;
+      nnull += collide_pair(p, s_x, s_r, s_m, a, bb, s_tv[a], s_tv[bb], scale_p, VOLUME, key,
+                            slot_pairs, jj, w);
     }
     __syncwarp();
     const uint32_t totnull = warp_sum_u(nnull);
@@ -780,13 +835,10 @@ k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b
     for (uint32_t jj = tid; jj < npairs; jj += B_THREADS) {
       const uint32_t a = P[2 * jj], bb = P[2 * jj + 1];
       const Where w{c.err, g, (uint64_t)base + 2 * jj};
-      Drop dA{Sx[a], Sr[a], Sm[a]};
-      Drop dB{Sx[bb], Sr[bb], Sm[bb]};
-      const double tvA = LARGE ? pair_tv(p, dA.r) : Stv[a];
-      const double tvB = LARGE ? pair_tv(p, dB.r) : Stv[bb];
-      nnull += collide_pair(p, dA, dB, tvA, tvB, scale_p, VOLUME, key, slot_pairs, jj, w);
-      Sx[a] = dA.xi; Sr[a] = dA.r; Sm[a] = dA.msol;
-      Sx[bb] = dB.xi; Sr[bb] = dB.r; Sm[bb] = dB.msol;
+      const double tvA = LARGE ? pair_tv(p, Sr[a]) : Stv[a];
+      const double tvB = LARGE ? pair_tv(p, Sr[bb]) : Stv[bb];
+      nnull += collide_pair(p, Sx, Sr, Sm, a, bb, tvA, tvB, scale_p, VOLUME, key, slot_pairs, jj,
+                            w);
     }
     const uint32_t totnull = block_sum(nnull, shw);
     const uint32_t nvalid = n - totnull;

@@ -23,10 +23,15 @@ struct BatchScratch {
   double* th_u3;     // per gridbox unique_a3(akoh)
   double* dm;        // per superdroplet condensed mass x xi
   uint32_t* its;     // per superdroplet Newton iterations
+  double* qm;        // per superdroplet condensate mass x xi before the solves, when the first
+                     // condensation sub-step after motion also gives qcond (else null)
+  double* tv;        // per superdroplet pair terminal velocity (pair_tv) for the warp kernel,
+                     // two elements of padding for its bulk copies
   double* zres;      // per deferred direct solve: pass A's iterate that pass B resumes from
   uint32_t* lkeys;   // cost keys of deferred solves
   uint32_t* lvals;   // positions of deferred solves
   uint32_t* bucket;  // [4][ngbxs] gridbox lists per size bucket
+  uint4* brec;       // [2][ngbxs] the warp kernel's buckets as {gridbox, start, count, RNG slot}
   uint32_t* slot;    // per gridbox RNG slot offset within the SDM step
   uint32_t* ctr;     // [0] deferred solves, [1..4] bucket counts, [5..8] bucket heads,
                      // [9] restarts among the deferred solves

@@ -571,7 +571,7 @@ int cleo_b200_mlp_infer(cleo_b200_mlp* m, size_t n, const float* d_features, flo
   const uint32_t nn = (uint32_t)n;
   if (path == CLEO_MLP_TCGEN05) {
     const uint32_t tiles = (nn + TILE_M - 1) / TILE_M;
-    const uint32_t grid = tiles < 148u * 4u ? tiles : 148u * 4u;
+    const uint32_t grid = tiles < TC_GRID_MAX ? tiles : TC_GRID_MAX;
     k_mlp_tc<ArrayIO><<<grid, 128, TC_SMEM, m->stream>>>(w, io, nn);
   } else if (path == CLEO_MLP_MMA_SYNC) {
     const uint32_t tiles = (nn + 15) / 16;

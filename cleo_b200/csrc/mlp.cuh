@@ -221,6 +221,9 @@ constexpr uint32_t SM_FW = SM_B + W2_UMMA_BYTES;                      // 24576
 constexpr uint32_t SM_BAR = SM_FW + ((NFW * 4 + 15) / 16) * 16;       // 27216
 constexpr uint32_t SM_TSLOT = SM_BAR + 8;
 constexpr uint32_t TC_SMEM = 32768;  // rounded up: at most 7 CTAs per SM, 448 of 512 TMEM columns
+// persistent grid of the tensor-core kernel: every SM's 7 resident CTAs (tile phases of different
+// CTAs overlap: the CUDA-core layers of one with the MMA of another)
+constexpr uint32_t TC_GRID_MAX = 148u * 7u;
 static_assert(SM_TSLOT + 4 <= TC_SMEM, "tensor-core kernel shared memory");
 constexpr uint32_t MBAR_TRIES = 1u << 22;
 

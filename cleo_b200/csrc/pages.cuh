@@ -148,11 +148,12 @@ __global__ void k_full_commit(const __grid_constant__ DevCtx c, const uint32_t* 
 
 // ---- re-sort after motion ----
 // pg_ctr: [0] pages touched, [1] a page outgrows its slots (repack), [2] movers into the
-// out-of-domain store (their first sorted index), [3] unused
+// out-of-domain store (their first sorted index), [3] the re-sort's stamp (counts re-sorts)
 __global__ void k_pg_reset(const __grid_constant__ DevCtx c) {
   c.pg_ctr[0] = 0;
   c.pg_ctr[1] = 0;
   c.pg_ctr[2] = 0;
+  c.pg_ctr[3] += 1;
 }
 // the movers' records, in their sorted order
 __global__ void __launch_bounds__(256)
@@ -177,32 +178,115 @@ __global__ void k_pg_touch(const __grid_constant__ DevCtx c, const uint32_t* __r
   }
 }
 
-// One page's new content, worked out by a CTA: per gridbox (a warp each) its stayers, counted
-// and (stage) copied compacted into the scratch fields at its old range, and the sorted movers into
-// it, split at its old start; then the new starts (a scan over the page's gridboxes).
+// each gridbox's run of sorted movers [mv_lo, mv_hi), stamped with this re-sort's stamp (a
+// gridbox whose stamp is older has no arrivals)
+__global__ void k_mv_runs(const __grid_constant__ DevCtx c, const uint32_t* __restrict__ mk,
+                          const uint32_t* __restrict__ m_ptr) {
+  const uint32_t m = *m_ptr, stamp = c.pg_ctr[3];
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    const uint32_t k = mk[j];
+    if (k >= c.ngbxs) continue;
+    if (j == 0 || mk[j - 1] != k) {
+      c.mv_lo[k] = j;
+      c.mv_stamp[k] = stamp;
+    }
+    if (j + 1 == m || mk[j + 1] != k) c.mv_hi[k] = j + 1;
+  }
+}
+
+// One page's new content, worked out by a CTA: per gridbox (a warp each) its stayers counted and
+// the sorted movers into it, split at its old start (plan_page); then where each gridbox goes
+// (place_page) and which gridboxes are rewritten.
 struct PagePlan {
-  uint32_t b[PAGE_GBXS];     // old start
-  uint32_t ns[PAGE_GBXS];    // stayers
-  uint32_t lo[PAGE_GBXS];    // first sorted mover into the gridbox
-  uint32_t nl[PAGE_GBXS];    // movers from positions before its old start
-  uint32_t na[PAGE_GBXS];    // movers into it
-  uint32_t st[PAGE_GBXS];    // new start relative to the page's first slot
-  uint32_t total;
+  uint32_t b[PAGE_GBXS];   // old start
+  uint32_t oc[PAGE_GBXS];  // old count
+  uint32_t ns[PAGE_GBXS];  // stayers
+  uint32_t lo[PAGE_GBXS];  // first sorted mover into the gridbox
+  uint32_t nl[PAGE_GBXS];  // movers from positions before its old start
+  uint32_t na[PAGE_GBXS];  // movers into it
+  uint32_t st[PAGE_GBXS];  // new start (absolute slot)
+  uint8_t rw[PAGE_GBXS];   // rewritten (content or start changes)
+  uint32_t total;          // new count of the page
 };
-__device__ void plan_page(const DevCtx& c, uint32_t p, const uint32_t* mk, const uint32_t* mvp,
-                          uint32_t m, bool stage, PagePlan& pl) {
+__device__ void plan_page(const DevCtx& c, uint32_t p, const uint32_t* mvp, PagePlan& pl) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const uint32_t g0 = p * PAGE_GBXS, ng = min(PAGE_GBXS, c.ngbxs - g0);
-  const Fields& S = c.sd;
   for (uint32_t q = warp; q < ng; q += nw) {
     const uint32_t g = g0 + q;
     const uint32_t b = c.gstart[g], n = c.gcount[g];
     uint32_t nst = 0;
     for (uint32_t k0 = 0; k0 < n; k0 += 32) {
       const uint32_t k = k0 + lane;
+      nst += __popc(__ballot_sync(0xFFFFFFFFu, k < n && c.sd.gbx[b + k] == g));
+    }
+    // the movers into g (k_mv_runs), sorted by position: those before its old start lead
+    const bool has = c.mv_stamp[g] == c.pg_ctr[3];
+    const uint32_t lo = has ? c.mv_lo[g] : 0u, na = has ? c.mv_hi[g] - lo : 0u;
+    uint32_t nl = 0;
+    for (uint32_t t = lane; t < na; t += 32) nl += mvp[lo + t] < b ? 1u : 0u;
+    nl = __reduce_add_sync(0xFFFFFFFFu, nl);
+    if (lane == 0) {
+      pl.b[q] = b;
+      pl.oc[q] = n;
+      pl.ns[q] = nst;
+      pl.lo[q] = lo;
+      pl.na[q] = na;
+      pl.nl[q] = nl;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t s = 0;
+    for (uint32_t q = 0; q < ng; ++q) s += pl.ns[q] + pl.na[q];
+    pl.total = s;
+  }
+  __syncthreads();
+}
+// Where the page's gridboxes go in [pbase, pend). In place (keep), each keeps its start unless
+// the one before it now reaches past it, so that a superdroplet moving between neighbouring
+// gridboxes rewrites those two and the free slots stay where superdroplets left; when that does
+// not fit (or into a fresh page), the gridboxes are packed from pbase. A gridbox is rewritten
+// when superdroplets left or entered it or its start moved; the others stay where they are.
+__device__ void place_page(const DevCtx& c, uint32_t p, uint32_t pbase, uint32_t pend, bool keep,
+                           PagePlan& pl) {
+  if (threadIdx.x == 0) {
+    const uint32_t ng = min(PAGE_GBXS, c.ngbxs - p * PAGE_GBXS);
+    bool fits = false;
+    if (keep) {
+      uint32_t e = pbase;
+      for (uint32_t q = 0; q < ng; ++q) {
+        const uint32_t s = max(pl.b[q], e);
+        pl.st[q] = s;
+        e = s + pl.ns[q] + pl.na[q];
+      }
+      fits = e <= pend;
+    }
+    if (!fits) {
+      uint32_t e = pbase;
+      for (uint32_t q = 0; q < ng; ++q) {
+        pl.st[q] = e;
+        e += pl.ns[q] + pl.na[q];
+      }
+    }
+    for (uint32_t q = 0; q < ng; ++q)
+      pl.rw[q] = (!keep || pl.ns[q] != pl.oc[q] || pl.na[q] != 0 || pl.st[q] != pl.b[q]) ? 1 : 0;
+  }
+  __syncthreads();
+}
+// the stayers of the rewritten gridboxes, compacted into the scratch fields at their old ranges
+__device__ void stage_page(const DevCtx& c, uint32_t p, const PagePlan& pl) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const uint32_t g0 = p * PAGE_GBXS, ng = min(PAGE_GBXS, c.ngbxs - g0);
+  const Fields& S = c.sd;
+  for (uint32_t q = warp; q < ng; q += nw) {
+    if (!pl.rw[q]) continue;  // uniform across the warp
+    const uint32_t g = g0 + q, b = pl.b[q], n = pl.oc[q];
+    uint32_t nst = 0;
+    for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+      const uint32_t k = k0 + lane;
       const bool st = k < n && S.gbx[b + k] == g;
       const unsigned bal = __ballot_sync(0xFFFFFFFFu, st);
-      if (stage && st) {
+      if (st) {
         const uint32_t o = b + nst + __popc(bal & ((1u << lane) - 1u));
         const uint32_t i = b + k;
         c.scr_c3[o] = S.c3[i];
@@ -215,23 +299,6 @@ __device__ void plan_page(const DevCtx& c, uint32_t p, const uint32_t* mk, const
       }
       nst += __popc(bal);
     }
-    if (lane == 0) {
-      const uint32_t lo = lower_bound_u32(mk, m, g), hi = lower_bound_u32(mk, m, g + 1);
-      pl.b[q] = b;
-      pl.ns[q] = nst;
-      pl.lo[q] = lo;
-      pl.na[q] = hi - lo;
-      pl.nl[q] = lower_bound_u32(mvp + lo, hi - lo, b);  // movers sorted by position within g
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t s = 0;
-    for (uint32_t q = 0; q < ng; ++q) {
-      pl.st[q] = s;
-      s += pl.ns[q] + pl.na[q];
-    }
-    pl.total = s;
   }
   __syncthreads();
 }
@@ -241,58 +308,68 @@ __global__ void __launch_bounds__(256)
 k_pg_plan(const __grid_constant__ DevCtx c, const uint32_t* __restrict__ mk,
           const uint32_t* __restrict__ mvp, const uint32_t* __restrict__ m_ptr) {
   __shared__ PagePlan pl;
-  const uint32_t np = c.pg_ctr[0], m = *m_ptr;
+  const uint32_t np = c.pg_ctr[0];
   for (uint32_t it = blockIdx.x; it < np; it += gridDim.x) {
     const uint32_t p = c.pg_list[it];
-    plan_page(c, p, mk, mvp, m, false, pl);
+    plan_page(c, p, mvp, pl);
     if (threadIdx.x == 0 && pl.total > c.pstart[p + 1] - c.pstart[p]) atomicExch(&c.pg_ctr[1], 1u);
     __syncthreads();
   }
 }
 
 // A page written from its plan: REPACK = false rewrites the touched pages in place (taken when no
-// page outgrows its slots); REPACK = true writes every page into dst at the new page starts
-// (taken when one does; then dst is copied back).
+// page outgrows its slots), REPACK = true writes every page packed into dst at the new page starts
+// (taken when one does; then dst is copied back). Every slot of the page outside its gridboxes'
+// new ranges is left a hole.
 template <bool REPACK>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)  // (256) alone caps it at 32 registers, with spills
 k_pg_write(const __grid_constant__ DevCtx c, Fields dst, const uint32_t* __restrict__ mk,
            const uint32_t* __restrict__ mvp, const uint32_t* __restrict__ m_ptr,
            const uint32_t* __restrict__ pnew) {
   __shared__ PagePlan pl;
   if ((c.pg_ctr[1] != 0) != REPACK) return;  // the other path is taken
-  const uint32_t np = REPACK ? c.npages : c.pg_ctr[0], m = *m_ptr;
+  const uint32_t np = REPACK ? c.npages : c.pg_ctr[0];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const Fields& M = c.mvrec;
   for (uint32_t it = blockIdx.x; it < np; it += gridDim.x) {
     const uint32_t p = REPACK ? it : c.pg_list[it];
-    plan_page(c, p, mk, mvp, m, true, pl);
+    plan_page(c, p, mvp, pl);
     const uint32_t g0 = p * PAGE_GBXS, ng = min(PAGE_GBXS, c.ngbxs - g0);
     const uint32_t base = pnew[p], end = pnew[p + 1];
+    place_page(c, p, base, end, !REPACK, pl);
+    stage_page(c, p, pl);
     for (uint32_t q = warp; q < ng; q += nw) {
-      const uint32_t g = g0 + q, ns = base + pl.st[q];
+      const uint32_t g = g0 + q, ns = pl.st[q];
       const uint32_t nl = pl.nl[q], nst = pl.ns[q], na = pl.na[q], lo = pl.lo[q], b = pl.b[q];
-      for (uint32_t t = lane; t < na + nst; t += 32) {
-        const bool arrival = t < nl || t >= nl + nst;
-        const uint32_t o = ns + t;
-        if (arrival) {
-          copy_rec(M, lo + (t < nl ? t : t - nst), dst, o);
-        } else {
-          const uint32_t i = b + (t - nl);
-          dst.gbx[o] = g;
-          dst.c3[o] = c.scr_c3[i];
-          dst.c1[o] = c.scr_c1[i];
-          dst.c2[o] = c.scr_c2[i];
-          dst.xi[o] = c.scr_x[i];
-          dst.r[o] = c.scr_r[i];
-          dst.msol[o] = c.scr_m[i];
-          dst.id[o] = c.scr_id[i];
+      if (pl.rw[q]) {
+        for (uint32_t t = lane; t < na + nst; t += 32) {
+          const bool arrival = t < nl || t >= nl + nst;
+          const uint32_t o = ns + t;
+          if (arrival) {
+            copy_rec(M, lo + (t < nl ? t : t - nst), dst, o);
+          } else {
+            const uint32_t i = b + (t - nl);
+            dst.gbx[o] = g;
+            dst.c3[o] = c.scr_c3[i];
+            dst.c1[o] = c.scr_c1[i];
+            dst.c2[o] = c.scr_c2[i];
+            dst.xi[o] = c.scr_x[i];
+            dst.r[o] = c.scr_r[i];
+            dst.msol[o] = c.scr_m[i];
+            dst.id[o] = c.scr_id[i];
+          }
         }
       }
+      // the free slots after the gridbox, up to the next one's start (or the page's end), and
+      // before the first one
+      const uint32_t gap_end = q + 1 < ng ? pl.st[q + 1] : end;
+      for (uint32_t o = ns + na + nst + lane; o < gap_end; o += 32) set_hole(dst, o);
+      if (q == 0)
+        for (uint32_t o = base + lane; o < ns; o += 32) set_hole(dst, o);
     }
-    for (uint32_t o = base + pl.total + threadIdx.x; o < end; o += blockDim.x) set_hole(dst, o);
     __syncthreads();  // every warp has read the page's old starts from pl
     for (uint32_t q = threadIdx.x; q < ng; q += blockDim.x) {
-      c.gstart[g0 + q] = base + pl.st[q];
+      c.gstart[g0 + q] = pl.st[q];
       c.gcount[g0 + q] = pl.ns[q] + pl.na[q];
     }
     if (!REPACK && threadIdx.x == 0) c.pg_flag[p] = 0;
@@ -306,9 +383,8 @@ k_pg_sizes_repack(const __grid_constant__ DevCtx c, const uint32_t* __restrict__
                   uint32_t* __restrict__ psize) {
   __shared__ PagePlan pl;
   if (c.pg_ctr[1] == 0) return;
-  const uint32_t m = *m_ptr;
   for (uint32_t p = blockIdx.x; p < c.npages; p += gridDim.x) {
-    plan_page(c, p, mk, mvp, m, false, pl);
+    plan_page(c, p, mvp, pl);
     if (threadIdx.x == 0) psize[p] = pl.total + PAGE_SLACK;
     __syncthreads();
   }

@@ -125,9 +125,11 @@ __device__ __forceinline__ double tv_simmel(double radius) {  // :57-85
   if (radius >= r3) return a4;
   const double massconst = 4.0 / 3.0 * PI * Rho_l;  // watermass :32-40
   const double MASS = (massconst * radius * radius * radius) * MASS0grams;
-  if (radius >= r2) return a3 * dpow(MASS, 1.0 / 6.0);
-  if (radius >= r1) return a2 * dpow(MASS, 1.0 / 3.0);
-  return a1 * dpow(MASS, 2.0 / 3.0);
+  // the three branches' a * MASS^y with one inlined pow (the same values)
+  const bool big = radius >= r2, mid = radius >= r1;
+  const double a = big ? a3 : (mid ? a2 : a1);
+  const double y = big ? 1.0 / 6.0 : (mid ? 1.0 / 3.0 : 2.0 / 3.0);
+  return a * dpow(MASS, y);
 }
 __device__ __forceinline__ double tv_rogersyau(double radius) {  // :95-117
   const double r1 = 3e-5 / R0;
@@ -149,11 +151,13 @@ __device__ __forceinline__ double tv_rogersgk(double radius) {  // :127-147
   const double acaps = 9.65 / W0;
   const double bcaps = 10.43 / W0;
   const double ccaps = -1.0 * 2.0 * 0.6 * 1000 * R0;
-  if (radius < radius0) {
-    const double term = 1.0 - dexp(smallk * radius);
+  const bool small = radius < radius0;  // both branches with one inlined exp (same values)
+  const double e = dexp((small ? smallk : ccaps) * radius);
+  if (small) {
+    const double term = 1.0 - e;
     return term * kcaps * radius;
   }
-  return acaps - bcaps * dexp(ccaps * radius);
+  return acaps - bcaps * e;
 }
 __device__ __forceinline__ double terminalv(int kind, double radius) {
   switch (kind) {

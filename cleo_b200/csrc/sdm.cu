@@ -89,6 +89,7 @@ struct DevCtx {
   // buffers' length (capacity plus the pages' slack)
   uint32_t npages, slots;
   uint32_t *pstart, *pg_flag, *pg_list, *pg_ctr;
+  uint32_t *mv_lo, *mv_hi, *mv_stamp;  // per gridbox: its run of sorted movers, the re-sort's stamp
   Fields mvrec;
   // scratch
   double *scr_r, *scr_m, *scr_c3, *scr_c1, *scr_c2;
@@ -109,27 +110,6 @@ struct CondSeedIO {
   }
   __device__ __forceinline__ uint32_t rows(uint32_t n) const { return n; }
 };
-// the same for the batched form: row j is the j-th entry of pass A's sorted list, whose first
-// *count entries are the direct solves (key 0)
-struct CondListSeedIO {
-  const double *radius, *msol, *temp, *press, *s_ratio, *delt;
-  const uint32_t* list;
-  const uint32_t* count;
-  double* seed;
-  __device__ __forceinline__ void features(uint32_t j, float x[mlp::NIN]) const {
-    const uint32_t i = list[j];
-    mlp::raw_features(radius[i], msol[i], temp[i], press[i], s_ratio[i], delt[i], x);
-  }
-  __device__ __forceinline__ void store(uint32_t j, float t) const {
-    const uint32_t i = list[j];
-    seed[i] = mlp::seed_from(radius[i], t);
-  }
-  __device__ __forceinline__ uint32_t rows(uint32_t n) const {
-    const uint32_t c = *count;
-    return c < n ? c : n;
-  }
-};
-
 }  // namespace
 
 #include "batched_types.cuh"
@@ -145,6 +125,7 @@ struct cleo_b200_ctx {
   uint32_t *keys[2], *vals[2], *hist, *tile_sums;
   uint32_t *gs_tsums = nullptr, *mv_count = nullptr;  // scan tile totals, the mover count
   uint32_t *pstart_new = nullptr, *ps_tsums = nullptr;  // page re-sort: repacked page starts
+  double* qm_buf = nullptr;  // BatchScratch::qm's storage
   // re-sort choice: {movers, superdroplets} of the previous motion step, written by the device
   // into mapped pinned memory right after that step's motion kernel; an event recorded behind
   // the write (an external event node inside a captured step) lets the host wait for exactly
@@ -200,10 +181,11 @@ struct cleo_b200_ctx {
                           // compiled for
     uint32_t small_max;   // gridboxes up to this size go to the warp kernel
     int small_minb;       // 64-slot warp kernel: resident CTAs per SM it is compiled for
+    int condb_minb;       // pass-B variant (3, 4 or 5), tuned apart from pass A's
   };
-  TuneCfg cfg{256, 3, SMALL_MAX, 2};
+  TuneCfg cfg{256, 3, SMALL_MAX, 2, 3};
   std::vector<TuneCfg> cand;
-  std::vector<double> t_cond, t_coll;
+  std::vector<double> t_cond, t_condb, t_coll;
   size_t tune_step = 0, tune_total = 0;
   std::string tune_key;
   // CUDA graphs of batched SDM steps, keyed by what decides a step's launch sequence (the
@@ -252,6 +234,8 @@ struct cleo_b200_ctx {
 
 namespace {
 // RAII stage marker: records an event pair around a stage when profiling is on
+// stage indexes of cleo_b200_stage_times are 0..4; marks past them are the tuner's own
+constexpr int STAGE_COND_B = 5;
 struct StageMark {
   cleo_b200_ctx* x;
   int stage;
@@ -446,10 +430,13 @@ k_motion(const __grid_constant__ DevCtx c, uint32_t* __restrict__ keys, uint32_t
         idx = nghbr;
       }
     }
-    c.sd.c3[i] = n3;
-    c.sd.c1[i] = n1;
-    c.sd.c2[i] = n2;
-    c.sd.gbx[i] = idx;
+    // a field whose bits did not change is not stored (sedimentation alone changes coord3 only,
+    // and few superdroplets change gridbox): the same values, less DRAM written
+    const auto bits = [](double v) { return __double_as_longlong(v); };
+    if (bits(n3) != bits(c3)) c.sd.c3[i] = n3;
+    if (bits(n1) != bits(c1)) c.sd.c1[i] = n1;
+    if (bits(n2) != bits(c2)) c.sd.c2[i] = n2;
+    if (idx != g) c.sd.gbx[i] = idx;
     if (idx < ng) {  // CartesianCheckBounds (cartesian_motion.hpp:38-54)
       double l, h;
       bool bad = false;
@@ -886,12 +873,9 @@ namespace {
 
 // Two-pass form of the batch solve (the batched schedule), as k_cond_a / k_cond_b do for the
 // SDM step: pass A finishes every direct solve that converges within its first two iterations
-// and lists the rest, keyed by sub-step count; pass B solves the listed ones after the list has
-// been sorted by that key, so that neighbouring lanes carry similar work. With the surrogate
-// (defer_direct), pass A lists every direct solve at once (key 0, counted in ctr[1]) and leaves
-// them to the seeded solve of pass B: of independent droplets, nearly nine in ten direct solves
-// need more than two iterations from the reference guess, and the surrogate then only runs on the
-// direct solves, which are the ones that can use a seed (the sub-stepping solves cannot).
+// (or within the seeded attempt) and lists the rest, keyed by sub-step count; pass B solves the
+// listed ones after the list has been sorted by that key, so that neighbouring lanes carry
+// similar work. Iterations spent in pass A on an abandoned seed are carried in niters_out.
 __device__ __forceinline__ uint32_t cs_warp_append(uint32_t* ctr, bool flag) {
   const unsigned m = __ballot_sync(0xFFFFFFFFu, flag);
   uint32_t base = 0;
@@ -903,8 +887,8 @@ __device__ __forceinline__ uint32_t cs_warp_append(uint32_t* ctr, bool flag) {
 __global__ void __launch_bounds__(256)
 k_cs_a(const __grid_constant__ DevCtx c, uint32_t n, const double* __restrict__ radius, const double* __restrict__ msol,
        const double* __restrict__ temp, const double* __restrict__ press,
-       const double* __restrict__ s_ratio, const double* __restrict__ delt, bool defer_direct,
-       double* __restrict__ out, uint32_t* __restrict__ niters_out,
+       const double* __restrict__ s_ratio, const double* __restrict__ delt,
+       double* __restrict__ seeds, double* __restrict__ out, uint32_t* __restrict__ niters_out,
        double* __restrict__ zres, uint32_t* __restrict__ lkeys, uint32_t* __restrict__ lvals,
        uint32_t* __restrict__ ctr) {
   const NewtonCfg cfg{c.p.maxniters, c.p.rtol, c.p.atol};
@@ -924,41 +908,48 @@ k_cs_a(const __grid_constant__ DevCtx c, uint32_t n, const double* __restrict__ 
       const double z0 = initialguess(o, r);
       const bool ucrit1 = first_unique_criteria(o, r, z0);
       double crit = 0.0;
-      uint32_t ni = 0;
+      uint32_t ni = 0, carried = 0;
       if (ucrit1 || below_critical_timestep(o, dt, crit)) {
-        if (defer_direct) {
-          defer = true;  // a full solve in pass B, from the surrogate's seed
-          zres[i] = __longlong_as_double(0x7FF8000000000000ll);
-        } else {
-          bool conv = false, conv1 = false;
-          double z1 = 0.0;
-          GEval e = eval_g(o, dt, r, z0);
+        bool conv = false, seeded = false, conv1 = false;
+        double z1 = 0.0;
+        GEval e = eval_g(o, dt, r, z0);
+        if (seeds && seed_ok(seeds[i])) {  // the surrogate's seed, when its residual is smaller
+          const GEval es = eval_g(o, dt, r, seeds[i]);
+          if (fabs(es.g) < fabs(e.g)) {
+            double zs;
+            conv = integrate_seeded(cfg, o, dt, r, es, ni, zs) && seeded_root_ok(o, ucrit1, zs);
+            e.z = zs;
+            seeded = true;
+            if (!conv) {
+              seeds[i] = -1.0;  // pass B starts from the reference guess
+              carried = ni;
+            }
+          }
+        }
+        if (!seeded) {
           e = nr_iterate(cfg, o, dt, r, e, conv, ni);
           conv1 = conv;
           z1 = e.z;
           e = nr_iterate(cfg, o, dt, r, e, conv, ni);
-          if (conv) {
-            out[i] = max_dryradius(sqrt(e.z), msol[i]);
-            if (niters_out) niters_out[i] = ni | (failed ? CLEO_NITERS_FAILED : 0u);
-          } else {
-            defer = true;  // restart until converged (impliciteuler.cpp:136-140), key 0
-            zres[i] = conv1 ? -z1 : e.z;  // where pass B's restart continues
-          }
+        }
+        if (conv) {
+          out[i] = max_dryradius(sqrt(e.z), msol[i]);
+          if (niters_out) niters_out[i] = ni | (failed ? CLEO_NITERS_FAILED : 0u);
+        } else {
+          defer = true;  // restart until converged (impliciteuler.cpp:136-140), key 0
+          // where pass B's restart continues; NaN after an abandoned seed (a full solve)
+          zres[i] = seeded ? __longlong_as_double(0x7FF8000000000000ll) : (conv1 ? -z1 : e.z);
         }
       } else {
         defer = true;
         key = deferred_key(dt, fmax(crit, c.p.cond_minsubdelt), true);
       }
-      if (defer && niters_out) niters_out[i] = failed ? CLEO_NITERS_FAILED : 0u;
+      if (defer && niters_out) niters_out[i] = carried | (failed ? CLEO_NITERS_FAILED : 0u);
     }
     const uint32_t pos = cs_warp_append(ctr, defer);
     if (defer) {
       lkeys[pos] = key;
       lvals[pos] = i;
-    }
-    if (defer_direct) {  // the key-0 rows that lead the sorted list: the surrogate's rows
-      const unsigned dm = __ballot_sync(0xFFFFFFFFu, defer && key == 0u);
-      if (dm && (threadIdx.x & 31) == (unsigned)(__ffs(dm) - 1)) atomicAdd(&ctr[1], __popc(dm));
     }
   }
 }
@@ -996,8 +987,7 @@ k_cs_b(const __grid_constant__ DevCtx c, const double* __restrict__ radius, cons
       if (code) w.fail(code);
       newr = sqrt(rsqrd);
     } else {
-      // seeds exist for the key-0 rows only (the direct solves pass A left to pass B)
-      const double seed = (seeds && lkeys[j] == 0u) ? seeds[i] : 0.0;
+      const double seed = seeds ? seeds[i] : 0.0;
       newr = solve_condensation(cfg, dt, c.p.cond_minsubdelt, s_ratio[i], akoh, bkoh, ffactor, r,
                                 seed, ni, w);
     }
@@ -1133,19 +1123,22 @@ int sort_incremental(cleo_b200_ctx* x) {
   const int pgrid = 148 * 8;  // CTAs over the touched pages (persistent loop)
   Fields& cur = x->buf[x->cur];
   Fields& other = x->buf[1 - x->cur];
-  k_mv_gather<<<gs, 256, 0, s>>>(d, cur, mvp, x->mv_count);
-  k_pg_touch<<<gs, 256, 0, s>>>(d, mk, mvp, x->mv_count);
+  // grid-stride kernels over the movers, whose count only the device knows: one wave of CTAs
+  const int mgrid = 148 * 8;
+  k_mv_gather<<<mgrid, 256, 0, s>>>(d, cur, mvp, x->mv_count);
+  k_pg_touch<<<mgrid, 256, 0, s>>>(d, mk, mvp, x->mv_count);
+  k_mv_runs<<<mgrid, 256, 0, s>>>(d, mk, x->mv_count);
   k_pg_plan<<<pgrid, 256, 0, s>>>(d, mk, mvp, x->mv_count);
-  k_grave_movers<<<gs, 256, 0, s>>>(d, x->mv_count);
+  k_grave_movers<<<mgrid, 256, 0, s>>>(d, x->mv_count);
   k_grave_movers_commit<<<1, 1, 0, s>>>(d, x->mv_count);
   k_pg_write<false><<<pgrid, 256, 0, s>>>(d, cur, mk, mvp, x->mv_count, d.pstart);
-  x->launches += 6;
+  x->launches += 7;
   // the repack path: its kernels return at once unless k_pg_plan chose it
   k_pg_sizes_repack<<<pgrid, 256, 0, s>>>(d, mk, mvp, x->mv_count, x->pstart_new);
   x->launches += 1;
   scan_u32(x, x->pstart_new, d.npages, x->ps_tsums);
   k_pg_write<true><<<pgrid, 256, 0, s>>>(d, other, mk, mvp, x->mv_count, x->pstart_new);
-  k_pg_copy_back<<<gs, 256, 0, s>>>(d, other, x->pstart_new);
+  k_pg_copy_back<<<mgrid, 256, 0, s>>>(d, other, x->pstart_new);
   k_pg_commit<<<grid_for((size_t)d.npages + 1, 256), 256, 0, s>>>(d, x->pstart_new);
   x->launches += 3;
   CUDA_TRY(cudaGetLastError());
@@ -1165,13 +1158,18 @@ int radix_pairs_on(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, u
   int cur = 0;
   uint32_t* K[2] = {k0, k1};
   uint32_t* V[2] = {v0, v1};
+  // counts up to one tile (the usual mover list) are sorted by one block; the multi-tile passes
+  // below then return at once, and the other way round
+  k_rs_small<<<1, RS_THREADS, 0, s>>>(k0, v0, k1, v1, n_ptr, bits);
+  x->launches += 1;
+  constexpr uint32_t SMALL = (uint32_t)RS_TILE;
   for (uint32_t shift = 0; shift < bits; shift += 8) {
-    k_rs_upsweep<<<nt, RS_THREADS, 0, s>>>(K[cur], n_ptr, (int)shift, hist, nt);
-    k_scan_tiles<<<nscan_tiles, SCAN_THREADS, 0, s>>>(hist, hist, nh, tile_sums);
-    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(tile_sums, nscan_tiles, nullptr);
-    k_scan_add<<<(unsigned)((nh + 255) / 256), 256, 0, s>>>(hist, nh, tile_sums);
+    k_rs_upsweep<<<nt, RS_THREADS, 0, s>>>(K[cur], n_ptr, (int)shift, hist, nt, SMALL);
+    k_scan_tiles<<<nscan_tiles, SCAN_THREADS, 0, s>>>(hist, hist, nh, tile_sums, n_ptr, SMALL);
+    k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(tile_sums, nscan_tiles, nullptr, n_ptr, SMALL);
+    k_scan_add<<<(unsigned)((nh + 255) / 256), 256, 0, s>>>(hist, nh, tile_sums, n_ptr, SMALL);
     k_rs_downsweep<<<nt, RS_THREADS, 0, s>>>(K[cur], V[cur], n_ptr, (int)shift, hist, nt,
-                                             K[1 - cur], V[1 - cur]);
+                                             K[1 - cur], V[1 - cur], SMALL);
     x->launches += 5;
     cur = 1 - cur;
   }
@@ -1193,10 +1191,16 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
   const int gg = grid_for(d.ngbxs, 256);
   // warps of 32 gridboxes each
   const int gw = grid_for(((size_t)d.ngbxs + 31) / 32 * 32, SEQ_THREADS);
-  if (did_motion) {  // qcond from the moved superdroplets
+  // qcond from the moved superdroplets: summed by the first condensation sub-step's commit when
+  // it starts the step (pass A stores each droplet's condensate mass before its solve), else here
+  const bool fuse_qcond = did_motion && on_step(d.p.condstep, t_sdm);
+  if (did_motion && !fuse_qcond) {
     k_b_qcond<<<gw, SEQ_THREADS, 0, s>>>(d);
     x->launches += 1;
   }
+  b.qm = nullptr;
+  BatchScratch bq = b;  // the first sub-step's scratch
+  bq.qm = fuse_qcond ? x->qm_buf : nullptr;
   k_b_reset<<<gg, 256, 0, s>>>(d, b, 1);
   x->launches += 1;
   uint32_t subt = t_sdm;
@@ -1205,14 +1209,15 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
     const bool coll = on_step(d.p.collstep, subt);
     if (cond) {
       StageMark mc(x, 3);
+      const BatchScratch& bc = subt == t_sdm ? bq : b;  // qcond with the first sub-step's commit
       k_b_thermo<<<gg, 256, 0, s>>>(d, b);
       x->launches += 1;
       if (x->cfg.cond_minb == 5)
-        k_cond_a<5><<<grid_for(d.slots, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
+        k_cond_a<5><<<grid_for(d.slots, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, bc);
       else if (x->cfg.cond_minb == 4)
-        k_cond_a<4><<<grid_for(d.slots, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
+        k_cond_a<4><<<grid_for(d.slots, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, bc);
       else
-        k_cond_a<3><<<grid_for(d.slots, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, b);
+        k_cond_a<3><<<grid_for(d.slots, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, bc);
       x->launches += 1;
       const int where = radix_pairs(x, b.lkeys, b.lvals, x->keys[1], x->vals[1], b.ctr, 16);
       if (where != 0) return CLEO_ERR_CUDA;  // 16 key bits: two passes, result back in place
@@ -1224,25 +1229,29 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
         const SdmListSeedIO io{d.sd.gbx, d.sd.r,  d.sd.msol, d.temp, d.press, b.th_s,
                                d.p.cond_delt, b.lvals, b.ctr + 9, b.dm};
         const uint32_t tiles = (d.slots + mlp::TILE_M - 1) / mlp::TILE_M;
-        mlp::k_mlp_tc<SdmListSeedIO><<<tiles < 148u * 4u ? tiles : 148u * 4u, 128, mlp::TC_SMEM,
+        mlp::k_mlp_tc<SdmListSeedIO><<<tiles < mlp::TC_GRID_MAX ? tiles : mlp::TC_GRID_MAX, 128, mlp::TC_SMEM,
                                        s>>>(w, io, d.slots);
         x->launches += 1;
       }
-      // pass B with the register budget of pass A's variant (grid: twice its resident CTAs)
-      if (x->cfg.cond_minb >= 5)
-        k_cond_b<5><<<x->grid_condb[2], 256, 0, s>>>(d, b);
-      else if (x->cfg.cond_minb == 4)
-        k_cond_b<4><<<x->grid_condb[1], 256, 0, s>>>(d, b);
-      else
-        k_cond_b<3><<<x->grid_condb[0], 256, 0, s>>>(d, b);
+      {  // pass B in its own tuned variant (grid: twice its resident CTAs)
+        StageMark mb(x, STAGE_COND_B);
+        if (x->cfg.condb_minb >= 5)
+          k_cond_b<5><<<x->grid_condb[2], 256, 0, s>>>(d, b);
+        else if (x->cfg.condb_minb == 4)
+          k_cond_b<4><<<x->grid_condb[1], 256, 0, s>>>(d, b);
+        else
+          k_cond_b<3><<<x->grid_condb[0], 256, 0, s>>>(d, b);
+      }
       // every gridbox's condensed mass summed in order, its state updated
-      k_b_commit<<<gw, SEQ_THREADS, 0, s>>>(d, b);
+      k_b_commit<<<gw, SEQ_THREADS, 0, s>>>(d, bc);
       x->launches += 2;
     }
     if (coll) {
       StageMark mk(x, 4);
       k_b_reset<<<1, 32, 0, s>>>(d, b, 0);
       k_b_classify<<<gg, 256, 0, s>>>(d, b);
+      k_b_tv<<<grid_for(d.slots, 256), 256, 0, s>>>(d, b);
+      x->launches += 1;
       // the warp kernel's 64-slot variant takes gridboxes up to 64 superdroplets, its 128-slot
       // variant those of 65 .. small_max (when small_max > 64)
       const int wide = x->cfg.small_max > SMALL_MAX ? 1 : 0, m3 = x->cfg.small_minb == 3 ? 1 : 0;
@@ -1338,9 +1347,10 @@ std::mutex g_tune_mutex;
 std::map<std::string, cleo_b200_ctx::TuneCfg> g_tune_cache;
 
 const cleo_b200_ctx::TuneCfg COND_OPTS[4] = {
-    {128, 4, 0, 0}, {256, 4, 0, 0}, {128, 5, 0, 0}, {256, 5, 0, 0}};
+    {128, 4, 0, 0, 3}, {256, 4, 0, 0, 4}, {128, 5, 0, 0, 5}, {256, 5, 0, 0, 3}};
 const cleo_b200_ctx::TuneCfg COLL_OPTS[4] = {
-    {0, 0, SMALL_MAX, 2}, {0, 0, WARP_MAX, 2}, {0, 0, SMALL_MAX, 3}, {0, 0, WARP_MAX, 3}};
+    {0, 0, SMALL_MAX, 2, 0}, {0, 0, WARP_MAX, 2, 0}, {0, 0, SMALL_MAX, 3, 0},
+    {0, 0, WARP_MAX, 3, 0}};
 
 std::string tune_key(const cleo_b200_ctx* x) {
   cudaDeviceProp prop;
@@ -1356,6 +1366,7 @@ int run_tuning_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
   const size_t k = x->tune_step % 4;
   x->cfg.cond_block = COND_OPTS[k].cond_block;
   x->cfg.cond_minb = COND_OPTS[k].cond_minb;
+  x->cfg.condb_minb = COND_OPTS[k].condb_minb;
   x->cfg.small_max = COLL_OPTS[k].small_max;
   x->cfg.small_minb = COLL_OPTS[k].small_minb;
   const bool prof = x->profiling;
@@ -1364,11 +1375,12 @@ int run_tuning_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
   const int rc = run_sdm_step(x, t_sdm, t_sdm_next);
   x->profiling = prof;
   CUDA_TRY(cudaStreamSynchronize(x->stream));
-  double tc = 0.0, tl = 0.0;
+  double tc = 0.0, tb = 0.0, tl = 0.0;
   for (size_t i = m0; i < x->marks.size(); ++i) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, x->marks[i].a, x->marks[i].b);
     if (x->marks[i].stage == 3) tc += ms;
+    if (x->marks[i].stage == STAGE_COND_B) tb += ms;
     if (x->marks[i].stage == 4) tl += ms;
     if (!prof) {
       x->event_pool.push_back(x->marks[i].a);
@@ -1377,16 +1389,18 @@ int run_tuning_step(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next) {
   }
   if (!prof) x->marks.resize(m0);
   if (rc != CLEO_OK) return rc;
-  x->t_cond[k] += tc;
+  x->t_cond[k] += tc - tb;  // pass A and the rest of the stage
+  x->t_condb[k] += tb;
   x->t_coll[k] += tl;
   if (++x->tune_step == x->tune_total) {
-    size_t bc = 0, bl = 0;
+    size_t bc = 0, bb = 0, bl = 0;
     for (size_t i = 1; i < 4; ++i) {
       if (x->t_cond[i] < x->t_cond[bc]) bc = i;
+      if (x->t_condb[i] < x->t_condb[bb]) bb = i;
       if (x->t_coll[i] < x->t_coll[bl]) bl = i;
     }
     x->cfg = {COND_OPTS[bc].cond_block, COND_OPTS[bc].cond_minb, COLL_OPTS[bl].small_max,
-              COLL_OPTS[bl].small_minb};
+              COLL_OPTS[bl].small_minb, COND_OPTS[bb].condb_minb};
     x->tune_total = 0;
     x->drop_graphs();
     std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -1504,6 +1518,9 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &d.pg_flag, d.npages);
   rc |= dalloc(x, &d.pg_list, d.npages);
   rc |= dalloc(x, &d.pg_ctr, 4);
+  rc |= dalloc(x, &d.mv_lo, d.ngbxs);
+  rc |= dalloc(x, &d.mv_hi, d.ngbxs);
+  rc |= dalloc(x, &d.mv_stamp, d.ngbxs);
   rc |= dalloc(x, &x->pstart_new, (size_t)d.npages + 1);
   rc |= dalloc(x, &x->ps_tsums, ((size_t)d.npages + SCAN_TILE) / SCAN_TILE + 1);
   rc |= dalloc(x, &d.gstart, ng + 2);
@@ -1533,10 +1550,13 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &x->bs.th_u3, ng);
   rc |= dalloc(x, &x->bs.dm, cap);
   rc |= dalloc(x, &x->bs.its, cap);
+  rc |= dalloc(x, &x->bs.tv, cap + 2);
+  rc |= dalloc(x, &x->qm_buf, cap);
   rc |= dalloc(x, &x->bs.zres, cap);
   rc |= dalloc(x, &x->bs.lkeys, cap);
   rc |= dalloc(x, &x->bs.lvals, cap);
   rc |= dalloc(x, &x->bs.bucket, 4 * ng);
+  rc |= dalloc(x, &x->bs.brec, 2 * ng);
   rc |= dalloc(x, &x->bs.slot, ng);
   rc |= dalloc(x, &x->bs.ctr, 12);
   rc |= dalloc(x, &x->bs.tsdm, 1);
@@ -1605,6 +1625,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   CUDA_TRY(cudaMemsetAsync(d.pstart, 0, ((size_t)d.npages + 1) * 4, x->stream));
   CUDA_TRY(cudaMemsetAsync(d.pg_flag, 0, (size_t)d.npages * 4, x->stream));
   CUDA_TRY(cudaMemsetAsync(d.pg_ctr, 0, 16, x->stream));
+  CUDA_TRY(cudaMemsetAsync(d.mv_stamp, 0, (size_t)d.ngbxs * 4, x->stream));
   CUDA_TRY(cudaMemsetAsync(d.err, 0, sizeof(DevError), x->stream));
   CUDA_TRY(cudaFuncSetAttribute(k_micro, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MICRO_SMEM));
   CUDA_TRY(cudaMemsetAsync(x->bs.ctr, 0, 48, x->stream));
@@ -1714,12 +1735,27 @@ int cleo_b200_stage_times(cleo_b200_ctx* x, double ms[5], uint64_t count[5]) {
   for (auto& m : x->marks) {
     float t = 0.f;
     CUDA_TRY(cudaEventElapsedTime(&t, m.a, m.b));
-    ms[m.stage] += t;
-    count[m.stage] += 1;
+    if (m.stage < 5) {  // the tuner's inner marks are not stages of their own
+      ms[m.stage] += t;
+      count[m.stage] += 1;
+    }
     x->event_pool.push_back(m.a);
     x->event_pool.push_back(m.b);
   }
   x->marks.clear();
+  return CLEO_OK;
+}
+
+int cleo_b200_resort_stats(cleo_b200_ctx* x, uint64_t out[4]) {
+  if (!x || !out) return CLEO_ERR_ARGUMENT;
+  CUDA_TRY(cudaStreamSynchronize(x->stream));
+  uint32_t pg[4] = {0, 0, 0, 0}, m = 0;
+  CUDA_TRY(cudaMemcpy(pg, x->d.pg_ctr, sizeof pg, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(&m, x->mv_count, sizeof m, cudaMemcpyDeviceToHost));
+  out[0] = m;
+  out[1] = pg[1] ? x->d.npages : pg[0];
+  out[2] = pg[1] ? 1u : 0u;
+  out[3] = x->d.npages;
   return CLEO_OK;
 }
 
@@ -1902,6 +1938,7 @@ int cleo_b200_autotune(cleo_b200_ctx* x, int reps) {
   x->tune_step = 0;
   x->tune_total = (size_t)4 * (size_t)reps;
   x->t_cond.assign(4, 0.0);
+  x->t_condb.assign(4, 0.0);
   x->t_coll.assign(4, 0.0);
   return CLEO_OK;
 }
@@ -1921,7 +1958,7 @@ int cleo_b200_set_launch_config(cleo_b200_ctx* x, const int32_t cfg[4]) {
       cfg[2] > (int32_t)WARP_MAX || (cfg[3] != 2 && cfg[3] != 3))
     return CLEO_ERR_ARGUMENT;
   CUDA_TRY(cudaStreamSynchronize(x->stream));
-  x->cfg = {cfg[0], cfg[1], (uint32_t)cfg[2], cfg[3]};
+  x->cfg = {cfg[0], cfg[1], (uint32_t)cfg[2], cfg[3], 3};  // pass B at its unspilled budget
   x->tune_total = 0;  // ends a tuning run in progress
   x->tune_step = 0;
   x->drop_graphs();
@@ -2202,9 +2239,12 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_rad
     w.err = reinterpret_cast<uint32_t*>(&x->d.err->code);
   }
   const uint32_t tiles = (uint32_t)((n + mlp::TILE_M - 1) / mlp::TILE_M);
-  const uint32_t tc_grid = tiles < 148u * 4u ? tiles : 148u * 4u;
+  const uint32_t tc_grid = tiles < mlp::TC_GRID_MAX ? tiles : mlp::TC_GRID_MAX;
   const double* seeds = seeded ? x->seed_buf : nullptr;
-  if (seeded && !batched) {  // the plain form seeds every solve up front
+  // every solve seeded up front: most direct solves of independent droplets need more than the
+  // two iterations of pass A, so the seed saves them (the batched SDM step instead seeds only the
+  // solves that two iterations did not settle)
+  if (seeded) {
     const CondSeedIO io{d_radius, d_msol, d_temp, d_press, d_s_ratio, d_delt, x->seed_buf};
     mlp::k_mlp_tc<CondSeedIO><<<tc_grid, 128, mlp::TC_SMEM, x->stream>>>(w, io, (uint32_t)n);
     x->launches += 1;
@@ -2230,7 +2270,7 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_rad
       ok = ok && cudaMalloc(q, n * sizeof(uint32_t)) == cudaSuccess;
     ok = ok && cudaMalloc(&cs.hist, nh * sizeof(uint32_t)) == cudaSuccess;
     ok = ok && cudaMalloc(&cs.tsums, nsums * sizeof(uint32_t)) == cudaSuccess;
-    ok = ok && cudaMalloc(&cs.ctr, 2 * sizeof(uint32_t)) == cudaSuccess;
+    ok = ok && cudaMalloc(&cs.ctr, sizeof(uint32_t)) == cudaSuccess;
     ok = ok && cudaMalloc(&cs.zres, n * sizeof(double)) == cudaSuccess;
     if (!ok) {
       x->free_cs();
@@ -2240,21 +2280,14 @@ int cleo_b200_condensation_solve(cleo_b200_ctx* x, size_t n, const double* d_rad
     cs.cap = n;
     cs.nt = nt;
   }
-  // ctr[0]: listed solves, ctr[1]: the direct ones among them (with the surrogate)
-  CUDA_TRY(cudaMemsetAsync(cs.ctr, 0, 2 * sizeof(uint32_t), x->stream));
+  CUDA_TRY(cudaMemsetAsync(cs.ctr, 0, sizeof(uint32_t), x->stream));
   k_cs_a<<<grid_for(n, 256), 256, 0, x->stream>>>(
-      x->d, (uint32_t)n, d_radius, d_msol, d_temp, d_press, d_s_ratio, d_delt, seeded,
-      d_radius_out, d_niters_out, cs.zres, cs.k0, cs.v0, cs.ctr);
+      x->d, (uint32_t)n, d_radius, d_msol, d_temp, d_press, d_s_ratio, d_delt,
+      seeded ? x->seed_buf : nullptr, d_radius_out, d_niters_out, cs.zres, cs.k0, cs.v0, cs.ctr);
   x->launches += 1;
   const int where = radix_pairs_on(x, cs.k0, cs.v0, cs.k1, cs.v1, cs.ctr, 16, cs.hist, cs.tsums,
                                    cs.nt);
   if (where != 0) return CLEO_ERR_CUDA;  // two 8-bit passes leave the result in (k0, v0)
-  if (seeded) {  // seeds for the direct solves, which lead the sorted list
-    const CondListSeedIO io{d_radius, d_msol, d_temp,  d_press,    d_s_ratio,
-                            d_delt,   cs.v0,  cs.ctr + 1, x->seed_buf};
-    mlp::k_mlp_tc<CondListSeedIO><<<tc_grid, 128, mlp::TC_SMEM, x->stream>>>(w, io, (uint32_t)n);
-    x->launches += 1;
-  }
   k_cs_b<<<x->grid_flat * 2, 256, 0, x->stream>>>(x->d, d_radius, d_msol, d_temp, d_press,
                                                   d_s_ratio, d_delt, seeds, d_radius_out,
                                                   d_niters_out, cs.zres, cs.k0, cs.v0, cs.ctr);

@@ -278,6 +278,12 @@ void* cleo_b200_stream(cleo_b200_ctx* ctx);
 /* Number of kernels the context has launched since it was created (for launch accounting). */
 int cleo_b200_kernel_launches(cleo_b200_ctx* ctx, uint64_t* n);
 
+/* What the last re-sort after motion did (synchronises the context's stream): out[0] superdroplets
+ * that moved (changed gridbox, left the domain, or were made null by collisions), out[1] pages
+ * rewritten, out[2] 1 if every page was repacked, out[3] pages in the store (a page holds 64
+ * gridboxes). No reference counterpart: a measurement of the paged store. */
+int cleo_b200_resort_stats(cleo_b200_ctx* ctx, uint64_t out[4]);
+
 /*
  * Per-stage device timing with CUDA events on the context's stream, the counterpart of the
  * reference's Kokkos profiling regions (sdm_movement_*, timestep_sdm_microphysics;
