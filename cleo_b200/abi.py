@@ -52,6 +52,7 @@ EXEC_PLAIN, EXEC_BATCHED = 0, 1
 MLP_TCGEN05, MLP_MMA_SYNC, MLP_FP32 = 0, 1, 2
 MONITOR_MASSMOMENTS, MONITOR_RAINMASSMOMENTS, MONITOR_PRECIPITATION = 1, 2, 4
 NITERS_FAILED = 0x80000000  # or-ed into a batch solve's iteration count: that droplet aborted
+RESORT_AUTO, RESORT_PAGES, RESORT_FULL = 0, 1, 2
 MLP_NFEATURES, MLP_NHIDDEN, MLP_NPARAMS, MLP_NNORM = 7, 64, 4737, 16
 # enum cleo_obs_var: superdroplet output variables, with their output types
 OBS_VARS = {"sdId": (1, np.uint32), "sdgbxindex": (2, np.uint32), "xi": (4, np.uint64),
@@ -286,6 +287,7 @@ EXPORTED = (
     "cleo_b200_download_supers",
     "cleo_b200_download_state", "cleo_b200_download_budgets", "cleo_b200_condensation_solve",
     "cleo_b200_stream", "cleo_b200_kernel_launches", "cleo_b200_resort_stats",
+    "cleo_b200_set_resort_policy",
     "cleo_b200_set_profiling",
     "cleo_b200_stage_times", "cleo_b200_sort_by_gridbox_static", "cleo_b200_version",
     "cleo_b200_mlp_create", "cleo_b200_mlp_destroy", "cleo_b200_mlp_set_params",
@@ -326,6 +328,8 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
     lib.cleo_b200_kernel_launches.restype = C.c_int
     lib.cleo_b200_resort_stats.argtypes = [vp, C.POINTER(C.c_uint64)]
     lib.cleo_b200_resort_stats.restype = C.c_int
+    lib.cleo_b200_set_resort_policy.argtypes = [vp, C.c_int]
+    lib.cleo_b200_set_resort_policy.restype = C.c_int
     lib.cleo_b200_set_profiling.argtypes = [vp, C.c_int]
     lib.cleo_b200_set_profiling.restype = C.c_int
     lib.cleo_b200_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]

@@ -686,7 +686,10 @@ k_b_small(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch
 // each thread then walks the chains of its positions (about ln n lookups each). P receives the
 // origins, as fy_origin computes them. Ends with a barrier.
 constexpr uint32_t CHAIN_MAX = 16384;  // keys of up to 16384 swaps: 64 KB of shared memory
-constexpr uint32_t LARGE_SMEM = CHAIN_MAX * 4;
+// the keys, FIRST and NEXT of up to CHAIN_MAX swaps in shared memory (192 KB): the chain walks'
+// dependent lookups stay on chip
+constexpr uint32_t LARGE_SMEM = CHAIN_MAX * 4 * 3;
+constexpr uint32_t LARGE_THREADS = 1024;  // a gridbox of thousands: four times B_THREADS
 __device__ void cta_fy_origins(const uint32_t* J, uint32_t n, uint32_t* keys, uint32_t* FIRST,
                                uint32_t* NEXT, uint32_t* P) {
   constexpr uint32_t NONE = 0xFFFFFFFFu;
@@ -732,9 +735,9 @@ __device__ void cta_fy_origins(const uint32_t* J, uint32_t n, uint32_t* keys, ui
 
 // ---- medium and large gridboxes: one CTA per gridbox ----
 // medium: staged in shared memory with the non-staged fields permuted through registers;
-// large: staged in global scratch arrays, the shuffle's chain keys in LARGE_SMEM of shared memory.
+// large: staged in global scratch arrays, the shuffle's chain tables in LARGE_SMEM of shared memory.
 template <bool LARGE>
-__global__ void __launch_bounds__(B_THREADS)
+__global__ void __launch_bounds__(LARGE ? LARGE_THREADS : B_THREADS)
 k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b) {
   const uint32_t t_sdm = *b.tsdm;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -742,6 +745,7 @@ k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b
   __shared__ uint32_t s_item;
   __shared__ uint64_t s_bar;  // completion of the medium path's bulk copies
   constexpr uint32_t PT = MEDIUM_MAX / B_THREADS;  // superdroplets per thread (medium)
+  constexpr uint32_t NT = LARGE ? LARGE_THREADS : B_THREADS;  // threads of the block
   constexpr uint32_t MBUF = MEDIUM_MAX + 2;        // staged elements per field (medium)
   const cleo_b200_params& p = c.p;
   const int tid = threadIdx.x;
@@ -797,7 +801,7 @@ k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b
       }
       bar_parity ^= 1u;
     }
-    for (uint32_t k = tid; k < n; k += B_THREADS) {
+    for (uint32_t k = tid; k < n; k += NT) {
       if (LARGE) {
         Sr[k] = c.sd.r[base + k];
         Sm[k] = c.sd.msol[base + k];
@@ -809,13 +813,13 @@ k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b
     }
     __syncthreads();
     if (n <= FY_PARALLEL_MAX) {  // every thread traces its own positions
-      for (uint32_t k = tid; k < n; k += B_THREADS) P[k] = fy_origin(J, n, k);
+      for (uint32_t k = tid; k < n; k += NT) P[k] = fy_origin(J, n, k);
     } else if (LARGE && n <= CHAIN_MAX) {  // chains, as in the warp kernel (keys in smem)
       cta_fy_origins(J, n, reinterpret_cast<uint32_t*>(smem),
-                     reinterpret_cast<uint32_t*>(c.scr_c3 + base),
-                     reinterpret_cast<uint32_t*>(c.scr_c1 + base), P);
+                     reinterpret_cast<uint32_t*>(smem) + CHAIN_MAX,
+                     reinterpret_cast<uint32_t*>(smem) + 2 * CHAIN_MAX, P);
     } else {
-      for (uint32_t k = tid; k < n; k += B_THREADS) P[k] = k;
+      for (uint32_t k = tid; k < n; k += NT) P[k] = k;
       __syncthreads();
       if (tid == 0) {
         for (uint32_t it = n > 0 ? n - 1 : 0; it > 0; --it) {
@@ -832,7 +836,7 @@ k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b
     const double scale_p = (double)n * ((double)n - 1.0) / (2.0 * (double)npairs);
     const double VOLUME = c.volume[g] * VOL0;
     uint32_t nnull = 0;
-    for (uint32_t jj = tid; jj < npairs; jj += B_THREADS) {
+    for (uint32_t jj = tid; jj < npairs; jj += NT) {
       const uint32_t a = P[2 * jj], bb = P[2 * jj + 1];
       const Where w{c.err, g, (uint64_t)base + 2 * jj};
       const double tvA = LARGE ? pair_tv(p, Sr[a]) : Stv[a];
@@ -844,7 +848,7 @@ k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b
     const uint32_t nvalid = n - totnull;
     uint32_t cval = 0, cnull = 0;
     // destination of shuffled position k; J becomes the inverse map q -> source
-    for (uint32_t k0 = 0; k0 < n; k0 += B_THREADS) {
+    for (uint32_t k0 = 0; k0 < n; k0 += NT) {
       const uint32_t k = k0 + tid;
       const bool act = k < n;
       const uint32_t src = act ? P[k] : 0;
@@ -858,7 +862,7 @@ k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b
     }
     __syncthreads();
     if (LARGE) {
-      for (uint32_t q = tid; q < n; q += B_THREADS) {
+      for (uint32_t q = tid; q < n; q += NT) {
         const uint32_t s = base + J[q], o = base + q;
         c.scr_c3[o] = c.sd.c3[s];
         c.scr_c1[o] = c.sd.c1[s];
@@ -866,7 +870,7 @@ k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b
         c.scr_id[o] = c.sd.id[s];
       }
       __syncthreads();
-      for (uint32_t q = tid; q < n; q += B_THREADS) {
+      for (uint32_t q = tid; q < n; q += NT) {
         const uint32_t o = base + q;
         const uint32_t src = J[q];
         c.sd.r[o] = Sr[src];

@@ -211,6 +211,10 @@ CLEO_MATH_HD double bitsd(uint64_t b) {
 #endif
 }
 
+// 2^k for -1022 <= k <= 1023, exactly: multiplying by it is ldexp(x, k) wherever the product is
+// a normal double (both are the one correctly rounded value of x 2^k)
+CLEO_MATH_HD double pow2i(int k) { return bitsd((uint64_t)(k + 1023) << 52); }
+
 // ln x for positive normal finite x, relative error below 2^-70 (absolute below 2^-79 plus
 // 2^-100 |exponent|): x = 2^e m, m in [sqrt(1/2), sqrt(2)); rc ~ 1/c for the nearest centre
 // c = i/512, r = m rc - 1 exactly (|r| < 2^-9.4); ln m = -ln(rc) + log1p(r), the series
@@ -221,8 +225,10 @@ CLEO_MATH_HD dd fast_log(double x) {
 #else
   using namespace cleo_dd_host;
 #endif
-  int e = 0;
-  double m = std::frexp(x, &e);
+  // x = m 2^e, m in [0.5, 1) (frexp's split, read off the bits of the normal x)
+  const uint64_t xb = dbits(x);
+  int e = (int)((xb >> 52) & 0x7FF) - 1022;
+  double m = bitsd((xb & 0x000FFFFFFFFFFFFFull) | 0x3FE0000000000000ull);
   if (m < 0.70710678118654752440) {
     m *= 2.0;
     e -= 1;
@@ -234,10 +240,13 @@ CLEO_MATH_HD dd fast_log(double x) {
   const double rh = r.hi, rl = r.lo;
   const dd sq = two_prod(rh, rh);
   const dd s = two_sum(rh, -0.5 * sq.hi);
-  const double q =
-      CLEO_DD_THIRD_HI +
-      rh * (-0.25 + rh * (CLEO_DD_FIFTH_HI + rh * (-CLEO_DD_INV6_HI +
-                                                   rh * (CLEO_DD_SEVENTH_HI + rh * -0.125))));
+  // Horner's scheme with fused multiply-adds (each step rounds once, so no less accurately than
+  // the separate product and sum)
+  double q = dd_fma(rh, -0.125, CLEO_DD_SEVENTH_HI);
+  q = dd_fma(rh, q, -CLEO_DD_INV6_HI);
+  q = dd_fma(rh, q, CLEO_DD_FIFTH_HI);
+  q = dd_fma(rh, q, -0.25);
+  q = dd_fma(rh, q, CLEO_DD_THIRD_HI);
   // r^2/2 = rh^2/2 + rh rl + rl^2/2 (the last below 2^-115 |r|); r^3 q rounded: below 2^-72 |r|
   const double low = rl - 0.5 * sq.lo - rh * rl + (rh * sq.hi) * q;
   const dd l1p = fast_two_sum(s.hi, s.lo + low);
@@ -262,13 +271,17 @@ CLEO_MATH_HD dd fast_exp(dd a) {
   dd r = dd_add(a, dd{-p.hi, -p.lo});
   r = dd_add_d(r, -nf * (CLEO_DD_LN2_LO * 0x1p-9));
   const double rh = r.hi, rl = r.lo;
-  const double poly =
-      rh * rh * (0.5 + rh * (CLEO_DD_INV6_HI + rh * (CLEO_DD_INV24_HI + rh * CLEO_DD_INV120_HI)));
+  double c = dd_fma(rh, CLEO_DD_INV120_HI, CLEO_DD_INV24_HI);  // Horner with fused steps
+  c = dd_fma(rh, c, CLEO_DD_INV6_HI);
+  c = dd_fma(rh, c, 0.5);
+  const double poly = rh * rh * c;
   const dd em1 = fast_two_sum(rh, rl + rh * rl + poly);
   const dd tj{cleo_fast_exp2_tab[j][0], cleo_fast_exp2_tab[j][1]};
   dd v = dd_add(tj, dd_mul(tj, em1));
-  v.hi = std::ldexp(v.hi, k);
-  v.lo = std::ldexp(v.lo, k);
+  // |k| <= 866 and v.hi near [1, 2]: both products are normal, so exact (ldexp's values)
+  const double sk = pow2i(k);
+  v.hi *= sk;
+  v.lo *= sk;
   return v;
 }
 

@@ -1,22 +1,23 @@
 // sdm.cu — the B200 SDM step behind the C ABI of include/cleo_b200.h.
 //
 // Device layout: structure-of-arrays superdroplets (sdgbxindex u32, coord3/1/2 f64, xi u64,
-// radius f64, msol f64, sdid u64), double-buffered for the sort, with the in-domain superdroplets
-// sorted by gridbox in [0, nrange); per gridbox g the superdroplets [gstart[g], gstart[g] +
-// gcount[g]) are the ones SupersInGbx refs would select. Superdroplets that leave the domain or
-// become null are appended to a separate out-of-domain store (the reference keeps them at the tail
-// of its array in unspecified order). Null superdroplets made by collisions stay in their
-// gridbox's range, after the gcount valid ones, until the next sort (the reference re-sorts at
-// once, sdmmethods.hpp:221-229; both give the same in-domain superdroplets in the same order).
+// radius f64, msol f64, sdid u64) in the paged store of pages.cuh: pages of 64 gridboxes, each
+// page's gridboxes in index order with free slots between and after them; per gridbox g the
+// superdroplets [gstart[g], gstart[g] + gcount[g]) are the ones SupersInGbx refs would select.
+// Superdroplets that leave the domain or become null are appended to a separate out-of-domain
+// store (the reference keeps them at the tail of its array in unspecified order). Null
+// superdroplets made by collisions stay after the gcount valid ones of their gridbox until the
+// next re-sort (the reference re-sorts at once, sdmmethods.hpp:221-229; both give the same
+// in-domain superdroplets in the same order).
 //
 // One SDM step (SDMMethods::run_step, sdmmethods.hpp:319-332):
-//   motion  -> k_motion: predictor-corrector coords + new gridbox index + sort key per droplet,
-//              and (for the incremental re-sort) the flags and per-gridbox counts of the movers
-//   sort    -> chosen per step from the previous motion step's mover count: incremental (scan of
-//              the mover flags, radix sort of the movers only, one copy of every droplet to its
-//              place: k_mv_*) while at most a fifth of the droplets moved, else the full sort
-//              (radix passes over (key, position), gather of all fields, gridbox refs by binary
-//              search); then the append of out-of-domain droplets to the store
+//   motion  -> k_motion: predictor-corrector coords + new gridbox index per droplet, and either
+//              the movers of every 32 slots as a mask (the page re-sort) or the sort keys
+//   sort    -> chosen per step from the previous motion step's mover count: the page re-sort
+//              (the movers listed and radix-sorted alone, the gridboxes they leave or enter
+//              rewritten in place, pages.cuh) while at most a fifth of the droplets moved, else
+//              the full sort (radix passes over (key, position), every page written packed); then
+//              the append of out-of-domain droplets to the store
 //   microphysics -> plain schedule: k_micro, one CTA per gridbox: qcond from the moved droplets,
 //              condensation (FP64 Newton) and collisions (shared-memory shuffle, parallel pairs,
 //              null removal) for every sub-step of the SDM step; batched schedule: the kernels of
@@ -81,8 +82,9 @@ struct DevCtx {
   double *precip, *precip_c, *gbxarea;  // per gridbox, per superdroplet, per gridbox
   // re-sort after motion (pages.cuh): mover flags then their exclusive scan (slots + 1); a full
   // sort's per-key first sorted positions (ngbxs + 2)
-  uint32_t *mv_scan, *gstart_new;
-  uint32_t* mv_tsums;  // the flag scan's tile offsets (the scan's readers add them: mv_before)
+  uint32_t *mv_scan, *gstart_new;  // mv_scan: movers per 32 slots, scanned (exclusive)
+  uint32_t* mv_mask;   // the movers among each 32 slots, a bit each (k_motion)
+  uint32_t* mv_tsums;  // the count scan's tile offsets (the scan's readers add them: mv_before)
   uint32_t* mv_total;  // valid superdroplets that changed gridbox in the last motion step
   // paged layout (pages.cuh): pages of PAGE_GBXS gridboxes, their slot starts (npages + 1), the
   // touched-page flags and list, the re-sort's counters, the movers' records; slots = the SoA
@@ -135,6 +137,9 @@ struct cleo_b200_ctx {
   cudaEvent_t ev_report = nullptr;
   bool report_recorded = false;
   bool sort_full = false;
+  bool last_sort_full = false;  // what the last re-sort after motion was (cleo_b200_resort_stats)
+  int resort_policy = CLEO_RESORT_AUTO;
+  int sms = 148;                // the device's SMs
   // asynchronous state upload (cleo_b200_upload_state_async): staging area for the 11 state
   // fields, a copy stream, and events for "copied" and "taken by a step"
   double* stage_state = nullptr;
@@ -319,23 +324,22 @@ __device__ __forceinline__ bool beyond_domainboundary(uint32_t gbxindex, uint32_
 // and CartesianCheckBounds. For the full re-sort it writes each slot's sort key (its new
 // gridbox, ngbxs out of the domain, ngbxs + 1 for a free slot) and position; for the page re-sort
 // it flags the movers (pages.cuh).
-__global__ void __launch_bounds__(256, 4)  // 64 registers: measured 15% faster than 80
-k_motion(const __grid_constant__ DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, int incremental) {
-  const uint32_t n = c.counters[0];
+// One superdroplet's motion (movesupersindomain.hpp:255-261: the predictor-corrector step, the
+// neighbour search, the bounds check); returns whether it moves in the re-sort (changes gridbox,
+// leaves the domain, or is a null one collisions left). For the full sort it writes the sort key
+// (gridbox, ngbxs out of the domain, ngbxs + 1 for a free slot) and position.
+__device__ __forceinline__ bool move_superdroplet(const DevCtx& c, uint32_t i,
+                                                  uint32_t* __restrict__ keys,
+                                                  uint32_t* __restrict__ vals, int incremental) {
   const uint32_t ng = c.ngbxs;
   const double delt = c.p.motion_delt;
-  if (incremental && blockIdx.x == 0 && threadIdx.x == 0) c.mv_scan[n] = 0;  // scan total
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t g = c.sd.gbx[i];
-    if (!incremental) vals[i] = i;
-    if (g >= ng) {  // a null superdroplet left by collisions (out of the domain), or a free slot
-      const bool hole = is_hole(c.sd, i);
-      if (incremental)
-        c.mv_scan[i] = hole ? 0u : 1u;  // a null one moves to the out-of-domain store
-      else
-        keys[i] = hole ? ng + 1 : ng;
-      continue;
-    }
+  const uint32_t g = c.sd.gbx[i];
+  if (!incremental) vals[i] = i;
+  if (g >= ng) {  // a null superdroplet left by collisions (out of the domain), or a free slot
+    const bool hole = is_hole(c.sd, i);
+    if (!incremental) keys[i] = hole ? ng + 1 : ng;
+    return !hole;  // a null one moves to the out-of-domain store
+  }
     const Where w{c.err, g, i};
     double bzl, bzh, bxl, bxh, byl, byh;
     bounds_of(c.b3lo, c.b3hi, ng, g, bzl, bzh);
@@ -457,8 +461,25 @@ k_motion(const __grid_constant__ DevCtx c, uint32_t* __restrict__ keys, uint32_t
       const unsigned bm = __ballot_sync(am, mover);
       if (bm && (int)(threadIdx.x & 31) == __ffs(am) - 1) atomicAdd(c.mv_total, __popc(bm));
     }
-    if (!incremental) continue;
-    c.mv_scan[i] = mover ? 1u : 0u;
+    return mover;
+}
+__global__ void __launch_bounds__(256, 4)  // 64 registers: measured 15% faster than 80
+k_motion(const __grid_constant__ DevCtx c, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, int incremental) {
+  const uint32_t n = c.counters[0];
+  const uint32_t nchunks = (n + 31) / 32;
+  if (incremental && blockIdx.x == 0 && threadIdx.x == 0) c.mv_scan[nchunks] = 0;  // scan total
+  // i0 is the same for the whole block, so every warp's lanes cover 32 consecutive slots together
+  for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+    const uint32_t i = i0 + threadIdx.x;
+    bool mover = false;
+    if (i < n) mover = move_superdroplet(c, i, keys, vals, incremental);
+    if (incremental) {  // the movers of the warp's 32 slots: a mask and its count
+      const unsigned bm = __ballot_sync(0xFFFFFFFFu, mover);
+      if ((threadIdx.x & 31) == 0 && i < n) {
+        c.mv_mask[i >> 5] = bm;
+        c.mv_scan[i >> 5] = __popc(bm);
+      }
+    }
   }
 }
 __global__ void k_mv_report(const __grid_constant__ DevCtx c, uint32_t* __restrict__ out) {  // mapped host memory
@@ -467,25 +488,33 @@ __global__ void k_mv_report(const __grid_constant__ DevCtx c, uint32_t* __restri
 }
 
 // ---- the movers of a page re-sort (pages.cuh), listed in position order ----
-// the exclusive scan of the mover flags at position i: the scan within its tile plus the tile's
-// offset (the scan's own pass adding the offsets in place is left out; its readers add them)
-__device__ __forceinline__ uint32_t mv_before(const DevCtx& c, uint32_t i) {
-  return c.mv_scan[i] + c.mv_tsums[i / SCAN_TILE];
+// the exclusive scan of the per-32-slot mover counts at chunk w: the scan within its tile plus
+// the tile's offset (the scan's own pass adding the offsets in place is left out; its readers add
+// them)
+__device__ __forceinline__ uint32_t mv_before(const DevCtx& c, uint32_t w) {
+  return c.mv_scan[w] + c.mv_tsums[w / SCAN_TILE];
 }
-// the movers' keys: min(gbx, ngbxs) of the gridbox indices k_motion wrote
+// the movers, from the masks of the chunks that hold any: positions and keys (min(gbx, ngbxs) of
+// the gridbox indices k_motion wrote)
 __global__ void k_mv_list(const __grid_constant__ DevCtx c, uint32_t* __restrict__ mk, uint32_t* __restrict__ mvp) {
-  const uint32_t n = c.counters[0];
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t p = mv_before(c, i);
-    if (mv_before(c, i + 1) != p) {  // a mover: the exclusive scan steps over it
+  const uint32_t nchunks = (c.counters[0] + 31) / 32;
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < nchunks;
+       w += gridDim.x * blockDim.x) {
+    uint32_t m = c.mv_mask[w];
+    if (m == 0u) continue;
+    uint32_t p = mv_before(c, w);
+    while (m) {
+      const uint32_t i = w * 32 + (uint32_t)(__ffs(m) - 1);
+      m &= m - 1u;
       const uint32_t gbx = c.sd.gbx[i];
       mk[p] = gbx < c.ngbxs ? gbx : c.ngbxs;
       mvp[p] = i;
+      ++p;
     }
   }
 }
 __global__ void k_mv_count(const __grid_constant__ DevCtx c, uint32_t* __restrict__ count) {
-  *count = mv_before(c, c.counters[0]);  // number of movers
+  *count = mv_before(c, (c.counters[0] + 31) / 32);  // number of movers
 }
 // ---- superdroplet output: the domain superdroplets, gathered in gridbox order and converted
 // the way the reference's Collect* functors convert them (superdrops_observer.hpp:139-464) ----
@@ -1095,24 +1124,25 @@ int radix_pairs_on(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, u
                    const uint32_t* n_ptr, uint32_t bits, uint32_t* hist, uint32_t* tile_sums,
                    uint32_t nt);
 
-// The page re-sort after motion (pages.cuh; k_motion flagged the movers): scan of the flags, the
-// movers listed in position order and stably radix-sorted by key, copied out to the mover
+// The page re-sort after motion (pages.cuh; k_motion left a mover mask per 32 slots): scan of the
+// masks' counts, the movers listed in position order and stably radix-sorted by key, copied out
+// to the mover
 // buffer; the touched pages rewritten in place, or, when one would outgrow its slots, every page
 // rewritten into the other buffer and copied back (the device decides; both paths are launched);
 // movers out of the domain appended to their store. The current buffer stays current.
 int sort_incremental(cleo_b200_ctx* x) {
   DevCtx& d = x->d;
   cudaStream_t s = x->stream;
-  const uint64_t n1 = (uint64_t)d.slots + 1;
+  // exclusive scan of the per-32-slot mover counts, chunks + 1 of them for the slots' capacity
+  // (entries past the slots in use are stale but only move the values after them, which nothing
+  // reads) (readers add the tile offsets: mv_before)
+  const uint64_t n1 = ((uint64_t)d.slots + 31) / 32 + 1;
   const uint32_t nscan = (uint32_t)((n1 + SCAN_TILE - 1) / SCAN_TILE);
   k_pg_reset<<<1, 1, 0, s>>>(d);
-  // exclusive scan of slots + 1 flags (entries past nrange are stale but only move the values
-  // after index nrange, which nothing reads) (readers add the tile offsets: mv_before)
   k_scan_tiles<<<nscan, SCAN_THREADS, 0, s>>>(d.mv_scan, d.mv_scan, n1, d.mv_tsums);
   k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(d.mv_tsums, nscan, nullptr);
   x->launches += 3;
-  const int gs = grid_for(d.slots, 256);
-  k_mv_list<<<gs, 256, 0, s>>>(d, x->keys[1], x->vals[1]);
+  k_mv_list<<<grid_for(n1, 256), 256, 0, s>>>(d, x->keys[1], x->vals[1]);
   k_mv_count<<<1, 1, 0, s>>>(d, x->mv_count);
   x->launches += 2;
   // the movers stably by key (the mover count is read by the radix kernels on the device)
@@ -1265,7 +1295,7 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       if (wide) k_b_small<2, WARP_MAX><<<x->grid_wide, B_THREADS, SW, s>>>(d, b, 1);
       x->launches += wide;
       k_b_cta<false><<<x->grid_medium, B_THREADS, (size_t)MEDIUM_SMEM, s>>>(d, b);
-      k_b_cta<true><<<x->grid_large, B_THREADS, LARGE_SMEM, s>>>(d, b);
+      k_b_cta<true><<<x->grid_large, LARGE_THREADS, LARGE_SMEM, s>>>(d, b);
       x->launches += 5;
     }
     subt = min(next_step(d.p.condstep, subt), next_step(d.p.collstep, subt));
@@ -1561,7 +1591,8 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &x->bs.ctr, 12);
   rc |= dalloc(x, &x->bs.tsdm, 1);
   rc |= dalloc(x, &x->tile_sums, ((size_t)256 * x->ntiles_max + SCAN_TILE - 1) / SCAN_TILE + 1);
-  rc |= dalloc(x, &d.mv_scan, (size_t)cap + 1);
+  rc |= dalloc(x, &d.mv_scan, ((size_t)cap + 31) / 32 + 1);
+  rc |= dalloc(x, &d.mv_mask, ((size_t)cap + 31) / 32);
   rc |= dalloc(x, &d.mv_total, 1);
   if (cudaHostAlloc(&x->h_motion, 2 * sizeof(uint32_t), cudaHostAllocMapped) != cudaSuccess ||
       cudaHostGetDevicePointer(&x->d_motion, x->h_motion, 0) != cudaSuccess ||
@@ -1649,6 +1680,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
     int dev = 0, sms = 148, occ = 1;
     CUDA_TRY(cudaGetDevice(&dev));
     CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    x->sms = sms;
     constexpr int SW = (int)SmallLayout<WARP_MAX>::BYTES, SS = (int)SmallLayout<SMALL_MAX>::BYTES;
     CUDA_TRY(cudaFuncSetAttribute(k_b_small<2, SMALL_MAX>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, SS));
@@ -1670,7 +1702,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
     x->grid_medium = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaFuncSetAttribute(k_b_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)LARGE_SMEM));
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<true>, B_THREADS,
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<true>, LARGE_THREADS,
                                                            LARGE_SMEM));
     x->grid_large = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cond_b<3>, 256, 0));
@@ -1746,15 +1778,27 @@ int cleo_b200_stage_times(cleo_b200_ctx* x, double ms[5], uint64_t count[5]) {
   return CLEO_OK;
 }
 
+int cleo_b200_set_resort_policy(cleo_b200_ctx* x, int policy) {
+  if (!x || policy < CLEO_RESORT_AUTO || policy > CLEO_RESORT_FULL) return CLEO_ERR_ARGUMENT;
+  x->resort_policy = policy;
+  return CLEO_OK;
+}
+
 int cleo_b200_resort_stats(cleo_b200_ctx* x, uint64_t out[4]) {
   if (!x || !out) return CLEO_ERR_ARGUMENT;
   CUDA_TRY(cudaStreamSynchronize(x->stream));
   uint32_t pg[4] = {0, 0, 0, 0}, m = 0;
   CUDA_TRY(cudaMemcpy(pg, x->d.pg_ctr, sizeof pg, cudaMemcpyDeviceToHost));
   CUDA_TRY(cudaMemcpy(&m, x->mv_count, sizeof m, cudaMemcpyDeviceToHost));
-  out[0] = m;
-  out[1] = pg[1] ? x->d.npages : pg[0];
-  out[2] = pg[1] ? 1u : 0u;
+  if (x->last_sort_full) {  // every slot sorted, every page written
+    out[0] = x->h_motion[0];
+    out[1] = x->d.npages;
+    out[2] = 2;
+  } else {
+    out[0] = m;
+    out[1] = pg[1] ? x->d.npages : pg[0];
+    out[2] = pg[1] ? 1u : 0u;
+  }
   out[3] = x->d.npages;
   return CLEO_OK;
 }
@@ -1904,11 +1948,16 @@ int cleo_b200_step(cleo_b200_ctx* x, uint32_t t_mdl, uint32_t t_next) {
     const uint32_t t_sdm_next = t_next < next_move ? t_next : next_move;
     {  // full re-sort when more than a fifth of the superdroplets changed gridbox in the
        // previous motion step (whose report the event marks; it completes early in that step,
-       // while the rest of the step is still queued, so the device does not idle)
+       // while the rest of the step is still queued, so the device does not idle), or when the
+       // store has fewer pages than SMs (the page re-sort works a page per CTA: on a small
+       // domain of large gridboxes the few pages would run on a few SMs)
       if (x->report_recorded) CUDA_TRY(cudaEventSynchronize(x->ev_report));
       const volatile uint32_t* hm = x->h_motion;
       const uint32_t movers = hm[0], nsd = hm[1];
-      x->sort_full = (uint64_t)movers * 5 > (uint64_t)nsd;
+      x->sort_full = x->resort_policy == CLEO_RESORT_FULL ||
+                     (x->resort_policy == CLEO_RESORT_AUTO &&
+                      ((uint64_t)movers * 5 > (uint64_t)nsd || x->d.npages < (uint32_t)x->sms));
+      if (on_step(x->d.p.motionstep, t_sdm)) x->last_sort_full = x->sort_full;
     }
     int rc;
     if (batched) {

@@ -279,10 +279,20 @@ void* cleo_b200_stream(cleo_b200_ctx* ctx);
 int cleo_b200_kernel_launches(cleo_b200_ctx* ctx, uint64_t* n);
 
 /* What the last re-sort after motion did (synchronises the context's stream): out[0] superdroplets
- * that moved (changed gridbox, left the domain, or were made null by collisions), out[1] pages
- * rewritten, out[2] 1 if every page was repacked, out[3] pages in the store (a page holds 64
- * gridboxes). No reference counterpart: a measurement of the paged store. */
+ * that moved (changed gridbox, left the domain, or were made null by collisions; for a full sort,
+ * the valid ones that changed gridbox), out[1] pages rewritten, out[2] how: 0 the touched
+ * gridboxes in place, 1 every page repacked, 2 the full sort, out[3] pages in the store (a page
+ * holds 64 gridboxes). No reference counterpart: a measurement of the paged store. */
 int cleo_b200_resort_stats(cleo_b200_ctx* ctx, uint64_t out[4]);
+
+/* Which re-sort follows motion (same results either way): CLEO_RESORT_AUTO (default) the page
+ * re-sort unless more than a fifth of the superdroplets moved in the previous motion step or the
+ * store has fewer pages than the GPU has SMs, CLEO_RESORT_PAGES the page re-sort always,
+ * CLEO_RESORT_FULL the full sort always. */
+#define CLEO_RESORT_AUTO 0
+#define CLEO_RESORT_PAGES 1
+#define CLEO_RESORT_FULL 2
+int cleo_b200_set_resort_policy(cleo_b200_ctx* ctx, int policy);
 
 /*
  * Per-stage device timing with CUDA events on the context's stream, the counterpart of the
