@@ -96,12 +96,14 @@ def with_params(wl, **kw):
 #   superdroplet; collisions 24 B read + 24 B write (r, msol, xi) = 48 B; the whole SDM step,
 #   fused lower bound, 120 B per superdroplet-step;
 # * the library's own count of what its kernels must move: condensation reads r, msol, xi,
-#   sdgbxindex (28 B) and writes r, dm, its (20 B) per superdroplet, reads temp, press, qvap and
+#   sdgbxindex (28 B) and writes r, dm, its (20 B) per superdroplet, and after motion writes and
+#   reads each droplet's pre-solve condensate mass for qcond (16 B), reads temp, press, qvap and
 #   writes th_s, th_ff (40 B) per gridbox; collisions read r, msol, xi, coord3/1/2, id (56 B) and
-#   write the 8 permuted fields (60 B) per superdroplet, state, slot, bucket entry per gridbox.
+#   write the 8 permuted fields (60 B) per superdroplet, write and read its pair terminal
+#   velocity (16 B), state, slot, bucket record per gridbox.
 ALG_BYTES_PER_SD = {"condensation": 32, "collisions": 48}
 STEP_BYTES_PER_SD = 120
-OWN_BYTES = {"condensation": (48, 40), "collisions": (116, 64)}  # (per superdroplet, per gridbox)
+OWN_BYTES = {"condensation": (64, 40), "collisions": (132, 64)}  # (per superdroplet, per gridbox)
 
 
 def peaks():

@@ -91,9 +91,8 @@ __device__ __forceinline__ void warp_batch_sums(const DevCtx& c, uint32_t g0, ui
 }
 
 // ---- effect_on_hydrometeor_states (movesupersindomain.hpp:95-136) ----
-// qcond of every gridbox from its (moved and sorted) superdroplets' condensate masses, added in
-// their order (warp_batch_sums)
-// qcond of gridbox g from the sum m of its superdroplets' condensate masses x xi
+// qcond of gridbox g from the sum m of its superdroplets' condensate masses x xi (summed in their
+// order, by k_b_qcond or by the first condensation commit after motion)
 __device__ __forceinline__ void set_qcond(const DevCtx& c, uint32_t g, double m) {
   const double R0cubed_VOL0 = R0 * R0 * R0 / VOL0;
   const double rho_cond = m / c.volume[g] * R0cubed_VOL0;
@@ -779,8 +778,8 @@ k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b
     uint32_t* P = LARGE ? c.scr_p + base : reinterpret_cast<uint32_t*>(smem + 24 * MBUF);
     uint32_t* J = LARGE ? c.scr_j + base
                         : reinterpret_cast<uint32_t*>(smem + 24 * MBUF + 4 * MEDIUM_MAX);
-    // Simmel terminal velocities once per droplet (medium: shared memory after the five staged
-    // arrays; large: computed per pair)
+    // the pair terminal velocities k_b_tv computed (medium: copied to shared memory after the five
+    // staged arrays; large: read per pair)
     double* Stv = LARGE ? nullptr : reinterpret_cast<double*>(smem + 24 * MBUF + 8 * MEDIUM_MAX);
     if (!LARGE) {
       if (tid == 0) {  // the previous gridbox's accesses ended at the barriers above
@@ -807,7 +806,7 @@ k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b
         Sm[k] = c.sd.msol[base + k];
         Sx[k] = c.sd.xi[base + k];
       } else {
-        Stv[k] = pair_tv(p, Sr[k]);
+        Stv[k] = b.tv[base + k];  // k_b_tv's pair terminal velocity of the same radius
       }
       if (k >= 1) J[k] = (uint32_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - k)), 0, (uint64_t)k + 1);
     }
@@ -839,8 +838,8 @@ k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b
     for (uint32_t jj = tid; jj < npairs; jj += NT) {
       const uint32_t a = P[2 * jj], bb = P[2 * jj + 1];
       const Where w{c.err, g, (uint64_t)base + 2 * jj};
-      const double tvA = LARGE ? pair_tv(p, Sr[a]) : Stv[a];
-      const double tvB = LARGE ? pair_tv(p, Sr[bb]) : Stv[bb];
+      const double tvA = LARGE ? b.tv[base + a] : Stv[a];
+      const double tvB = LARGE ? b.tv[base + bb] : Stv[bb];
       nnull += collide_pair(p, Sx, Sr, Sm, a, bb, tvA, tvB, scale_p, VOLUME, key, slot_pairs, jj,
                             w);
     }

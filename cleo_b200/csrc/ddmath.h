@@ -79,6 +79,13 @@ CLEO_MATH_HD dd dd_add(dd a, dd b) {
   s.lo += t.lo;
   return fast_two_sum(s.hi, s.lo);
 }
+// a + b with one two-sum: absolute error below 2^-104 (|a| + |b|), all the first phase needs
+// (its bound is 2^-72 relative, and none of its sums cancels more than a small factor except the
+// reduction a - n ln2/512 of fast_exp, where the absolute error is what counts)
+CLEO_MATH_HD dd dd_add_fast(dd a, dd b) {
+  const dd s = two_sum(a.hi, b.hi);
+  return fast_two_sum(s.hi, s.lo + (a.lo + b.lo));
+}
 CLEO_MATH_HD dd dd_add_d(dd a, double b) {
   dd s = two_sum(a.hi, b);
   s.lo += a.lo;
@@ -252,7 +259,7 @@ CLEO_MATH_HD dd fast_log(double x) {
   const dd l1p = fast_two_sum(s.hi, s.lo + low);
   dd eln2 = two_prod((double)e, CLEO_DD_LN2_HI);
   eln2.lo += (double)e * CLEO_DD_LN2_LO;
-  return dd_add(eln2, dd_add(dd{t[1], t[2]}, l1p));
+  return dd_add_fast(eln2, dd_add_fast(dd{t[1], t[2]}, l1p));
 }
 
 // exp of a double-double with |a.hi| < 600, relative error below 2^-72: a = n ln2/512 + r,
@@ -268,7 +275,7 @@ CLEO_MATH_HD dd fast_exp(dd a) {
   const int j = n & 511;
   const int k = (n - j) / 512;
   const dd p = two_prod(nf, CLEO_DD_LN2_HI * 0x1p-9);
-  dd r = dd_add(a, dd{-p.hi, -p.lo});
+  dd r = dd_add_fast(a, dd{-p.hi, -p.lo});
   r = dd_add_d(r, -nf * (CLEO_DD_LN2_LO * 0x1p-9));
   const double rh = r.hi, rl = r.lo;
   double c = dd_fma(rh, CLEO_DD_INV120_HI, CLEO_DD_INV24_HI);  // Horner with fused steps
@@ -277,7 +284,7 @@ CLEO_MATH_HD dd fast_exp(dd a) {
   const double poly = rh * rh * c;
   const dd em1 = fast_two_sum(rh, rl + rh * rl + poly);
   const dd tj{cleo_fast_exp2_tab[j][0], cleo_fast_exp2_tab[j][1]};
-  dd v = dd_add(tj, dd_mul(tj, em1));
+  dd v = dd_add_fast(tj, dd_mul(tj, em1));
   // |k| <= 866 and v.hi near [1, 2]: both products are normal, so exact (ldexp's values)
   const double sk = pow2i(k);
   v.hi *= sk;

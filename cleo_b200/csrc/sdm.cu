@@ -1188,11 +1188,11 @@ int radix_pairs_on(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, u
   int cur = 0;
   uint32_t* K[2] = {k0, k1};
   uint32_t* V[2] = {v0, v1};
-  // counts up to one tile (the usual mover list) are sorted by one block; the multi-tile passes
+  // counts up to RS_SMALL_MAX (the usual mover list) are sorted by one block; the multi-tile passes
   // below then return at once, and the other way round
-  k_rs_small<<<1, RS_THREADS, 0, s>>>(k0, v0, k1, v1, n_ptr, bits);
+  k_rs_small<<<1, RS_SMALL_THREADS, 0, s>>>(k0, v0, k1, v1, n_ptr, bits);
   x->launches += 1;
-  constexpr uint32_t SMALL = (uint32_t)RS_TILE;
+  constexpr uint32_t SMALL = RS_SMALL_MAX;
   for (uint32_t shift = 0; shift < bits; shift += 8) {
     k_rs_upsweep<<<nt, RS_THREADS, 0, s>>>(K[cur], n_ptr, (int)shift, hist, nt, SMALL);
     k_scan_tiles<<<nscan_tiles, SCAN_THREADS, 0, s>>>(hist, hist, nh, tile_sums, n_ptr, SMALL);

@@ -100,26 +100,29 @@ k_rs_downsweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vi
   }
 }
 
-// The same stable LSD sort for n <= RS_TILE pairs (device count) in one block of RS_THREADS:
-// `bits` key bits in 8-bit passes between (k0, v0) and (k1, v1), leaving the result where the
-// multi-tile passes would (in (k0, v0) after an even number of passes). Returns at once for
-// larger n, which the multi-tile passes sort.
-__global__ void __launch_bounds__(RS_THREADS)
+// The same stable LSD sort for n <= RS_SMALL_MAX pairs (device count) in one block of
+// RS_SMALL_THREADS: `bits` key bits in 8-bit passes between (k0, v0) and (k1, v1), leaving the
+// result where the multi-tile passes would (in (k0, v0) after an even number of passes). Returns
+// at once for larger n, which the multi-tile passes sort.
+constexpr int RS_SMALL_THREADS = 1024;
+constexpr int RS_SMALL_WARPS = RS_SMALL_THREADS / 32;
+constexpr uint32_t RS_SMALL_MAX = (uint32_t)RS_SMALL_THREADS * RS_ITEMS;  // 16384
+__global__ void __launch_bounds__(RS_SMALL_THREADS)
 k_rs_small(uint32_t* __restrict__ k0, uint32_t* __restrict__ v0, uint32_t* __restrict__ k1,
            uint32_t* __restrict__ v1, const uint32_t* __restrict__ n_ptr, uint32_t bits) {
-  static_assert(RS_THREADS == 256, "one thread per digit");
-  __shared__ uint32_t wcount[RS_WARPS][256];
+  __shared__ uint32_t wcount[RS_SMALL_WARPS][256];
   __shared__ uint32_t dbase[256];
-  __shared__ uint32_t wsum[RS_WARPS];
+  __shared__ uint32_t wsum[8];
   const uint32_t n = *n_ptr;
-  if (n > (uint32_t)RS_TILE) return;
+  if (n > RS_SMALL_MAX) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   uint32_t* K[2] = {k0, k1};
   uint32_t* V[2] = {v0, v1};
   int cur = 0;
   for (uint32_t shift = 0; shift < bits; shift += 8) {
-    for (int i = threadIdx.x; i < RS_WARPS * 256; i += RS_THREADS) (&wcount[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < RS_SMALL_WARPS * 256; i += RS_SMALL_THREADS)
+      (&wcount[0][0])[i] = 0;
     __syncthreads();
     uint32_t kk[RS_ITEMS], vv[RS_ITEMS], rk[RS_ITEMS];
 #pragma unroll
@@ -139,23 +142,26 @@ k_rs_small(uint32_t* __restrict__ k0, uint32_t* __restrict__ v0, uint32_t* __res
       rk[j] = valid ? (prev + __popc(peers & lt)) : 0xFFFFFFFFu;
     }
     __syncthreads();
-    {  // digit d = thread: its per-warp offsets, then the exclusive scan of the digit totals
-      const uint32_t d = threadIdx.x;
-      uint32_t tot = 0;
-#pragma unroll
-      for (int w = 0; w < RS_WARPS; ++w) {
+    // digit d = thread d < 256: its per-warp offsets, then the exclusive scan of the digit totals
+    // over the first 8 warps
+    const uint32_t d = threadIdx.x;
+    uint32_t tot = 0, x = 0;
+    if (d < 256) {
+      for (int w = 0; w < RS_SMALL_WARPS; ++w) {
         const uint32_t c = wcount[w][d];
         wcount[w][d] = tot;
         tot += c;
       }
-      uint32_t x = tot;
+      x = tot;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
         if (lane >= o) x += y;
       }
       if (lane == 31) wsum[warp] = x;
-      __syncthreads();
+    }
+    __syncthreads();
+    if (d < 256) {
       uint32_t before = 0;
       for (int w = 0; w < warp; ++w) before += wsum[w];
       dbase[d] = before + x - tot;
@@ -164,8 +170,8 @@ k_rs_small(uint32_t* __restrict__ k0, uint32_t* __restrict__ v0, uint32_t* __res
 #pragma unroll
     for (int j = 0; j < RS_ITEMS; ++j) {
       if (rk[j] != 0xFFFFFFFFu) {
-        const uint32_t d = (kk[j] >> shift) & 255u;
-        const uint32_t pos = dbase[d] + wcount[warp][d] + rk[j];
+        const uint32_t dg = (kk[j] >> shift) & 255u;
+        const uint32_t pos = dbase[dg] + wcount[warp][dg] + rk[j];
         K[1 - cur][pos] = kk[j];
         V[1 - cur][pos] = vv[j];
       }
