@@ -40,4 +40,20 @@ struct BatchScratch {
   uint32_t medium_max;  // small_max..medium_max: CTA kernel in shared memory (<= MEDIUM_MAX)
 };
 
+// scratch of the one-gridbox collision path (onebox.cuh)
+constexpr uint32_t OB_NONE = 0xFFFFFFFFu;
+
+struct OneBox {
+  uint32_t* J;      // swap draws, index s (1 .. n-1)
+  uint32_t* cnt;    // per value: bucket size, then (scanned) bucket start; n + 1 entries
+  uint32_t* fill;   // per value: placement cursor
+  uint32_t* bkt;    // bucket contents (swap indexes), n entries
+  uint32_t* first;  // per value
+  uint32_t* next;   // per swap index
+  uint32_t* P;      // origin of shuffled position k
+  uint32_t* vflag;  // 1 for a valid superdroplet at shuffled position q, scanned; n + 1 entries
+  uint32_t* tsums;  // the scans' tile totals
+  uint32_t* nnull;  // nulls made by this sub-step's collisions
+};
+
 }  // namespace

@@ -128,6 +128,8 @@ struct cleo_b200_ctx {
   uint32_t *gs_tsums = nullptr, *mv_count = nullptr;  // scan tile totals, the mover count
   uint32_t *pstart_new = nullptr, *ps_tsums = nullptr;  // page re-sort: repacked page starts
   double* qm_buf = nullptr;  // BatchScratch::qm's storage
+  bool one_box = false;      // a one-gridbox domain: collisions by the kernels of onebox.cuh
+  OneBox ob{};
   // re-sort choice: {movers, superdroplets} of the previous motion step, written by the device
   // into mapped pinned memory right after that step's motion kernel; an event recorded behind
   // the write (an external event node inside a captured step) lets the host wait for exactly
@@ -897,6 +899,7 @@ __global__ void k_mon_precip(const __grid_constant__ DevCtx c) {
 }  // namespace
 
 #include "batched.cuh"
+#include "onebox.cuh"
 
 namespace {
 
@@ -1276,7 +1279,27 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       k_b_commit<<<gw, SEQ_THREADS, 0, s>>>(d, bc);
       x->launches += 2;
     }
-    if (coll) {
+    if (coll && x->one_box) {  // the one gridbox's collision step over the whole GPU
+      StageMark mk(x, 4);
+      const OneBox& o = x->ob;
+      const int go = grid_for((size_t)d.slots + 1, 256);
+      k_b_tv<<<grid_for(d.slots, 256), 256, 0, s>>>(d, b);
+      k_ob_draw<<<go, 256, 0, s>>>(d, b, o);
+      k_ob_count<<<go, 256, 0, s>>>(d, o);
+      x->launches += 3;
+      scan_u32(x, o.cnt, d.slots + 1, o.tsums);  // bucket starts (entries past n unused)
+      k_ob_place<<<go, 256, 0, s>>>(d, o);
+      k_ob_chains<<<go, 256, 0, s>>>(d, o);
+      k_ob_origin<<<go, 256, 0, s>>>(d, o);
+      k_ob_pairs<<<go, 256, 0, s>>>(d, b, o);
+      k_ob_flags<<<go, 256, 0, s>>>(d, o);
+      x->launches += 5;
+      scan_u32(x, o.vflag, d.slots + 1, o.tsums);  // valid ones before each shuffled position
+      k_ob_gather<<<go, 256, 0, s>>>(d, o);
+      k_ob_commit<<<go, 256, 0, s>>>(d, b, o);
+      k_ob_finish<<<1, 1, 0, s>>>(d, b, o);
+      x->launches += 3;
+    } else if (coll) {
       StageMark mk(x, 4);
       k_b_reset<<<1, 32, 0, s>>>(d, b, 0);
       k_b_classify<<<gg, 256, 0, s>>>(d, b);
@@ -1582,6 +1605,14 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &x->bs.its, cap);
   rc |= dalloc(x, &x->bs.tv, cap + 2);
   rc |= dalloc(x, &x->qm_buf, cap);
+  if (ng == 1) {  // one gridbox: its collisions by the whole GPU (onebox.cuh)
+    OneBox& o = x->ob;
+    for (uint32_t** q : {&o.J, &o.cnt, &o.fill, &o.bkt, &o.first, &o.next, &o.P, &o.vflag})
+      rc |= dalloc(x, q, cap + 2);
+    rc |= dalloc(x, &o.tsums, (cap + 2 + SCAN_TILE - 1) / SCAN_TILE + 1);
+    rc |= dalloc(x, &o.nnull, 1);
+    x->one_box = true;
+  }
   rc |= dalloc(x, &x->bs.zres, cap);
   rc |= dalloc(x, &x->bs.lkeys, cap);
   rc |= dalloc(x, &x->bs.lvals, cap);
