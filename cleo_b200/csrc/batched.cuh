@@ -209,7 +209,10 @@ k_cond_a(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch 
               z1 = e.z;
             }
           }
-          if (!conv) b.zres[i] = conv1 ? -z1 : e.z;  // where pass B's restart continues
+          if (!conv) {
+            b.zres[i] = conv1 ? -z1 : e.z;  // where pass B's restart continues
+            b.ffv[i] = ffactor_fv;
+          }
           if (conv) {
             const double rnew = max_dryradius(sqrt(e.z), msol);  // change_radius
             b.dm[i] = (condensate_mass(rnew, msol, w) - condensate_mass(r, msol, w)) *
@@ -222,6 +225,7 @@ k_cond_a(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch 
         } else {
           defer = true;
           key = deferred_key(p.cond_delt, fmax(crit, p.cond_minsubdelt), true);
+          b.ffv[i] = ffactor_fv;  // pass B's sub-stepping solve starts from it
         }
       }
     }
@@ -260,8 +264,7 @@ k_cond_b(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch 
     if (b.lkeys[j] == 0u && cfg.maxniters >= 2) {
       // a direct solve whose two iterations in pass A did not converge: the restart continues
       // from them (resume_restart), unless the surrogate's seed converges first
-      const double ffactor_fv = b.th_ff[g] / ventilation_factor(r);
-      const OdeConsts o{b.th_s[g], akoh, bkoh, ffactor_fv};
+      const OdeConsts o{b.th_s[g], akoh, bkoh, b.ffv[i]};  // pass A's th_ff / ventilation
       ni = 2;
       double rsqrd = 0.0;
       bool done = false;
@@ -279,8 +282,9 @@ k_cond_b(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch 
       }
       newr = sqrt(rsqrd);
     } else {
-      newr = solve_condensation(cfg, p.cond_delt, p.cond_minsubdelt, b.th_s[g], akoh, bkoh,
-                                b.th_ff[g], r, seed, ni, w);
+      // (b.ffv: pass A's th_ff / ventilation_factor(r), what solve_condensation computes first)
+      newr = solve_condensation_fv(cfg, p.cond_delt, p.cond_minsubdelt, b.th_s[g], akoh, bkoh,
+                                   b.ffv[i], r, seed, ni, w);
     }
     const double rnew = max_dryradius(newr, msol);
     b.dm[i] = (condensate_mass(rnew, msol, w) - condensate_mass(r, msol, w)) * (double)c.sd.xi[i];

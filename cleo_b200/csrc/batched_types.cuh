@@ -28,6 +28,7 @@ struct BatchScratch {
   double* tv;        // per superdroplet pair terminal velocity (pair_tv) for the warp kernel,
                      // two elements of padding for its bulk copies
   double* zres;      // per deferred direct solve: pass A's iterate that pass B resumes from
+  double* ffv;       // per deferred solve: pass A's diffusion factor over the ventilation factor
   uint32_t* lkeys;   // cost keys of deferred solves
   uint32_t* lvals;   // positions of deferred solves
   uint32_t* bucket;  // [4][ngbxs] gridbox lists per size bucket

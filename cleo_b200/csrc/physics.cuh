@@ -747,12 +747,14 @@ __device__ __forceinline__ double max_dryradius(double r, double msol) {
 }
 // solve_condensation: impliciteuler.cpp:35-54 (+ substepping :98-113). A usable seed_rsqrd
 // replaces the Newton start of the direct branch (not the branch decision) by a predicted r^2.
-__device__ __forceinline__ double solve_condensation(const NewtonCfg& c, double delt,
-                                                     double minsubdelt, double s_ratio,
-                                                     double akoh, double bkoh, double ffactor,
-                                                     double rprev, double seed_rsqrd,
-                                                     uint32_t& niters, const Where& w) {
-  const double ffactor_fv = ffactor / ventilation_factor(rprev);
+// solve_condensation_fv takes the diffusion factor already divided by the ventilation factor of
+// rprev (what solve_condensation computes first), for a caller that holds it
+__device__ __forceinline__ double solve_condensation_fv(const NewtonCfg& c, double delt,
+                                                        double minsubdelt, double s_ratio,
+                                                        double akoh, double bkoh,
+                                                        double ffactor_fv, double rprev,
+                                                        double seed_rsqrd, uint32_t& niters,
+                                                        const Where& w) {
   const OdeConsts o{s_ratio, akoh, bkoh, ffactor_fv};
   double ziter = initialguess(o, rprev);
   // ucrit1 || ucrit2: the critical timestep (a general pow) is only needed when ucrit1 fails
@@ -790,6 +792,14 @@ __device__ __forceinline__ double solve_condensation(const NewtonCfg& c, double 
     rsqrd = ziter;
   }
   return sqrt(rsqrd);
+}
+__device__ __forceinline__ double solve_condensation(const NewtonCfg& c, double delt,
+                                                     double minsubdelt, double s_ratio,
+                                                     double akoh, double bkoh, double ffactor,
+                                                     double rprev, double seed_rsqrd,
+                                                     uint32_t& niters, const Where& w) {
+  return solve_condensation_fv(c, delt, minsubdelt, s_ratio, akoh, bkoh,
+                               ffactor / ventilation_factor(rprev), rprev, seed_rsqrd, niters, w);
 }
 
 // ---- scheduling: microphysicalprocess.hpp:222-248 ----

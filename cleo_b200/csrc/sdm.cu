@@ -1614,6 +1614,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
     x->one_box = true;
   }
   rc |= dalloc(x, &x->bs.zres, cap);
+  rc |= dalloc(x, &x->bs.ffv, cap);
   rc |= dalloc(x, &x->bs.lkeys, cap);
   rc |= dalloc(x, &x->bs.lvals, cap);
   rc |= dalloc(x, &x->bs.bucket, 4 * ng);

@@ -300,3 +300,30 @@ def test_gpu_bubble_flow_1m(lib):
     g, o = run_pair(lib, w, 10, cfg=TUNED)
     K.assert_identical_run(g, o, "bubble3d 32x64x32")
     g.close()
+
+
+def test_gpu_resort_policy_and_stats(lib):
+    """The re-sort policies give the same run (the page re-sort, the full sort, the automatic
+    choice), and cleo_b200_resort_stats reports which re-sort ran and how much it rewrote."""
+    runs = {}
+    for policy in (abi.RESORT_AUTO, abi.RESORT_PAGES, abi.RESORT_FULL):
+        w = W.bubble3d(ndims=(8, 16, 8), seed=21)
+        w["params"].exec_mode = abi.EXEC_BATCHED
+        g = make_sdm(w, lib=lib)
+        assert lib.cleo_b200_set_resort_policy(g.ctx, policy) == 0
+        for s in range(4):
+            g.run_step(s * w["tstep"], (s + 1) * w["tstep"])
+        g.check()
+        st = (C.c_uint64 * 4)()
+        assert lib.cleo_b200_resort_stats(g.ctx, st) == 0
+        movers, rewritten, how, pages = (int(v) for v in st)
+        assert pages == (w["grid"]["ngbxs"] + 63) // 64 and movers > 0
+        assert rewritten <= pages
+        if policy == abi.RESORT_PAGES:
+            assert how in (0, 1)  # in place, or every page repacked
+        else:  # 16 pages, fewer than the GPU's SMs: the automatic choice is the full sort too
+            assert how == 2
+        runs[policy] = g.download_supers()
+    for policy in (abi.RESORT_PAGES, abi.RESORT_FULL):
+        K.assert_same_domain(runs[policy], runs[abi.RESORT_AUTO], rtol=0.0, what=f"policy {policy}")
+    assert lib.cleo_b200_set_resort_policy(None, 0) != 0
