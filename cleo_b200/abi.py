@@ -297,7 +297,7 @@ EXPORTED = (
     "cleo_b200_tuned_config", "cleo_b200_set_launch_config", "cleo_b200_monitors_begin",
     "cleo_b200_download_monitors",
     "cleo_b200_upload_state_async", "cleo_b200_download_budgets_async", "cleo_b200_synchronize",
-    "cleo_b200_check_bounded_wait",
+    "cleo_b200_check_bounded_wait", "cleo_b200_check_math",
     "cleo_b200_gather_supers", "cleo_b200_zarr_open", "cleo_b200_zarr_observe",
     "cleo_b200_zarr_observe_host", "cleo_b200_zarr_close",
 )
@@ -360,6 +360,7 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
             ("download_budgets_async", [vp, vp, vp]),
             ("synchronize", [vp]),
             ("check_bounded_wait", [C.c_uint32]),
+            ("check_math", [vp, vp, vp, C.c_size_t]),
             ("gather_supers", [vp, C.c_uint32, C.POINTER(ObsSupers), C.c_size_t,
                                C.POINTER(C.c_size_t)]),
             ("zarr_open", [C.c_char_p, C.c_size_t, C.c_uint32, C.c_uint32, C.POINTER(vp)]),

@@ -57,37 +57,77 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
 // contiguous range [gstart[g0], gstart[g0 + nb]). The warp reads it coalesced, SEQ_WIN elements
 // at a time, into its shared buffers (term(k) -> dbuf, iters(k) -> ubuf), and lane j adds the
 // terms of gridbox g0 + j's valid superdroplets [gstart, gstart + gcount) one after another: the
-// reference's sequential loop (seq_sum's order), with every element of the range loaded once.
+// reference's sequential loop (seq_sum's order). Each window starts at the first element a lane
+// still has to add, so ranges no lane adds are not read. With skip_big, a gridbox of more than
+// SEQ_BIG superdroplets is left out (its lane adds nothing): warp_seq_sum sums it with a warp of
+// its own, so that one long sequential sum does not hold up its batch and large gridboxes are
+// summed in parallel.
 constexpr uint32_t SEQ_WIN = 256;
 constexpr int SEQ_THREADS = 256;
+constexpr uint32_t SEQ_BIG = 128;
 template <class Term, class Iters>
 __device__ __forceinline__ void warp_batch_sums(const DevCtx& c, uint32_t g0, uint32_t nb,
                                                 double* dbuf, uint32_t* ubuf, Term term,
                                                 Iters iters, double& sum,
-                                                unsigned long long& its) {
+                                                unsigned long long& its, bool skip_big) {
   const int lane = threadIdx.x & 31;
-  const uint32_t lo = c.gstart[g0], hi = c.gstart[g0 + nb];
+  const uint32_t hi = c.gstart[g0 + nb];
   const bool own = (uint32_t)lane < nb;
   const uint32_t s = own ? c.gstart[g0 + lane] : hi;
-  const uint32_t e = own ? s + c.gcount[g0 + lane] : hi;
+  uint32_t e = own ? s + c.gcount[g0 + lane] : hi;
+  if (skip_big && e - s > SEQ_BIG) e = s;
   double acc = 0.0;
   unsigned long long it = 0;
-  for (uint32_t w0 = lo; w0 < hi; w0 += SEQ_WIN) {
+  uint32_t cur = s;  // this lane's next element to add
+  while (true) {
+    const uint32_t w0 = __reduce_min_sync(0xFFFFFFFFu, cur < e ? cur : 0xFFFFFFFFu);
+    if (w0 == 0xFFFFFFFFu) break;
     const uint32_t w1 = hi - w0 < SEQ_WIN ? hi : w0 + SEQ_WIN;
     for (uint32_t k = w0 + lane; k < w1; k += 32) {
       dbuf[k - w0] = term(k);
       ubuf[k - w0] = iters(k);
     }
     __syncwarp();
-    const uint32_t a = s > w0 ? s : w0, b = e < w1 ? e : w1;
-    for (uint32_t k = a; k < b; ++k) {
+    const uint32_t b = e < w1 ? e : w1;
+    for (uint32_t k = cur; k < b; ++k) {
       acc += dbuf[k - w0];
       it += ubuf[k - w0];
     }
+    if (cur < b) cur = b;
     __syncwarp();
   }
   sum = acc;
   its = it;
+}
+// the same sequential sum for one gridbox's range [s, e) by a whole warp: 32 terms loaded at a
+// time (the next 32 in flight meanwhile), broadcast one by one and added in order by every lane;
+// the iterations (integers, any order) per lane, then across the warp
+template <class Term, class Iters>
+__device__ __forceinline__ void warp_seq_sum(uint32_t s, uint32_t e, Term term, Iters iters,
+                                             double& sum, unsigned long long& its) {
+  const uint32_t lane = threadIdx.x & 31;
+  double acc = 0.0;
+  unsigned long long it = 0;
+  double v = s + lane < e ? term(s + lane) : 0.0;
+  uint32_t u = s + lane < e ? iters(s + lane) : 0u;
+  for (uint32_t k0 = s; k0 < e; k0 += 32) {
+    const uint32_t kn = k0 + 32 + lane;
+    const double vn = kn < e ? term(kn) : 0.0;
+    const uint32_t un = kn < e ? iters(kn) : 0u;
+    const uint32_t m = e - k0 < 32 ? e - k0 : 32;
+#pragma unroll
+    for (uint32_t j = 0; j < 32; ++j) {
+      const double t = __shfl_sync(0xFFFFFFFFu, v, j);
+      if (j < m) acc += t;
+    }
+    it += u;
+    v = vn;
+    u = un;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) it += __shfl_down_sync(0xFFFFFFFFu, it, o);
+  sum = acc;
+  its = __shfl_sync(0xFFFFFFFFu, it, 0);
 }
 
 // ---- effect_on_hydrometeor_states (movesupersindomain.hpp:95-136) ----
@@ -116,7 +156,7 @@ __global__ void __launch_bounds__(SEQ_THREADS) k_b_qcond(const __grid_constant__
                                    (double)c.sd.xi[i]
                              : 0.0;
         },
-        [](uint32_t) { return 0u; }, m, unused);
+        [](uint32_t) { return 0u; }, m, unused, false);
     if ((uint32_t)lane < nb) set_qcond(c, g0 + lane, m);
   }
 }
@@ -126,7 +166,7 @@ __global__ void __launch_bounds__(SEQ_THREADS) k_b_qcond(const __grid_constant__
 // temperature with it)
 __global__ void k_b_thermo(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b) {
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < c.ngbxs; g += gridDim.x * blockDim.x) {
-    if (g == 0) b.ctr[0] = b.ctr[9] = 0;  // deferred solves, of which restarts
+    if (g == 0) b.ctr[0] = b.ctr[9] = b.ctr[10] = 0;  // deferred solves, restarts, big gridboxes
     const Where w{c.err, g, c.gstart[g]};
     const double temp = c.temp[g];
     const double psat = saturation_pressure(temp, w);
@@ -346,6 +386,7 @@ __device__ __forceinline__ void cond_commit(const DevCtx& c, uint32_t g, double 
 // The condensed mass of each gridbox's superdroplets added in their order (warp_batch_sums, the
 // reference's sequential reduction, condensation.cpp:29-35), their Newton iterations, then the
 // state update (cond_commit). Empty gridboxes commit a zero change, as the reference's do.
+// Gridboxes of more than SEQ_BIG superdroplets are listed for k_b_commit_big instead.
 __global__ void __launch_bounds__(SEQ_THREADS) k_b_commit(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b) {
   __shared__ double dbuf[SEQ_THREADS / 32][SEQ_WIN];
   __shared__ uint32_t ubuf[SEQ_THREADS / 32][SEQ_WIN];
@@ -354,19 +395,43 @@ __global__ void __launch_bounds__(SEQ_THREADS) k_b_commit(const __grid_constant_
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (uint32_t g0 = warp * 32; g0 < c.ngbxs; g0 += nwarps * 32) {
     const uint32_t nb = c.ngbxs - g0 < 32 ? c.ngbxs - g0 : 32;
+    const bool own = (uint32_t)lane < nb;
+    const bool big = own && c.gcount[g0 + lane] > SEQ_BIG;
+    const uint32_t pos = warp_append(&b.ctr[10], big);
+    if (big) b.big[pos] = g0 + lane;
     double m;
     unsigned long long it;
     if (b.qm) {  // qcond from the moved superdroplets first (k_b_qcond's sums, from pass A)
       warp_batch_sums(
           c, g0, nb, dbuf[wib], ubuf[wib], [&](uint32_t i) { return b.qm[i]; },
-          [](uint32_t) { return 0u; }, m, it);
-      if ((uint32_t)lane < nb) set_qcond(c, g0 + lane, m);
+          [](uint32_t) { return 0u; }, m, it, true);
+      if (own && !big) set_qcond(c, g0 + lane, m);
     }
     // (positions past a gridbox's valid superdroplets are loaded but not added)
     warp_batch_sums(
         c, g0, nb, dbuf[wib], ubuf[wib], [&](uint32_t i) { return b.dm[i]; },
-        [&](uint32_t i) { return b.its[i]; }, m, it);
-    if ((uint32_t)lane < nb) cond_commit(c, g0 + lane, m, it);
+        [&](uint32_t i) { return b.its[i]; }, m, it, true);
+    if (own && !big) cond_commit(c, g0 + lane, m, it);
+  }
+}
+// the listed gridboxes of more than SEQ_BIG superdroplets, a warp each (the same sums and
+// updates as k_b_commit's lanes make)
+__global__ void __launch_bounds__(SEQ_THREADS) k_b_commit_big(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t nbig = b.ctr[10];
+  for (uint32_t j = warp; j < nbig; j += nwarps) {
+    const uint32_t g = b.big[j];
+    const uint32_t s = c.gstart[g], e = s + c.gcount[g];
+    double m;
+    unsigned long long it;
+    if (b.qm) {
+      warp_seq_sum(s, e, [&](uint32_t i) { return b.qm[i]; }, [](uint32_t) { return 0u; }, m, it);
+      if ((threadIdx.x & 31) == 0) set_qcond(c, g, m);
+    }
+    warp_seq_sum(s, e, [&](uint32_t i) { return b.dm[i]; }, [&](uint32_t i) { return b.its[i]; },
+                 m, it);
+    if ((threadIdx.x & 31) == 0) cond_commit(c, g, m, it);
   }
 }
 

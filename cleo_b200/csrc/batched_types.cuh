@@ -35,7 +35,8 @@ struct BatchScratch {
   uint4* brec;       // [2][ngbxs] the warp kernel's buckets as {gridbox, start, count, RNG slot}
   uint32_t* slot;    // per gridbox RNG slot offset within the SDM step
   uint32_t* ctr;     // [0] deferred solves, [1..4] bucket counts, [5..8] bucket heads,
-                     // [9] restarts among the deferred solves
+                     // [9] restarts among the deferred solves, [10] big gridboxes (commit)
+  uint32_t* big;     // gridboxes whose condensation commit takes a warp each (k_b_commit_big)
   uint32_t* tsdm;    // the SDM step's start time (keys the injected random numbers)
   uint32_t small_max;   // gridboxes with 1..small_max superdroplets: warp kernel (<= WARP_MAX)
   uint32_t medium_max;  // small_max..medium_max: CTA kernel in shared memory (<= MEDIUM_MAX)

@@ -314,6 +314,67 @@ CLEO_MATH_HD double dexp(double x) {
   return dexp_dd(x);
 }
 
+// First phase for the exponents 1/6, 1/3 and 2/3 (as doubles: k/6 - eps with eps = 2^-57/3,
+// 2^-56/3, 2^-55/3), for 2^-600 <= x <= 2^600, relative error below 2^-76:
+//   x = 2^(3q) m with m in [1, 8); x^y = 2^(qk/2) m^(k/6) exp(-eps L), L = ln x, |eps L| <
+//   2^-45.9, so exp(-eps L) = 1 - w + w^2/2 with w = eps L (remainder below 2^-136). w's
+//   absolute error is eps times L's, so L from the exponent and a single-precision log2 of the
+//   leading significand (absolute error below 2^-22) puts at most 2^-77 into the result;
+//   m^(1/3): the inverse cube root y from a single-precision start (relative 2^-22) by two Newton
+//   steps y (1 + (1 - m y^3) / 3) (error 2 e^2 each, so to the double's precision), c0 = m y^2
+//   (within 2^-50), then one Newton step for the cube root with the exact residual: c0^2 = t + e1
+//   and t c0 = u + ul exactly (fused multiply-adds), m - u exact (Sterbenz), the residual to
+//   2^-102 m, the step res y^2 / 3 to 2^-99 c, the step's own truncation below 2^-99;
+//   m^(2/3) the double-double square of it, m^(1/6) its double-double square root (one step from
+//   the correctly rounded sqrt of the high part, whose residual fma is exact).
+constexpr double Y16 = 1.0 / 6.0, Y13 = 1.0 / 3.0, Y23 = 2.0 / 3.0;
+CLEO_MATH_HD dd fast_sixth_pow(double x, double yexp) {
+  const uint64_t xb = dbits(x);
+  const int e = (int)((xb >> 52) & 0x7FF) - 1023;
+  const int q = e >= 0 ? e / 3 : -((2 - e) / 3);  // floor(e / 3)
+  const double m = bitsd((xb & 0x000FFFFFFFFFFFFFull) | ((uint64_t)(1023 + e - 3 * q) << 52));
+#if defined(__CUDA_ARCH__)
+  double y = (double)rcbrtf((float)m);
+#else
+  double y = (double)(1.0f / std::cbrt((float)m));
+#endif
+  y = y + y * (1.0 - m * y * y * y) * (1.0 / 3.0);
+  y = y + y * (1.0 - m * y * y * y) * (1.0 / 3.0);
+  const double y2 = y * y;
+  const double c0 = m * y2;
+  const double t = c0 * c0;
+  const double e1 = dd_fma(c0, c0, -t);
+  const double u = t * c0;
+  const double ul = dd_fma(t, c0, -u);
+  const double res = ((m - u) - ul) - e1 * c0;
+  dd c = fast_two_sum(c0, res * y2 * (1.0 / 3.0));
+  double eps;
+  int shift;  // x^(k/6) = 2^shift m^(k/6) with shift = q k / 2, q even where k = 1
+  if (yexp == Y13) {
+    eps = 0x1.5555555555555p-56;
+    shift = q;
+  } else if (yexp == Y23) {
+    eps = 0x1.5555555555555p-55;
+    shift = 2 * q;
+    const dd s2 = two_prod(c.hi, c.hi);
+    c = fast_two_sum(s2.hi, s2.lo + 2.0 * c.hi * c.lo);
+  } else {  // 1/6: sqrt(2^q m^(1/3)), 2^q's odd part moved under the root
+    eps = 0x1.5555555555555p-57;
+    if (q & 1) {
+      c.hi *= 2.0;
+      c.lo *= 2.0;
+    }
+    shift = (q - (q & 1)) / 2;
+    const double s0 = std::sqrt(c.hi);
+    const double r = dd_fma(-s0, s0, c.hi) + c.lo;
+    c = fast_two_sum(s0, r / (2.0 * s0));
+  }
+  const float mf = (float)bitsd((xb & 0x000FFFFFFFFFFFFFull) | 0x3FF0000000000000ull);
+  const double w = eps * (((double)e + (double)std::log2(mf)) * 0.69314718055994530942);
+  const double sk = pow2i(shift);
+  return fast_two_sum(c.hi * sk, (c.lo - c.hi * (w - 0.5 * w * w)) * sk);
+}
+
 // pow(x, y) for the exponents CLEO uses, rounded once
 CLEO_MATH_HD double dpow(double x, double y) {
   if (y == 2.0) return x * x;
@@ -325,6 +386,11 @@ CLEO_MATH_HD double dpow(double x, double y) {
   if (y == 3.0) {
     const dd x2 = two_prod(x, x);
     return round_dd(dd_mul_d(x2, x));
+  }
+  if ((y == Y13 || y == Y23 || y == Y16) && x >= 0x1p-600 && x <= 0x1p600) {
+    const dd v = fast_sixth_pow(x, y);
+    if (fast_round_ok(v)) return v.hi;
+    return dpow_dd(x, y);
   }
   const dd z = dd_mul_d(fast_log(x), y);
   if (z.hi > -600.0 && z.hi < 600.0) {

@@ -386,13 +386,15 @@ __device__ __forceinline__ bool move_superdroplet(const DevCtx& c, uint32_t i,
     // change_if_coord3nghbr: finite z, coordinate unchanged at the edge (cartesianmaps.cpp:184-213)
     uint32_t idx = g;
     int flag = flag_sdgbxindex(idx, ng, bzl, bzh, n3);
+    bool crossed = flag != 0;  // whether any face was crossed (then idx may differ from g)
     if (flag == 1) idx = c.back3[idx];
     else if (flag == 2) idx = c.fwd3[idx];
     // change_if_coord1nghbr: periodic x (cartesianmaps.cpp:148-179)
     {
-      double l, h;
-      bounds_of(c.b1lo, c.b1hi, ng, idx, l, h);
+      double l = bxl, h = bxh;  // g's own bounds unless z moved the superdroplet
+      if (crossed) bounds_of(c.b1lo, c.b1hi, ng, idx, l, h);
       flag = flag_sdgbxindex(idx, ng, l, h, n1);
+      crossed |= flag != 0;
       const uint32_t incre = c.ndims[0];
       if (flag == 1) {
         const uint32_t nghbr = c.back1[idx];
@@ -414,9 +416,10 @@ __device__ __forceinline__ bool move_superdroplet(const DevCtx& c, uint32_t i,
     }
     // change_if_coord2nghbr: periodic y (cartesianmaps.cpp:112-143)
     {
-      double l, h;
-      bounds_of(c.b2lo, c.b2hi, ng, idx, l, h);
+      double l = byl, h = byh;
+      if (crossed) bounds_of(c.b2lo, c.b2hi, ng, idx, l, h);
       flag = flag_sdgbxindex(idx, ng, l, h, n2);
+      crossed |= flag != 0;
       const uint32_t incre = c.ndims[0] * c.ndims[1];
       if (flag == 1) {
         const uint32_t nghbr = c.back2[idx];
@@ -443,7 +446,9 @@ __device__ __forceinline__ bool move_superdroplet(const DevCtx& c, uint32_t i,
     if (bits(n1) != bits(c1)) c.sd.c1[i] = n1;
     if (bits(n2) != bits(c2)) c.sd.c2[i] = n2;
     if (idx != g) c.sd.gbx[i] = idx;
-    if (idx < ng) {  // CartesianCheckBounds (cartesian_motion.hpp:38-54)
+    // CartesianCheckBounds (cartesian_motion.hpp:38-54); a superdroplet that crossed no face
+    // stays in g with every coordinate inside g's bounds (the three flags were 0), so passes it
+    if (crossed && idx < ng) {
       double l, h;
       bool bad = false;
       bounds_of(c.b3lo, c.b3hi, ng, idx, l, h);
@@ -556,6 +561,12 @@ k_obs_gather(const __grid_constant__ DevCtx c, ObsOut o, const uint32_t* __restr
 
 // self-check of the bounded waits: an mbarrier that nothing arrives on, waited for with the
 // same bounded wait as the bulk-copy and tensor-core waits; the bound must run out
+__global__ void k_math_check(const double* __restrict__ x, const double* __restrict__ y,
+                             double* __restrict__ out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = y ? cleo::dpow(x[i], y[i]) : cleo::dexp(x[i]);
+}
 __global__ void k_wait_check(uint32_t max_tries, int* __restrict__ out) {
   __shared__ uint64_t bar;
   if (threadIdx.x == 0) mlp::mbar_init(&bar, 1);
@@ -1275,9 +1286,11 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
         else
           k_cond_b<3><<<x->grid_condb[0], 256, 0, s>>>(d, b);
       }
-      // every gridbox's condensed mass summed in order, its state updated
+      // every gridbox's condensed mass summed in order, its state updated (the gridboxes of
+      // more than SEQ_BIG superdroplets by a warp each)
       k_b_commit<<<gw, SEQ_THREADS, 0, s>>>(d, bc);
-      x->launches += 2;
+      k_b_commit_big<<<x->sms * 4, SEQ_THREADS, 0, s>>>(d, bc);
+      x->launches += 3;
     }
     if (coll && x->one_box) {  // the one gridbox's collision step over the whole GPU
       StageMark mk(x, 4);
@@ -1618,6 +1631,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   rc |= dalloc(x, &x->bs.lkeys, cap);
   rc |= dalloc(x, &x->bs.lvals, cap);
   rc |= dalloc(x, &x->bs.bucket, 4 * ng);
+  rc |= dalloc(x, &x->bs.big, ng);
   rc |= dalloc(x, &x->bs.brec, 2 * ng);
   rc |= dalloc(x, &x->bs.slot, ng);
   rc |= dalloc(x, &x->bs.ctr, 12);
@@ -2043,6 +2057,15 @@ int cleo_b200_set_launch_config(cleo_b200_ctx* x, const int32_t cfg[4]) {
   x->tune_total = 0;  // ends a tuning run in progress
   x->tune_step = 0;
   x->drop_graphs();
+  return CLEO_OK;
+}
+
+int cleo_b200_check_math(const double* d_x, const double* d_y, double* d_out, size_t n) {
+  if (n == 0) return CLEO_OK;
+  if (!d_x || !d_out) return CLEO_ERR_ARGUMENT;
+  k_math_check<<<grid_for(n, 256), 256>>>(d_x, d_y, d_out, n);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaDeviceSynchronize());
   return CLEO_OK;
 }
 

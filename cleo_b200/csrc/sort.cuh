@@ -50,9 +50,6 @@ k_rs_downsweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vi
                uint32_t small_n = 0) {
   __shared__ uint32_t wcount[RS_WARPS][256];
   __shared__ uint32_t dbase[256];
-  __shared__ uint32_t lbase[256];  // the tile's own digit starts
-  __shared__ uint32_t wsum[RS_WARPS];
-  __shared__ uint32_t skey[RS_TILE], sval[RS_TILE];  // the tile in digit order
   const uint32_t n = *n_ptr;
   const uint32_t tile = blockIdx.x;
   const uint64_t base = (uint64_t)tile * RS_TILE;
@@ -82,49 +79,24 @@ k_rs_downsweep(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vi
     rk[j] = valid ? (prev + __popc(peers & lt)) : 0xFFFFFFFFu;
   }
   __syncthreads();
-  static_assert(RS_THREADS == 256, "one thread per digit");
-  {  // digit d = thread: its per-warp offsets, then the tile's digit starts (exclusive scan)
-    const uint32_t d = threadIdx.x;
-    uint32_t tot = 0;
+  for (int d = threadIdx.x; d < 256; d += RS_THREADS) {
+    uint32_t s = 0;
 #pragma unroll
     for (int w = 0; w < RS_WARPS; ++w) {
       const uint32_t c = wcount[w][d];
-      wcount[w][d] = tot;
-      tot += c;
+      wcount[w][d] = s;
+      s += c;
     }
-    uint32_t x = tot;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) wsum[warp] = x;
-    __syncthreads();
-    uint32_t before = 0;
-    for (int w = 0; w < warp; ++w) before += wsum[w];
-    lbase[d] = before + x - tot;
   }
   __syncthreads();
-  // the tile in digit order in shared memory (each key at its rank within the tile) ...
 #pragma unroll
   for (int j = 0; j < RS_ITEMS; ++j) {
     if (rk[j] != 0xFFFFFFFFu) {
       const uint32_t d = (kk[j] >> shift) & 255u;
-      const uint32_t lp = lbase[d] + wcount[warp][d] + rk[j];
-      skey[lp] = kk[j];
-      sval[lp] = vv[j];
+      const uint32_t pos = dbase[d] + wcount[warp][d] + rk[j];
+      kout[pos] = kk[j];
+      vout[pos] = vv[j];
     }
-  }
-  __syncthreads();
-  // ... then written out in that order: consecutive threads write consecutive positions of a
-  // digit's run (the same positions as each key's rank would give, so the same result)
-  const uint32_t m = n - base < (uint64_t)RS_TILE ? (uint32_t)(n - base) : (uint32_t)RS_TILE;
-  for (uint32_t i = threadIdx.x; i < m; i += RS_THREADS) {
-    const uint32_t key = skey[i];
-    const uint32_t d = (key >> shift) & 255u;
-    const uint32_t pos = dbase[d] + (i - lbase[d]);
-    kout[pos] = key;
-    vout[pos] = sval[i];
   }
 }
 

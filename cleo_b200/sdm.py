@@ -179,7 +179,9 @@ def _main(argv=None):
 
     from . import workloads as W
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="uneven3d", choices=["uneven3d", "bubble3d"])
+    ap.add_argument("--workload", default="uneven3d", choices=["uneven3d", "bubble3d", "rainshaft"],
+                    help="rainshaft: the 1x1x256 column of 256 superdroplets per gridbox "
+                         "(--ndims ignored)")
     ap.add_argument("--ndims", type=int, nargs=3, default=(32, 64, 64))
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--plain", action="store_true", help="the plain schedule (default batched)")
@@ -188,8 +190,11 @@ def _main(argv=None):
                          "CTAs per SM of the warp kernel's 64-slot variant "
                          "(cleo_b200_set_launch_config)")
     a = ap.parse_args(argv)
-    build = W.uneven3d if a.workload == "uneven3d" else W.bubble3d
-    w = build(ndims=tuple(a.ndims))
+    if a.workload == "rainshaft":
+        w = W.rainshaft()
+    else:
+        build = W.uneven3d if a.workload == "uneven3d" else W.bubble3d
+        w = build(ndims=tuple(a.ndims))
     w["params"].exec_mode = abi.EXEC_PLAIN if a.plain else abi.EXEC_BATCHED
     g = make_sdm(w)
     if a.launch_config is not None:

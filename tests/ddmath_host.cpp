@@ -40,6 +40,11 @@ extern "C" void dd_compare_pow(uint64_t seed, uint64_t n, double lx0, double lx1
       }
       ++mm;
     }
+    // the first phase dpow takes for (x, y)
+    if ((y == cleo::Y13 || y == cleo::Y23 || y == cleo::Y16) && x >= 0x1p-600 && x <= 0x1p600) {
+      if (!cleo::fast_round_ok(cleo::fast_sixth_pow(x, y))) ++df;
+      continue;
+    }
     const cleo::dd z = cleo::dd_mul_d(cleo::fast_log(x), y);
     if (!(z.hi > -600.0 && z.hi < 600.0) || !cleo::fast_round_ok(cleo::fast_exp(z))) ++df;
   }
@@ -94,4 +99,26 @@ extern "C" double dd_fast_pow_maxerr(uint64_t seed, uint64_t n, double lx0, doub
     if (rel > worst) worst = rel;
   }
   return worst;
+}
+
+// largest relative difference between the first phase for the exponents 1/6, 1/3, 2/3 and the
+// accurate double-double pow, over n random x = 2^U[lx0, lx1) (within the phase's range)
+extern "C" double dd_fast_sixth_maxerr(uint64_t seed, uint64_t n, double lx0, double lx1) {
+  const double ys[3] = {cleo::Y16, cleo::Y13, cleo::Y23};
+  double worst = 0.0;
+  for (uint64_t i = 0; i < n; ++i) {
+    const double x = std::exp2(lx0 + (lx1 - lx0) * unit(mix(seed ^ (2 * i))));
+    const double y = ys[mix(seed ^ (2 * i + 1)) % 3];
+    const cleo::dd f = cleo::fast_sixth_pow(x, y);
+    const cleo::dd a = cleo::dd_exp(cleo::dd_mul_d(cleo::dd_log(x), y));
+    const cleo::dd d = cleo::dd_add(f, cleo::dd{-a.hi, -a.lo});
+    const double rel = std::fabs(d.hi / a.hi);
+    if (rel > worst) worst = rel;
+  }
+  return worst;
+}
+
+// out[i] = dpow(x[i], y[i]), or dexp(x[i]) when y is null (the host side of the device check)
+extern "C" void dd_eval_array(const double* x, const double* y, double* out, uint64_t n) {
+  for (uint64_t i = 0; i < n; ++i) out[i] = y ? cleo::dpow(x[i], y[i]) : cleo::dexp(x[i]);
 }

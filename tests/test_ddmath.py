@@ -71,21 +71,23 @@ def test_agreement_with_host_libm(lib):
         assert np.all(ulps <= 1.0), (y, ulps.max())
 
 
-FAST_CASES = [  # (x = 2^U[lx0, lx1), y from EXPONENTS or U[y0, y1))
-    (-40.0, 40.0, True, 0.0, 0.0),
-    (-1000.0, 1000.0, False, -0.6, 0.6),
-    (-5.0, 5.0, False, -60.0, 60.0),
-    (-1.0, 1.0, False, -3.0, 3.0),
+THIRDS = (1.0 / 6.0, 1.0 / 3.0, 2.0 / 3.0)
+FAST_CASES = [  # (x = 2^U[lx0, lx1), y from the listed exponents or U[y0, y1))
+    (-40.0, 40.0, EXPONENTS, 0.0, 0.0),
+    (-1000.0, 1000.0, None, -0.6, 0.6),
+    (-5.0, 5.0, None, -60.0, 60.0),
+    (-1.0, 1.0, None, -3.0, 3.0),
+    (-600.0, 600.0, THIRDS, 0.0, 0.0),  # the cube-root first phase over its whole range
 ]
 
 
 @pytest.mark.parametrize("case", FAST_CASES)
 def test_fast_pow_phase_is_bit_identical(lib, case):
     lx0, lx1, listed, y0, y1 = case
-    ys = (C.c_double * len(EXPONENTS))(*EXPONENTS) if listed else None
+    ys = (C.c_double * len(listed))(*listed) if listed else None
     mm, df, bad = C.c_uint64(), C.c_uint64(), (C.c_double * 2)()
     n = 1_000_000
-    lib.dd_compare_pow(11, n, lx0, lx1, ys, len(EXPONENTS) if listed else 0, y0, y1,
+    lib.dd_compare_pow(11, n, lx0, lx1, ys, len(listed) if listed else 0, y0, y1,
                        C.byref(mm), C.byref(df), bad)
     assert mm.value == 0, (mm.value, list(bad))
     assert df.value < 1e-3 * n  # the accurate phase runs rarely
@@ -103,6 +105,16 @@ def test_fast_phase_error_inside_its_bound(lib):
     # the rounding test assumes 2^-67; the analysis gives 2^-72
     for lx0, lx1, y0, y1 in [(-40, 40, -3, 3), (-1000, 1000, -0.5, 0.5), (-5, 5, -60, 60)]:
         assert lib.dd_fast_pow_maxerr(5, 300_000, lx0, lx1, y0, y1) < 2.0 ** -71
+
+
+def test_cube_root_phase_error_inside_its_bound(lib):
+    # the first phase of the exponents 1/6, 1/3, 2/3 (cube root by Newton steps, the exponent's
+    # rounding from a single-precision logarithm): 2^-76 by its analysis, against the accurate
+    # phase's double-double value (itself good to about 2^-100); the rounding test assumes 2^-67
+    lib.dd_fast_sixth_maxerr.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double]
+    lib.dd_fast_sixth_maxerr.restype = C.c_double
+    for lx0, lx1 in [(-40, 40), (-600, 600), (-1, 1)]:
+        assert lib.dd_fast_sixth_maxerr(7, 300_000, lx0, lx1) < 2.0 ** -76
 
 
 def test_pow_pair_matches_two_pows(lib):
