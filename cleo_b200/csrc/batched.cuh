@@ -58,7 +58,8 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
 // at a time, into its shared buffers (term(k) -> dbuf, iters(k) -> ubuf), and lane j adds the
 // terms of gridbox g0 + j's valid superdroplets [gstart, gstart + gcount) one after another: the
 // reference's sequential loop (seq_sum's order). Each window starts at the first element a lane
-// still has to add, so ranges no lane adds are not read. With skip_big, a gridbox of more than
+// still has to add, so ranges no lane adds are not read, and is loaded into registers while the
+// window before it is being added. With skip_big, a gridbox of more than
 // SEQ_BIG superdroplets is left out (its lane adds nothing): warp_seq_sum sums it with a warp of
 // its own, so that one long sequential sum does not hold up its batch and large gridboxes are
 // summed in parallel.
@@ -70,6 +71,8 @@ __device__ __forceinline__ void warp_batch_sums(const DevCtx& c, uint32_t g0, ui
                                                 double* dbuf, uint32_t* ubuf, Term term,
                                                 Iters iters, double& sum,
                                                 unsigned long long& its, bool skip_big) {
+  constexpr int PER = SEQ_WIN / 32;  // elements of a window per lane
+  constexpr uint32_t NONE = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const uint32_t hi = c.gstart[g0 + nb];
   const bool own = (uint32_t)lane < nb;
@@ -79,54 +82,86 @@ __device__ __forceinline__ void warp_batch_sums(const DevCtx& c, uint32_t g0, ui
   double acc = 0.0;
   unsigned long long it = 0;
   uint32_t cur = s;  // this lane's next element to add
-  while (true) {
-    const uint32_t w0 = __reduce_min_sync(0xFFFFFFFFu, cur < e ? cur : 0xFFFFFFFFu);
-    if (w0 == 0xFFFFFFFFu) break;
+  // the window [w0, w0 + SEQ_WIN) clipped to hi, loaded into registers a window ahead
+  double pv[PER];
+  uint32_t pu[PER];
+  const auto load = [&](uint32_t w0) {
     const uint32_t w1 = hi - w0 < SEQ_WIN ? hi : w0 + SEQ_WIN;
-    for (uint32_t k = w0 + lane; k < w1; k += 32) {
-      dbuf[k - w0] = term(k);
-      ubuf[k - w0] = iters(k);
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const uint32_t k = w0 + 32 * q + lane;
+      pv[q] = k < w1 ? term(k) : 0.0;
+      pu[q] = k < w1 ? iters(k) : 0u;
+    }
+  };
+  uint32_t w0 = __reduce_min_sync(0xFFFFFFFFu, cur < e ? cur : NONE);
+  if (w0 != NONE) load(w0);
+  while (w0 != NONE) {
+    const uint32_t w1 = hi - w0 < SEQ_WIN ? hi : w0 + SEQ_WIN;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      dbuf[32 * q + lane] = pv[q];
+      ubuf[32 * q + lane] = pu[q];
     }
     __syncwarp();
     const uint32_t b = e < w1 ? e : w1;
+    const uint32_t next = cur < b ? b : cur;  // the cursor after this window
+    const uint32_t nw0 = __reduce_min_sync(0xFFFFFFFFu, next < e ? next : NONE);
+    if (nw0 != NONE) load(nw0);  // in flight while this window is added
     for (uint32_t k = cur; k < b; ++k) {
       acc += dbuf[k - w0];
       it += ubuf[k - w0];
     }
-    if (cur < b) cur = b;
+    cur = next;
     __syncwarp();
+    w0 = nw0;
   }
   sum = acc;
   its = it;
 }
-// the same sequential sum for one gridbox's range [s, e) by a whole warp: 32 terms loaded at a
-// time (the next 32 in flight meanwhile), broadcast one by one and added in order by every lane;
-// the iterations (integers, any order) per lane, then across the warp
-template <class Term, class Iters>
-__device__ __forceinline__ void warp_seq_sum(uint32_t s, uint32_t e, Term term, Iters iters,
-                                             double& sum, unsigned long long& its) {
+// the same sequential sums for one gridbox's range [s, e) by a whole warp: up to SEQ_GROUP chunks
+// of 32 terms loaded at once, each chunk's terms broadcast one by one and added in order by every
+// lane. Two sums (qcond's condensate masses qm, when given, and the condensed masses dm) are
+// independent chains and run interleaved; the iterations (integers, any order) are added per lane,
+// then across the warp.
+constexpr int SEQ_GROUP = 8;
+__device__ __forceinline__ void warp_seq_sums(uint32_t s, uint32_t e, const double* qm,
+                                              const double* dm, const uint32_t* its_in,
+                                              double& qsum, double& dsum,
+                                              unsigned long long& its) {
   const uint32_t lane = threadIdx.x & 31;
-  double acc = 0.0;
+  double aq = 0.0, ad = 0.0;
   unsigned long long it = 0;
-  double v = s + lane < e ? term(s + lane) : 0.0;
-  uint32_t u = s + lane < e ? iters(s + lane) : 0u;
-  for (uint32_t k0 = s; k0 < e; k0 += 32) {
-    const uint32_t kn = k0 + 32 + lane;
-    const double vn = kn < e ? term(kn) : 0.0;
-    const uint32_t un = kn < e ? iters(kn) : 0u;
-    const uint32_t m = e - k0 < 32 ? e - k0 : 32;
+  for (uint32_t k0 = s; k0 < e; k0 += 32 * SEQ_GROUP) {
+    double vq[SEQ_GROUP], vd[SEQ_GROUP];
 #pragma unroll
-    for (uint32_t j = 0; j < 32; ++j) {
-      const double t = __shfl_sync(0xFFFFFFFFu, v, j);
-      if (j < m) acc += t;
+    for (int q = 0; q < SEQ_GROUP; ++q) {
+      const uint32_t k = k0 + 32 * q + lane;
+      const bool in = k < e;
+      vq[q] = in && qm ? qm[k] : 0.0;
+      vd[q] = in ? dm[k] : 0.0;
+      it += in ? its_in[k] : 0u;
     }
-    it += u;
-    v = vn;
-    u = un;
+#pragma unroll
+    for (int q = 0; q < SEQ_GROUP; ++q) {
+      const uint32_t c0 = k0 + 32 * q;
+      if (c0 >= e) break;  // uniform across the warp
+      const uint32_t m = e - c0 < 32 ? e - c0 : 32;
+#pragma unroll
+      for (uint32_t j = 0; j < 32; ++j) {
+        const double tq = __shfl_sync(0xFFFFFFFFu, vq[q], j);
+        const double td = __shfl_sync(0xFFFFFFFFu, vd[q], j);
+        if (j < m) {
+          aq += tq;
+          ad += td;
+        }
+      }
+    }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) it += __shfl_down_sync(0xFFFFFFFFu, it, o);
-  sum = acc;
+  qsum = aq;
+  dsum = ad;
   its = __shfl_sync(0xFFFFFFFFu, it, 0);
 }
 
@@ -423,15 +458,13 @@ __global__ void __launch_bounds__(SEQ_THREADS) k_b_commit_big(const __grid_const
   for (uint32_t j = warp; j < nbig; j += nwarps) {
     const uint32_t g = b.big[j];
     const uint32_t s = c.gstart[g], e = s + c.gcount[g];
-    double m;
+    double mq, md;
     unsigned long long it;
-    if (b.qm) {
-      warp_seq_sum(s, e, [&](uint32_t i) { return b.qm[i]; }, [](uint32_t) { return 0u; }, m, it);
-      if ((threadIdx.x & 31) == 0) set_qcond(c, g, m);
+    warp_seq_sums(s, e, b.qm, b.dm, b.its, mq, md, it);
+    if ((threadIdx.x & 31) == 0) {
+      if (b.qm) set_qcond(c, g, mq);  // qcond from the moved superdroplets first
+      cond_commit(c, g, md, it);
     }
-    warp_seq_sum(s, e, [&](uint32_t i) { return b.dm[i]; }, [&](uint32_t i) { return b.its[i]; },
-                 m, it);
-    if ((threadIdx.x & 31) == 0) cond_commit(c, g, m, it);
   }
 }
 

@@ -1136,7 +1136,7 @@ int sort_current(cleo_b200_ctx* x) {
 
 int radix_pairs_on(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1,
                    const uint32_t* n_ptr, uint32_t bits, uint32_t* hist, uint32_t* tile_sums,
-                   uint32_t nt);
+                   uint32_t nt, uint32_t unsorted_max = 0);
 
 // The page re-sort after motion (pages.cuh; k_motion left a mover mask per 32 slots): scan of the
 // masks' counts, the movers listed in position order and stably radix-sorted by key, copied out
@@ -1195,7 +1195,7 @@ int sort_incremental(cleo_b200_ctx* x) {
 // scan of the table)
 int radix_pairs_on(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1,
                    const uint32_t* n_ptr, uint32_t bits, uint32_t* hist, uint32_t* tile_sums,
-                   uint32_t nt) {
+                   uint32_t nt, uint32_t unsorted_max) {
   cudaStream_t s = x->stream;
   const uint64_t nh = (uint64_t)256 * nt;
   const uint32_t nscan_tiles = (uint32_t)((nh + SCAN_TILE - 1) / SCAN_TILE);
@@ -1204,7 +1204,9 @@ int radix_pairs_on(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, u
   uint32_t* V[2] = {v0, v1};
   // counts up to RS_SMALL_MAX (the usual mover list) are sorted by one block; the multi-tile passes
   // below then return at once, and the other way round
-  k_rs_small<<<1, RS_SMALL_THREADS, 0, s>>>(k0, v0, k1, v1, n_ptr, bits);
+  // (with unsorted_max, counts up to it stay as they are: a caller for whom the order is only a
+  // schedule, and an even number of passes, so that the sorted result would be in place too)
+  k_rs_small<<<1, RS_SMALL_THREADS, 0, s>>>(k0, v0, k1, v1, n_ptr, bits, unsorted_max);
   x->launches += 1;
   constexpr uint32_t SMALL = RS_SMALL_MAX;
   for (uint32_t shift = 0; shift < bits; shift += 8) {
@@ -1220,8 +1222,9 @@ int radix_pairs_on(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, u
   return cur;
 }
 int radix_pairs(cleo_b200_ctx* x, uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1,
-                const uint32_t* n_ptr, uint32_t bits) {
-  return radix_pairs_on(x, k0, v0, k1, v1, n_ptr, bits, x->hist, x->tile_sums, x->ntiles_max);
+                const uint32_t* n_ptr, uint32_t bits, uint32_t unsorted_max = 0) {
+  return radix_pairs_on(x, k0, v0, k1, v1, n_ptr, bits, x->hist, x->tile_sums, x->ntiles_max,
+                        unsorted_max);
 }
 
 // the microphysics of one SDM step on the batched schedule (batched.cuh)
@@ -1263,8 +1266,14 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       else
         k_cond_a<3><<<grid_for(d.slots, x->cfg.cond_block), x->cfg.cond_block, 0, s>>>(d, bc);
       x->launches += 1;
-      const int where = radix_pairs(x, b.lkeys, b.lvals, x->keys[1], x->vals[1], b.ctr, 16);
-      if (where != 0) return CLEO_ERR_CUDA;  // 16 key bits: two passes, result back in place
+      // 16 key bits: two passes, result back in place. The order (most expensive solves first)
+      // balances pass B's load; a list of up to RS_SMALL_MAX solves runs at once on pass B's
+      // resident threads whatever its order, so it stays unsorted, unless the surrogate needs
+      // its restarts at the front
+      const uint32_t unsorted_max = d.p.nr_seed == CLEO_NRSEED_MLP ? 0u : RS_SMALL_MAX;
+      const int where =
+          radix_pairs(x, b.lkeys, b.lvals, x->keys[1], x->vals[1], b.ctr, 16, unsorted_max);
+      if (where != 0) return CLEO_ERR_CUDA;
       if (d.p.nr_seed == CLEO_NRSEED_MLP) {
         // the surrogate seeds only the direct solves pass A left unconverged, in b.dm
         mlp::Infer w;

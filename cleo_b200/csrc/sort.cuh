@@ -109,12 +109,13 @@ constexpr int RS_SMALL_WARPS = RS_SMALL_THREADS / 32;
 constexpr uint32_t RS_SMALL_MAX = (uint32_t)RS_SMALL_THREADS * RS_ITEMS;  // 16384
 __global__ void __launch_bounds__(RS_SMALL_THREADS)
 k_rs_small(uint32_t* __restrict__ k0, uint32_t* __restrict__ v0, uint32_t* __restrict__ k1,
-           uint32_t* __restrict__ v1, const uint32_t* __restrict__ n_ptr, uint32_t bits) {
+           uint32_t* __restrict__ v1, const uint32_t* __restrict__ n_ptr, uint32_t bits,
+           uint32_t unsorted_max = 0) {
   __shared__ uint32_t wcount[RS_SMALL_WARPS][256];
   __shared__ uint32_t dbase[256];
   __shared__ uint32_t wsum[8];
   const uint32_t n = *n_ptr;
-  if (n > RS_SMALL_MAX) return;
+  if (n > RS_SMALL_MAX || n <= unsorted_max) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   uint32_t* K[2] = {k0, k1};
