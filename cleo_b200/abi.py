@@ -53,6 +53,7 @@ MLP_TCGEN05, MLP_MMA_SYNC, MLP_FP32 = 0, 1, 2
 MONITOR_MASSMOMENTS, MONITOR_RAINMASSMOMENTS, MONITOR_PRECIPITATION = 1, 2, 4
 NITERS_FAILED = 0x80000000  # or-ed into a batch solve's iteration count: that droplet aborted
 RESORT_AUTO, RESORT_PAGES, RESORT_FULL = 0, 1, 2
+MATH_POW, MATH_EXP, MATH_VENT = 0, 1, 2  # cleo_b200_check_math's functions
 MLP_NFEATURES, MLP_NHIDDEN, MLP_NPARAMS, MLP_NNORM = 7, 64, 4737, 16
 # enum cleo_obs_var: superdroplet output variables, with their output types
 OBS_VARS = {"sdId": (1, np.uint32), "sdgbxindex": (2, np.uint32), "xi": (4, np.uint64),
@@ -360,7 +361,7 @@ def load_library(path: os.PathLike | str | None = None) -> C.CDLL:
             ("download_budgets_async", [vp, vp, vp]),
             ("synchronize", [vp]),
             ("check_bounded_wait", [C.c_uint32]),
-            ("check_math", [vp, vp, vp, C.c_size_t]),
+            ("check_math", [C.c_int, vp, vp, vp, C.c_size_t]),
             ("gather_supers", [vp, C.c_uint32, C.POINTER(ObsSupers), C.c_size_t,
                                C.POINTER(C.c_size_t)]),
             ("zarr_open", [C.c_char_p, C.c_size_t, C.c_uint32, C.c_uint32, C.POINTER(vp)]),

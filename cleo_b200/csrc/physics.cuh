@@ -474,7 +474,8 @@ __device__ __forceinline__ double diffusion_factor(double press, double temp, do
   const double fdl = TEMP / (DIFFUSE_V * PSAT) / F0;
   return Rho_l * (fkl + fdl);
 }
-__device__ __forceinline__ double ventilation_factor(double radius) {
+// ventilation_factor (impliciteuler.cpp:131-145) with the correctly rounded powers
+__device__ __forceinline__ double ventilation_factor_cr(double radius) {
   const double vent_factor_max = 20;
   const double C1 = 6.954e+7;
   const double A = 1.963;
@@ -486,6 +487,46 @@ __device__ __forceinline__ double ventilation_factor(double radius) {
   const double b = 1.0 / (C2 * pb);
   const double vent_factor = 1.0 + 1.0 / (a + b);
   return fmin(vent_factor, vent_factor_max);
+}
+// x^y for 2^-60 <= x < 1 (x = 2^e m, m in [1, 2)) from the library's log2 and exp2, relative
+// error below 2^-50: log2 m to 2^-53 absolute (1 ulp documented, |log2 m| < 1), so y log2 m to
+// 2^-51 with its rounding (y < 2); y e exact as a double-double; exp2 of the sum's high part
+// (2 ulp documented) times 1 + lo ln2 (lo below 2^-46, so the omitted term is below 2^-93)
+__device__ __forceinline__ double vent_pow(double y, int e, double lm) {
+  const dd ye = two_prod(y, (double)e);
+  dd z = two_sum(ye.hi, y * lm);
+  z = fast_two_sum(z.hi, z.lo + ye.lo);
+  return exp2(z.hi) * (1.0 + z.lo * 0.69314718055994530942);
+}
+// The same doubles as ventilation_factor_cr, from powers good to 2^-50 where they decide it.
+// The result is 1 + d, d = 1 / (a + b), rounded once. With the powers off by at most eps
+// (relative) from the correctly rounded ones, each of the five rounded steps up to d adds at most
+// 2^-52, so d is within (eps + 2^-50) d of the reference's; when 1 + d lies farther than that
+// from the rounding boundaries around RN(1 + d) (two_sum gives its exact remainder), the
+// reference rounds to the same double. eps is taken as 2^-48 (the analysis gives 2^-49.6 with the
+// correctly rounded value's half ulp). The check fails in about 2^6 d of the cases, so a warp
+// tries this form only when all its droplets are below 1.5 um (d below about 2e-4); otherwise,
+// and when the check fails, the correctly rounded powers decide.
+__device__ __forceinline__ double ventilation_factor(double radius) {
+  const double x = radius * R0;
+  const bool quick = x >= 0x1p-60 && x < 1.5e-6;
+  if (__all_sync(__activemask(), quick)) {
+    const uint64_t xb = dbits(x);
+    const int e = (int)((xb >> 52) & 0x7FF) - 1023;
+    const double lm = log2(bitsd((xb & 0x000FFFFFFFFFFFFFull) | 0x3FF0000000000000ull));
+    const double pa = vent_pow(1.963, e, lm), pb = vent_pow(0.702, e, lm);
+    const double a = 1.0 / (6.954e+7 * pa);
+    const double b = 1.0 / (1.069e+3 * pb);
+    const double d = 1.0 / (a + b);
+    const dd v = two_sum(1.0, d);  // v.hi = RN(1 + d), v.lo = 1 + d - v.hi exactly
+    const double bound = d * 0x1p-47;
+    const uint64_t vb = dbits(v.hi);
+    const double u = bitsd(vb & 0x7FF0000000000000ull) * 0x1p-52;  // ulp of v.hi in [1, 20)
+    const double d_up = 0.5 * u;
+    const double d_down = (vb & 0x000FFFFFFFFFFFFFull) == 0 ? 0.25 * u : 0.5 * u;
+    if (v.hi < 19.0 && v.lo + bound < d_up && v.lo - bound > -d_down) return v.hi;
+  }
+  return ventilation_factor_cr(radius);
 }
 __device__ __forceinline__ double kohler_a(double temp) {
   const double akoh_constant = 3.3e-7 / (TEMP0 * R0);

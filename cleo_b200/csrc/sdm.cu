@@ -561,11 +561,13 @@ k_obs_gather(const __grid_constant__ DevCtx c, ObsOut o, const uint32_t* __restr
 
 // self-check of the bounded waits: an mbarrier that nothing arrives on, waited for with the
 // same bounded wait as the bulk-copy and tensor-core waits; the bound must run out
-__global__ void k_math_check(const double* __restrict__ x, const double* __restrict__ y,
+__global__ void k_math_check(int fn, const double* __restrict__ x, const double* __restrict__ y,
                              double* __restrict__ out, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
-    out[i] = y ? cleo::dpow(x[i], y[i]) : cleo::dexp(x[i]);
+    out[i] = fn == CLEO_MATH_POW   ? cleo::dpow(x[i], y[i])
+             : fn == CLEO_MATH_EXP ? cleo::dexp(x[i])
+                                   : ventilation_factor(x[i]);
 }
 __global__ void k_wait_check(uint32_t max_tries, int* __restrict__ out) {
   __shared__ uint64_t bar;
@@ -2069,10 +2071,12 @@ int cleo_b200_set_launch_config(cleo_b200_ctx* x, const int32_t cfg[4]) {
   return CLEO_OK;
 }
 
-int cleo_b200_check_math(const double* d_x, const double* d_y, double* d_out, size_t n) {
+int cleo_b200_check_math(int fn, const double* d_x, const double* d_y, double* d_out,
+                         size_t n) {
+  if (fn != CLEO_MATH_POW && fn != CLEO_MATH_EXP && fn != CLEO_MATH_VENT) return CLEO_ERR_ARGUMENT;
   if (n == 0) return CLEO_OK;
-  if (!d_x || !d_out) return CLEO_ERR_ARGUMENT;
-  k_math_check<<<grid_for(n, 256), 256>>>(d_x, d_y, d_out, n);
+  if (!d_x || !d_out || (fn == CLEO_MATH_POW && !d_y)) return CLEO_ERR_ARGUMENT;
+  k_math_check<<<grid_for(n, 256), 256>>>(fn, d_x, d_y, d_out, n);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaDeviceSynchronize());
   return CLEO_OK;

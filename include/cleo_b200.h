@@ -518,12 +518,18 @@ int cleo_b200_zarr_close(cleo_b200_zarr* z);
 int cleo_b200_check_bounded_wait(uint32_t max_tries);
 
 /*
- * Self-check of the device math (no counterpart in the reference): out[i] = the device's
- * correctly rounded pow(x[i], y[i]), or exp(x[i]) when y is NULL, for n elements of device
- * arrays, on the current device's default stream (synchronised before return). The same
- * functions built for the host give the values to compare with, bit for bit.
+ * Self-check of the device math (no counterpart in the reference), for n elements of device
+ * arrays on the current device's default stream (synchronised before return):
+ *   fn = CLEO_MATH_POW:  out[i] = the correctly rounded pow(x[i], y[i])
+ *   fn = CLEO_MATH_EXP:  out[i] = the correctly rounded exp(x[i])  (y unused)
+ *   fn = CLEO_MATH_VENT: out[i] = the ventilation factor of radius x[i] (impliciteuler.cpp:
+ *                        131-145, as the condensation kernels evaluate it; y unused)
+ * The same functions built for the host give the values to compare with, bit for bit.
  */
-int cleo_b200_check_math(const double* d_x, const double* d_y, double* d_out, size_t n);
+#define CLEO_MATH_POW 0
+#define CLEO_MATH_EXP 1
+#define CLEO_MATH_VENT 2
+int cleo_b200_check_math(int fn, const double* d_x, const double* d_y, double* d_out, size_t n);
 
 /* Library version string. */
 const char* cleo_b200_version(void);

@@ -122,3 +122,15 @@ extern "C" double dd_fast_sixth_maxerr(uint64_t seed, uint64_t n, double lx0, do
 extern "C" void dd_eval_array(const double* x, const double* y, double* out, uint64_t n) {
   for (uint64_t i = 0; i < n; ++i) out[i] = y ? cleo::dpow(x[i], y[i]) : cleo::dexp(x[i]);
 }
+
+// the ventilation factor (impliciteuler.cpp:131-145) with the correctly rounded powers, radius in
+// CLEO's units (1e-6 m)
+extern "C" void dd_vent_array(const double* radius, double* out, uint64_t n) {
+  for (uint64_t i = 0; i < n; ++i) {
+    double pa, pb;
+    cleo::dpow2(radius[i] * 1e-6, 1.963, 0.702, pa, pb);
+    const double a = 1.0 / (6.954e+7 * pa);
+    const double b = 1.0 / (1.069e+3 * pb);
+    out[i] = std::fmin(1.0 + 1.0 / (a + b), 20.0);
+  }
+}
