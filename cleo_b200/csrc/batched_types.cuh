@@ -56,6 +56,7 @@ struct OneBox {
   uint32_t* vflag;  // 1 for a valid superdroplet at shuffled position q, scanned; n + 1 entries
   uint32_t* tsums;  // the scans' tile totals
   uint32_t* nnull;  // nulls made by this sub-step's collisions
+  uint32_t* ninv;   // superdroplets left with multiplicity 0 (the flags' zeros)
 };
 
 }  // namespace

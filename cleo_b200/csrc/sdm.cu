@@ -1307,18 +1307,28 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       StageMark mk(x, 4);
       const OneBox& o = x->ob;
       const int go = grid_for((size_t)d.slots + 1, 256);
-      k_b_tv<<<grid_for(d.slots, 256), 256, 0, s>>>(d, b);
+      if (d.p.coll_prob == CLEO_PROB_LONG) {  // otherwise the pair terminal velocities stay 0
+        k_b_tv<<<grid_for(d.slots, 256), 256, 0, s>>>(d, b);
+        x->launches += 1;
+      }
+      // scans of n + 1 entries (entries past n unused): one block while the slots allow
+      const bool one_block = (uint64_t)d.slots + 1 <= OB_SCAN_MAX;
+      const auto scan = [&](uint32_t* a, const uint32_t* skip) {
+        if (one_block) {
+          k_ob_scan<<<1, SCAN_THREADS, 0, s>>>(d, a, skip);
+          x->launches += 1;
+        } else {
+          scan_u32(x, a, d.slots + 1, o.tsums);
+        }
+      };
       k_ob_draw<<<go, 256, 0, s>>>(d, b, o);
-      k_ob_count<<<go, 256, 0, s>>>(d, o);
-      x->launches += 3;
-      scan_u32(x, o.cnt, d.slots + 1, o.tsums);  // bucket starts (entries past n unused)
+      x->launches += 1;
+      scan(o.cnt, nullptr);  // bucket starts
       k_ob_place<<<go, 256, 0, s>>>(d, o);
       k_ob_chains<<<go, 256, 0, s>>>(d, o);
-      k_ob_origin<<<go, 256, 0, s>>>(d, o);
       k_ob_pairs<<<go, 256, 0, s>>>(d, b, o);
-      k_ob_flags<<<go, 256, 0, s>>>(d, o);
-      x->launches += 5;
-      scan_u32(x, o.vflag, d.slots + 1, o.tsums);  // valid ones before each shuffled position
+      x->launches += 3;
+      scan(o.vflag, o.ninv);  // valid ones before each shuffled position (none to count: left out)
       k_ob_gather<<<go, 256, 0, s>>>(d, o);
       k_ob_commit<<<go, 256, 0, s>>>(d, b, o);
       k_ob_finish<<<1, 1, 0, s>>>(d, b, o);
@@ -1327,8 +1337,10 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       StageMark mk(x, 4);
       k_b_reset<<<1, 32, 0, s>>>(d, b, 0);
       k_b_classify<<<gg, 256, 0, s>>>(d, b);
-      k_b_tv<<<grid_for(d.slots, 256), 256, 0, s>>>(d, b);
-      x->launches += 1;
+      if (d.p.coll_prob == CLEO_PROB_LONG) {  // otherwise the pair terminal velocities stay 0
+        k_b_tv<<<grid_for(d.slots, 256), 256, 0, s>>>(d, b);
+        x->launches += 1;
+      }
       // the warp kernel's 64-slot variant takes gridboxes up to 64 superdroplets, its 128-slot
       // variant those of 65 .. small_max (when small_max > 64)
       const int wide = x->cfg.small_max > SMALL_MAX ? 1 : 0, m3 = x->cfg.small_minb == 3 ? 1 : 0;
@@ -1635,6 +1647,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
       rc |= dalloc(x, q, cap + 2);
     rc |= dalloc(x, &o.tsums, (cap + 2 + SCAN_TILE - 1) / SCAN_TILE + 1);
     rc |= dalloc(x, &o.nnull, 1);
+    rc |= dalloc(x, &o.ninv, 1);
     x->one_box = true;
   }
   rc |= dalloc(x, &x->bs.zres, cap);
@@ -1714,6 +1727,12 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
   CUDA_TRY(cudaMemsetAsync(d.pg_flag, 0, (size_t)d.npages * 4, x->stream));
   CUDA_TRY(cudaMemsetAsync(d.pg_ctr, 0, 16, x->stream));
   CUDA_TRY(cudaMemsetAsync(d.mv_stamp, 0, (size_t)d.ngbxs * 4, x->stream));
+  // pair terminal velocities: 0 unless the Long kernel's k_b_tv writes them
+  CUDA_TRY(cudaMemsetAsync(x->bs.tv, 0, ((size_t)d.slots + 2) * 8, x->stream));
+  if (x->one_box) {  // the one-box counts start at zero (k_ob_gather clears what a step used)
+    CUDA_TRY(cudaMemsetAsync(x->ob.cnt, 0, ((size_t)d.slots + 2) * 4, x->stream));
+    CUDA_TRY(cudaMemsetAsync(x->ob.fill, 0, ((size_t)d.slots + 2) * 4, x->stream));
+  }
   CUDA_TRY(cudaMemsetAsync(d.err, 0, sizeof(DevError), x->stream));
   CUDA_TRY(cudaFuncSetAttribute(k_micro, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MICRO_SMEM));
   CUDA_TRY(cudaMemsetAsync(x->bs.ctr, 0, 48, x->stream));

@@ -179,9 +179,10 @@ def _main(argv=None):
 
     from . import workloads as W
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="uneven3d", choices=["uneven3d", "bubble3d", "rainshaft"],
-                    help="rainshaft: the 1x1x256 column of 256 superdroplets per gridbox "
-                         "(--ndims ignored)")
+    ap.add_argument("--workload", default="uneven3d",
+                    choices=["uneven3d", "bubble3d", "rainshaft", "box"],
+                    help="rainshaft: the 1x1x256 column of 256 superdroplets per gridbox; box: "
+                         "the Golovin box model of 8192 superdroplets (--ndims ignored)")
     ap.add_argument("--ndims", type=int, nargs=3, default=(32, 64, 64))
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--plain", action="store_true", help="the plain schedule (default batched)")
@@ -192,6 +193,8 @@ def _main(argv=None):
     a = ap.parse_args(argv)
     if a.workload == "rainshaft":
         w = W.rainshaft()
+    elif a.workload == "box":
+        w = W.box_golovin()
     else:
         build = W.uneven3d if a.workload == "uneven3d" else W.bubble3d
         w = build(ndims=tuple(a.ndims))
