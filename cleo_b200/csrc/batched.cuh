@@ -60,7 +60,7 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
 // reference's sequential loop (seq_sum's order). Each window starts at the first element a lane
 // still has to add, so ranges no lane adds are not read, and is loaded into registers while the
 // window before it is being added. With skip_big, a gridbox of more than
-// SEQ_BIG superdroplets is left out (its lane adds nothing): warp_seq_sum sums it with a warp of
+// SEQ_BIG superdroplets is left out (its lane adds nothing): warp_seq_sums sums it with a warp of
 // its own, so that one long sequential sum does not hold up its batch and large gridboxes are
 // summed in parallel.
 constexpr uint32_t SEQ_WIN = 256;
@@ -1027,7 +1027,12 @@ k_b_cta(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b
 // the device copy of the SDM step time: set before a step whose time the device does not hold,
 // advanced by the last kernel of every step (so one captured step graph serves every step)
 __global__ void k_b_set_t(BatchScratch b, uint32_t t) { *b.tsdm = t; }
-__global__ void k_b_advance_t(BatchScratch b, uint32_t dt) { *b.tsdm += dt; }
+// the SDM step's end: its start time advanced; with zero_slot0 (a one-gridbox domain, whose step
+// has no per-gridbox reset) the gridbox's RNG slot is reset for the next step here
+__global__ void k_b_advance_t(BatchScratch b, uint32_t dt, int zero_slot0) {
+  *b.tsdm += dt;
+  if (zero_slot0) b.slot[0] = 0;
+}
 
 __global__ void k_b_reset(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b, int slots) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;

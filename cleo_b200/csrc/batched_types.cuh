@@ -57,6 +57,7 @@ struct OneBox {
   uint32_t* tsums;  // the scans' tile totals
   uint32_t* nnull;  // nulls made by this sub-step's collisions
   uint32_t* ninv;   // superdroplets left with multiplicity 0 (the flags' zeros)
+  uint32_t* nstep;  // the gridbox's count at the step's start (for k_ob_commit)
 };
 
 }  // namespace

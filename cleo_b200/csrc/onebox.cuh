@@ -20,7 +20,7 @@
 //   (exclusive scan of the flags)
 //   k_ob_gather  thread per destination: valid superdroplets in shuffled order, then the nulls,
 //                into scratch; it also clears cnt and fill for the next step. k_ob_commit copies
-//                the records back, k_ob_finish sets the count and RNG slot
+//                the records back and sets the count and RNG slot
 // The host takes this path for domains of one gridbox; every array is sized by the store's slots.
 #pragma once
 
@@ -171,6 +171,7 @@ __global__ void k_ob_gather(const __grid_constant__ DevCtx c, OneBox o) {
   const uint32_t n = c.gcount[0], base = c.gstart[0];
   const uint32_t nvalid = n - *o.nnull;
   const uint32_t ninv = *o.ninv;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *o.nstep = n;  // k_ob_commit updates the count
   for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q <= n; q += gridDim.x * blockDim.x) {
     o.cnt[q] = 0u;
     o.fill[q] = 0u;
@@ -191,10 +192,17 @@ __global__ void k_ob_gather(const __grid_constant__ DevCtx c, OneBox o) {
     c.scr_id[t] = c.sd.id[i];
   }
 }
+// the records back from scratch; the gridbox's count and RNG slot after the step (its count at
+// the step's start comes from k_ob_gather, so no thread reads the count this kernel sets)
 __global__ void k_ob_commit(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b,
                             OneBox o) {
-  const uint32_t n = c.gcount[0], base = c.gstart[0];
+  const uint32_t n = *o.nstep, base = c.gstart[0];
   const uint32_t nvalid = n - *o.nnull;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const uint64_t slot_pairs = (uint64_t)b.slot[0] + (n >= 1 ? n - 1 : 0);
+    c.gcount[0] = nvalid;
+    b.slot[0] = (uint32_t)(slot_pairs + 2ull * (n / 2));
+  }
   for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
     const uint32_t t = base + q;
     c.sd.r[t] = c.scr_r[t];
@@ -206,14 +214,6 @@ __global__ void k_ob_commit(const __grid_constant__ DevCtx c, const __grid_const
     c.sd.id[t] = c.scr_id[t];
     c.sd.gbx[t] = q < nvalid ? 0u : OOB;
   }
-}
-__global__ void k_ob_finish(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b,
-                            OneBox o) {
-  const uint32_t n = c.gcount[0];
-  const uint32_t npairs = n / 2;
-  const uint64_t slot_pairs = (uint64_t)b.slot[0] + (n >= 1 ? n - 1 : 0);
-  c.gcount[0] = n - *o.nnull;
-  b.slot[0] = (uint32_t)(slot_pairs + 2ull * npairs);
 }
 
 }  // namespace

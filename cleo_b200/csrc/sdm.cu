@@ -1250,8 +1250,12 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
   b.qm = nullptr;
   BatchScratch bq = b;  // the first sub-step's scratch
   bq.qm = fuse_qcond ? x->qm_buf : nullptr;
-  k_b_reset<<<gg, 256, 0, s>>>(d, b, 1);
-  x->launches += 1;
+  // every gridbox's RNG slot from 0 at the step's start (a one-gridbox domain's was reset by the
+  // previous step's k_b_advance_t, or at creation)
+  if (!x->one_box) {
+    k_b_reset<<<gg, 256, 0, s>>>(d, b, 1);
+    x->launches += 1;
+  }
   uint32_t subt = t_sdm;
   while (subt < t_sdm_next) {
     const bool cond = on_step(d.p.condstep, subt);
@@ -1331,8 +1335,7 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
       scan(o.vflag, o.ninv);  // valid ones before each shuffled position (none to count: left out)
       k_ob_gather<<<go, 256, 0, s>>>(d, o);
       k_ob_commit<<<go, 256, 0, s>>>(d, b, o);
-      k_ob_finish<<<1, 1, 0, s>>>(d, b, o);
-      x->launches += 3;
+      x->launches += 2;
     } else if (coll) {
       StageMark mk(x, 4);
       k_b_reset<<<1, 32, 0, s>>>(d, b, 0);
@@ -1359,7 +1362,7 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
     }
     subt = min(next_step(d.p.condstep, subt), next_step(d.p.collstep, subt));
   }
-  k_b_advance_t<<<1, 1, 0, s>>>(b, t_sdm_next - t_sdm);
+  k_b_advance_t<<<1, 1, 0, s>>>(b, t_sdm_next - t_sdm, x->one_box ? 1 : 0);
   x->launches += 1;
   CUDA_TRY(cudaGetLastError());
   return CLEO_OK;
@@ -1648,6 +1651,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
     rc |= dalloc(x, &o.tsums, (cap + 2 + SCAN_TILE - 1) / SCAN_TILE + 1);
     rc |= dalloc(x, &o.nnull, 1);
     rc |= dalloc(x, &o.ninv, 1);
+    rc |= dalloc(x, &o.nstep, 1);
     x->one_box = true;
   }
   rc |= dalloc(x, &x->bs.zres, cap);
