@@ -6,7 +6,8 @@
 //   k_ob_draw    thread per swap index s >= 1: J[s], the Fisher-Yates draw (shuffle.hpp:80-87),
 //                counted per value J (cnt, all zero on entry)
 //   (exclusive scan of cnt: the start of each value's bucket; k_ob_scan, one block, when the
-//   store's slots allow)
+//   store's slots allow; k_ob_front does these four phases in one block for stores of up to
+//   OB_FRONT_MAX slots)
 //   k_ob_place   thread per s: s into its value's bucket (unordered)
 //   k_ob_chains  thread per value v: its bucket sorted (increasing s), FIRST[v] and NEXT[s] (the
 //                chains of the warp kernel: FIRST[v] the first swap index with J = v, NEXT[s] the
@@ -113,6 +114,79 @@ __global__ void k_ob_chains(const __grid_constant__ DevCtx c, OneBox o) {
     }
     o.first[v] = a < e ? o.bkt[a] : OB_NONE;
     for (uint32_t i = a; i < e; ++i) o.next[o.bkt[i]] = i + 1 < e ? o.bkt[i + 1] : OB_NONE;
+  }
+}
+// The front of the step (k_ob_draw, the counts' scan, k_ob_place, k_ob_chains: the same values)
+// in one block for a store of up to OB_FRONT_MAX slots, the counting sort's tables in shared
+// memory: cnt and fill (n + 1 each), J and the buckets as 16-bit indexes (n each). J, FIRST and
+// NEXT go to global memory for k_ob_pairs. Four launches become one.
+constexpr uint32_t OB_FRONT_THREADS = 1024;
+constexpr uint32_t OB_FRONT_MAX = 16384;
+constexpr size_t ob_front_smem(uint32_t slots) {
+  return (size_t)(slots + 1) * 8 + (size_t)slots * 4 + 16;
+}
+__global__ void __launch_bounds__(OB_FRONT_THREADS)
+k_ob_front(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b, OneBox o) {
+  extern __shared__ __align__(16) unsigned char ob_smem[];
+  __shared__ uint32_t wsum[32];
+  const uint32_t n = c.gcount[0];
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(ob_smem);
+  uint32_t* fill = cnt + (n + 1);
+  uint16_t* J = reinterpret_cast<uint16_t*>(fill + (n + 1));
+  uint16_t* bkt = J + n;  // the n - 1 swap indexes by value
+  const uint32_t t = threadIdx.x;
+  for (uint32_t v = t; v <= n; v += blockDim.x) {
+    cnt[v] = 0u;
+    fill[v] = 0u;
+  }
+  if (t == 0) {
+    *o.nnull = 0;
+    *o.ninv = 0;
+  }
+  __syncthreads();
+  const uint64_t key = cleo_rng_key(c.p.seed, *b.tsdm, 0);
+  const uint64_t slot = b.slot[0];
+  for (uint32_t s = 1 + t; s < n; s += blockDim.x) {
+    const uint32_t j =
+        (uint32_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - s)), 0, (uint64_t)s + 1);
+    J[s] = (uint16_t)j;
+    o.J[s] = j;
+    atomicAdd(&cnt[j], 1u);
+  }
+  __syncthreads();
+  {  // exclusive scan of cnt[0 .. n]: thread t its contiguous share, then across the block
+    const uint32_t m = n + 1, per = (m + blockDim.x - 1) / blockDim.x;
+    const uint32_t lo = t * per < m ? t * per : m;
+    const uint32_t hi = lo + per < m ? lo + per : m;
+    uint32_t sum = 0;
+    for (uint32_t i = lo; i < hi; ++i) sum += cnt[i];
+    uint32_t total;
+    uint32_t run = block_exclusive_scan_1024(sum, wsum, total);
+    for (uint32_t i = lo; i < hi; ++i) {
+      const uint32_t x = cnt[i];
+      cnt[i] = run;
+      run += x;
+    }
+  }
+  __syncthreads();
+  for (uint32_t s = 1 + t; s < n; s += blockDim.x) {
+    const uint32_t v = J[s];
+    bkt[cnt[v] + atomicAdd(&fill[v], 1u)] = (uint16_t)s;
+  }
+  __syncthreads();
+  for (uint32_t v = t; v < n; v += blockDim.x) {
+    const uint32_t a = cnt[v], e = cnt[v + 1];
+    for (uint32_t i = a + 1; i < e; ++i) {  // insertion sort: buckets hold a few indexes
+      const uint16_t x = bkt[i];
+      uint32_t j = i;
+      while (j > a && bkt[j - 1] > x) {
+        bkt[j] = bkt[j - 1];
+        --j;
+      }
+      bkt[j] = x;
+    }
+    o.first[v] = a < e ? (uint32_t)bkt[a] : OB_NONE;
+    for (uint32_t i = a; i < e; ++i) o.next[bkt[i]] = i + 1 < e ? (uint32_t)bkt[i + 1] : OB_NONE;
   }
 }
 // the origin of shuffled position k (what fy_origin computes), by the chains (first: FIRST[])
