@@ -116,14 +116,15 @@ __global__ void k_ob_chains(const __grid_constant__ DevCtx c, OneBox o) {
     for (uint32_t i = a; i < e; ++i) o.next[o.bkt[i]] = i + 1 < e ? o.bkt[i + 1] : OB_NONE;
   }
 }
-// The front of the step (k_ob_draw, the counts' scan, k_ob_place, k_ob_chains: the same values)
-// in one block for a store of up to OB_FRONT_MAX slots, the counting sort's tables in shared
-// memory: cnt and fill (n + 1 each), J and the buckets as 16-bit indexes (n each). J, FIRST and
-// NEXT go to global memory for k_ob_pairs. Four launches become one.
+// The front of the step (k_ob_draw, the counts' scan, k_ob_place, k_ob_chains and the chain
+// walks: the same values) in one block for a store of up to OB_FRONT_MAX slots, the tables in
+// shared memory: cnt and fill (n + 1 each; fill then holds FIRST), J, the buckets and NEXT as
+// 16-bit indexes (n each). The origins P go to global memory, so k_ob_pairs reads them instead of
+// walking the chains in global memory. Five phases, four launches, become one launch.
 constexpr uint32_t OB_FRONT_THREADS = 1024;
-constexpr uint32_t OB_FRONT_MAX = 16384;
+constexpr uint32_t OB_FRONT_MAX = 16000;
 constexpr size_t ob_front_smem(uint32_t slots) {
-  return (size_t)(slots + 1) * 8 + (size_t)slots * 4 + 16;
+  return (size_t)(slots + 1) * 8 + (size_t)slots * 6 + 16;
 }
 __global__ void __launch_bounds__(OB_FRONT_THREADS)
 k_ob_front(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b, OneBox o) {
@@ -133,7 +134,9 @@ k_ob_front(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratc
   uint32_t* cnt = reinterpret_cast<uint32_t*>(ob_smem);
   uint32_t* fill = cnt + (n + 1);
   uint16_t* J = reinterpret_cast<uint16_t*>(fill + (n + 1));
-  uint16_t* bkt = J + n;  // the n - 1 swap indexes by value
+  uint16_t* bkt = J + n;    // the n - 1 swap indexes by value
+  uint16_t* nxt = bkt + n;  // NEXT
+  uint32_t* first = fill;   // FIRST, once the placement is done with fill
   const uint32_t t = threadIdx.x;
   for (uint32_t v = t; v <= n; v += blockDim.x) {
     cnt[v] = 0u;
@@ -150,7 +153,6 @@ k_ob_front(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratc
     const uint32_t j =
         (uint32_t)cleo_rng_range(cleo_rng_u64(key, slot + (n - 1 - s)), 0, (uint64_t)s + 1);
     J[s] = (uint16_t)j;
-    o.J[s] = j;
     atomicAdd(&cnt[j], 1u);
   }
   __syncthreads();
@@ -174,6 +176,7 @@ k_ob_front(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratc
     bkt[cnt[v] + atomicAdd(&fill[v], 1u)] = (uint16_t)s;
   }
   __syncthreads();
+  constexpr uint16_t NONE16 = 0xFFFFu;  // no index: n <= OB_FRONT_MAX < 2^16 - 1
   for (uint32_t v = t; v < n; v += blockDim.x) {
     const uint32_t a = cnt[v], e = cnt[v + 1];
     for (uint32_t i = a + 1; i < e; ++i) {  // insertion sort: buckets hold a few indexes
@@ -185,8 +188,18 @@ k_ob_front(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratc
       }
       bkt[j] = x;
     }
-    o.first[v] = a < e ? (uint32_t)bkt[a] : OB_NONE;
-    for (uint32_t i = a; i < e; ++i) o.next[bkt[i]] = i + 1 < e ? (uint32_t)bkt[i + 1] : OB_NONE;
+    first[v] = a < e ? (uint32_t)bkt[a] : OB_NONE;  // fill[v] is no longer needed
+    for (uint32_t i = a; i < e; ++i) nxt[bkt[i]] = i + 1 < e ? bkt[i + 1] : NONE16;
+  }
+  __syncthreads();
+  for (uint32_t k = t; k < n; k += blockDim.x) {  // the chain walks (ob_origin's)
+    uint32_t cur = k == 0 ? 0u : (uint32_t)J[k];
+    uint32_t nx = k == 0 ? first[0] : (nxt[k] == NONE16 ? OB_NONE : (uint32_t)nxt[k]);
+    while (nx != OB_NONE) {  // strictly increasing, so at most n hops
+      cur = nx;
+      nx = first[cur];
+    }
+    o.P[k] = cur;
   }
 }
 // the origin of shuffled position k (what fy_origin computes), by the chains (first: FIRST[])
@@ -199,8 +212,9 @@ __device__ __forceinline__ uint32_t ob_origin(const OneBox& o, const uint32_t* f
   }
   return cur;
 }
+// walked: the origins P are in global memory already (k_ob_front), else found here by the chains
 __global__ void k_ob_pairs(const __grid_constant__ DevCtx c, const __grid_constant__ BatchScratch b,
-                           OneBox o) {
+                           OneBox o, int walked) {
   const uint32_t n = c.gcount[0], base = c.gstart[0];
   const uint32_t npairs = n / 2;
   const uint32_t* first = o.first;
@@ -212,9 +226,16 @@ __global__ void k_ob_pairs(const __grid_constant__ DevCtx c, const __grid_consta
   for (uint32_t jj = blockIdx.x * blockDim.x + threadIdx.x; jj <= npairs;
        jj += gridDim.x * blockDim.x) {
     if (jj < npairs) {
-      const uint32_t a = ob_origin(o, first, 2 * jj), bb = ob_origin(o, first, 2 * jj + 1);
-      o.P[2 * jj] = a;
-      o.P[2 * jj + 1] = bb;
+      uint32_t a, bb;
+      if (walked) {
+        a = o.P[2 * jj];
+        bb = o.P[2 * jj + 1];
+      } else {
+        a = ob_origin(o, first, 2 * jj);
+        bb = ob_origin(o, first, 2 * jj + 1);
+        o.P[2 * jj] = a;
+        o.P[2 * jj + 1] = bb;
+      }
       const Where w{c.err, 0u, (uint64_t)base + 2 * jj};
       nnull += collide_pair(c.p, c.sd.xi + base, c.sd.r + base, c.sd.msol + base, a, bb,
                             b.tv[base + a], b.tv[base + bb], scale_p, VOLUME, key, slot_pairs,
@@ -226,7 +247,7 @@ __global__ void k_ob_pairs(const __grid_constant__ DevCtx c, const __grid_consta
       ninv += 2u - fa - fb;
     } else {  // an odd last position (no pair) and the flags' end entry
       if (n & 1u) {
-        const uint32_t p = ob_origin(o, first, n - 1);
+        const uint32_t p = walked ? o.P[n - 1] : ob_origin(o, first, n - 1);
         o.P[n - 1] = p;
         const uint32_t f = c.sd.xi[base + p] != 0 ? 1u : 0u;
         o.vflag[n - 1] = f;

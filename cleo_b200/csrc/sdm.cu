@@ -1325,7 +1325,8 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
           scan_u32(x, a, d.slots + 1, o.tsums);
         }
       };
-      if (d.slots <= OB_FRONT_MAX) {  // draws, counting sort and chains in one block
+      const bool front = d.slots <= OB_FRONT_MAX;
+      if (front) {  // draws, counting sort, chains and their walks in one block
         k_ob_front<<<1, OB_FRONT_THREADS, ob_front_smem(d.slots), s>>>(d, b, o);
         x->launches += 1;
       } else {
@@ -1336,7 +1337,7 @@ int run_batched_micro(cleo_b200_ctx* x, uint32_t t_sdm, uint32_t t_sdm_next, boo
         k_ob_chains<<<go, 256, 0, s>>>(d, o);
         x->launches += 2;
       }
-      k_ob_pairs<<<go, 256, 0, s>>>(d, b, o);
+      k_ob_pairs<<<go, 256, 0, s>>>(d, b, o, front ? 1 : 0);
       x->launches += 1;
       scan(o.vflag, o.ninv);  // valid ones before each shuffled position (none to count: left out)
       k_ob_gather<<<go, 256, 0, s>>>(d, o);
@@ -1788,7 +1789,7 @@ int cleo_b200_create(const cleo_b200_params* params, const cleo_b200_grid* grid,
     x->grid_medium = sms * (occ > 0 ? occ : 1);
     CUDA_TRY(cudaFuncSetAttribute(k_b_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)LARGE_SMEM));
-    if (x->one_box && x->d.slots <= OB_FRONT_MAX)  // at most 196 KB of tables
+    if (x->one_box && x->d.slots <= OB_FRONT_MAX)  // at most 219 KB of tables
       CUDA_TRY(cudaFuncSetAttribute(k_ob_front, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)ob_front_smem(x->d.slots)));
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_cta<true>, LARGE_THREADS,
