@@ -91,8 +91,7 @@ def with_params(wl, **kw):
 
 
 # Bytes per unit of the kernel groups, two counts, both reported:
-# * the algorithmic bytes the survey of the path sets (each touched superdroplet field read once
-#   and written once): condensation 24 B read (r, msol, xi) + 8 B write (r) = 32 B per
+# * the algorithmic bytes (each touched superdroplet field read once and written once): condensation 24 B read (r, msol, xi) + 8 B write (r) = 32 B per
 #   superdroplet; collisions 24 B read + 24 B write (r, msol, xi) = 48 B; the whole SDM step,
 #   fused lower bound, 120 B per superdroplet-step;
 # * the library's own count of what its kernels must move: condensation reads r, msol, xi,
