@@ -237,6 +237,25 @@ def test_gpu_all_bucket_sizes(lib, mode):
     K.assert_identical_run(g, o, "buckets")
 
 
+@pytest.mark.parametrize("small_xi", [False, True], ids=["golovin", "golovin_nulls"])
+def test_gpu_one_box_large_store(lib, small_xi):
+    """A one-gridbox domain whose store is too large for the one-block front kernel (more than
+    16 000 slots): the draws, counting sort and chain walks as separate kernels over the GPU, the
+    scans in several tiles; with small multiplicities collisions leave nulls, which the flags'
+    scan moves behind the valid superdroplets. Bit for bit against the oracle."""
+    w = W.box_golovin(20000, seed=31)
+    if small_xi:
+        rng = np.random.default_rng(31)
+        w["supers"]["xi"][:] = rng.integers(1, 4, 20000).astype(np.uint64)
+        w["state"]["volume"][:] = 1e-13  # large probabilities: about a third become null
+    with_mode(w, abi.EXEC_BATCHED)
+    g, o = run_pair(lib, w, 12)
+    K.assert_identical_run(g, o, "one box, large store")
+    if small_xi:
+        d = g.download_supers()
+        assert d["n_total"] > d["n_domain"]  # nulls left the domain
+
+
 def test_gpu_golovin_analytic(lib):
     """The box model (8192 superdroplets, Golovin kernel, 3600 steps of 1 s) reproduces the
     Golovin analytic spectrum on the GPU: mean over 8 seeds of the relative L1 distance of
